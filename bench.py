@@ -1,0 +1,376 @@
+"""Benchmark: Mvoxels/s of voronoi_otsu_labeling + statistics_of_labelled_pixels.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload nuclei|lightsheet|blobs2d]
+
+Default workload (N=1): the 3D nuclei volume, uint16 128x512x512 (2000
+ellipsoids, PSF, Poisson noise, seed 1); one step = voronoi_otsu_labeling
+(spot_sigma=2, outline_sigma=1) followed by statistics_of_labelled_pixels on
+the same intensity volume.  Data are synthetic (seeded generator with the
+workload's shapes and value distributions).
+
+  value   device-resident throughput: the input already in HBM, every step's
+          device time measured with CUDA events on the launching stream, L2
+          flushed (256 MiB write) between steps.
+  e2e     the same step through the public API with host buffers: pinned
+          host -> device copy of the uint16 volume, the two ops, the label
+          image and the statistics table copied back to pinned host memory.
+  roofline   the dominant kernel stage, timed live with the library's stage
+          events inside the timed steps; achieved = algorithmic bytes / time.
+  cpu_baseline   the CPU oracle (C/OpenMP restatement of the reference's
+          algorithm, all host threads) on the same workload.
+
+--impl reference times the reference's algorithm on the host cores: the
+reference itself cannot run here (pyopencl, a CPU OpenCL runtime and its
+clij-opencl-kernels sources are absent), so its C restatement (oracle/) runs
+instead, with every host thread.
+
+Multi-GPU: replicas (one process per GPU, each runs the full workload; no
+collective on the data path; timing = max over ranks).
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics as st
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mvoxels/s voronoi_otsu_labeling; p50/p99 latency served vs per-call"
+UNIT = "Mvoxels/s"
+
+WORKLOADS = {
+    "nuclei": dict(desc="nuclei volume uint16 128x512x512 (2000 ellipsoids, PSF (1.5,1,1), Poisson, seed 1): "
+                        "voronoi_otsu_labeling(spot_sigma=2, outline_sigma=1) + statistics_of_labelled_pixels",
+                   shape=(128, 512, 512), spot=2.0, outline=1.0),
+    "lightsheet": dict(desc="light-sheet volume uint16 512x1024x1024 (30000 ellipsoids, sinusoidal background, "
+                            "Poisson, seed 2): voronoi_otsu_labeling(spot_sigma=2, outline_sigma=2) + "
+                            "statistics_of_labelled_pixels", shape=(512, 1024, 1024), spot=2.0, outline=2.0),
+    "blobs2d": dict(desc="2D float32 256x256 blobs (seed 0): voronoi_otsu_labeling(spot_sigma=3.5, "
+                         "outline_sigma=1) + statistics_of_labelled_pixels", shape=(256, 256), spot=3.5,
+                    outline=1.0),
+}
+
+# Algorithmic bytes per voxel of each stage (each input read once, each
+# output written once; uint16 source).  Index = stage event interval.
+STAGES = ["blur_spot", "detect_maxima", "blur_outline", "minmax_hist_otsu", "threshold_seeds",
+          "seed_ccl", "voronoi_growth", None, "stats_pass1", "stats_final1", "stats_pass2",
+          "stats_final2"]
+ALGO_BYTES = {"blur_spot": 2 + 4, "detect_maxima": 4 + 1, "blur_outline": 2 + 4,
+              "minmax_hist_otsu": 4 + 4, "threshold_seeds": 4 + 1 + 1 + 4,
+              "stats_pass1": 4 + 2, "stats_pass2": 4 + 2}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_input(name, device=None):
+    from pyclesperanto_prototype_b200 import synthetic
+    w = WORKLOADS[name]
+    if name == "nuclei":
+        return synthetic.cached("c2_nuclei_128x512x512_s1", synthetic.nuclei_volume)
+    if name == "blobs2d":
+        return synthetic.blobs_2d((256, 256), 60, seed=0)
+    vol = synthetic.lightsheet_volume(w["shape"], 30000, seed=2, device=device)
+    return vol
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < len(self.FIELDS):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(x, world):
+    import torch
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline_sample(vol, spot, outline, reps=2):
+    """Oracle on the host cores (all threads); returns (Mvox/s, cores, sample)."""
+    import oracle
+    oracle.build()
+    cores = oracle.num_threads()
+    f = vol.astype(np.float32) if not hasattr(vol, "cpu") else vol.cpu().numpy().astype(np.float32)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        lab = oracle.voronoi_otsu_labeling(f, spot, outline)
+        oracle.statistics_of_labelled_pixels(f, lab)
+        ts.append(time.perf_counter() - t0)
+    t = min(ts)
+    return f.size / t / 1e6, cores, t
+
+
+def run_b200(args):
+    import torch
+    import pyclesperanto_prototype_b200 as cle
+    from pyclesperanto_prototype_b200 import _lib
+
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = _lib.load()
+    w = WORKLOADS[args.workload]
+    host = make_input(args.workload, device=dev)
+    if isinstance(host, torch.Tensor):
+        src = cle.B200Array(host.contiguous())
+        host_np = None
+    else:
+        host_np = host
+        src = cle.push_native(host_np)
+    nvox = int(np.prod(src.shape))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    labels = cle.create_labels_like(src)
+
+    def step():
+        cle._ops._vol(src, labels, w["spot"], w["outline"], check=False)
+        L = cle._ops._label_max(labels)
+        return cle.statistics_table(src, labels, L), L
+
+    # correctness of the loop status once (not timed)
+    cle._ops._vol(src, labels, w["spot"], w["outline"], check=True)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    lib.cle_profile_enable(1)
+    stage_buf = (ctypes.c_float * 16)()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = lib.cle_kernel_launches()
+    times, stage_ms = [], []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        table, L = step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        k = lib.cle_profile_stage_ms(stage_buf, 16)
+        stage_ms.append([stage_buf[i] for i in range(k)])
+    launches = lib.cle_kernel_launches() - n0
+    barrier(world)
+    clk = clocks.stop()
+    lib.cle_profile_enable(0)
+    total_ms = max_over_ranks(sum(times), world)
+    ms_per_step = total_ms / args.steps
+    value = nvox * world * args.steps / (total_ms / 1e3) / 1e6
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if host_np is not None:
+        pinned_in = torch.from_numpy(host_np).pin_memory()
+        pinned_lab = torch.empty(src.shape, dtype=torch.uint32).pin_memory()
+        t_e2e = []
+        for i in range(max(2, args.steps // 2) + 1):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            img = cle.push_native(pinned_in)
+            lab = cle.voronoi_otsu_labeling(img, spot_sigma=w["spot"], outline_sigma=w["outline"])
+            stats = cle.statistics_of_labelled_pixels(img, lab)
+            pinned_lab.copy_(lab.tensor, non_blocking=True)
+            torch.cuda.synchronize()
+            if i:
+                t_e2e.append(time.perf_counter() - t0)
+        te = max_over_ranks(st.mean(t_e2e), world)
+        L_e2e = len(stats["label"])
+        e2e = {"value": nvox * world / te / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(host_np.nbytes),
+               "d2h_bytes_per_step": int(nvox * 4 + 35 * L_e2e * 4 + 8),
+               "ms_per_step": te * 1e3}
+
+    # roofline: the dominant kernel stage
+    sm = np.array([s + [0.0] * (12 - len(s)) for s in stage_ms])[:, :12]
+    mean_stage = sm.mean(axis=0)
+    cands = [(mean_stage[i], STAGES[i]) for i in range(12) if STAGES[i] in ALGO_BYTES]
+    t_dom, dom = max(cands)
+    peak, peak_kind = load_peaks()
+    achieved = ALGO_BYTES[dom] * nvox / (t_dom / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": None, "algorithmic_bytes_per_voxel": ALGO_BYTES[dom]}
+    stages = {STAGES[i]: round(float(mean_stage[i]), 4) for i in range(12) if STAGES[i]}
+    lat = np.array(times)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and host_np is not None:
+        v, cores, t = cpu_baseline_sample(host_np, w["spot"], w["outline"])
+        cpu = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"full workload ({nvox} voxels) once per repetition, best of 2, {t:.2f} s"}
+    if rank == 0:
+        out = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic", "impl": "b200",
+               "config": {"workload": w["desc"], "voxels_per_step": nvox, "labels": int(L),
+                          "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas",
+                          "input_dtype": str(src.dtype)},
+               "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
+                              "p99": round(float(np.percentile(lat, 99)), 4)},
+               "stages_ms": stages, "e2e": e2e, "gpu_launches": int(launches),
+               "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    w = WORKLOADS[args.workload]
+    if args.workload == "lightsheet":
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement needs hours per step "
+                          "on this workload; timed on the nuclei workload instead"}))
+        return
+    host = make_input(args.workload)
+    f = host.astype(np.float32)
+    cores = oracle.num_threads()
+    # one untimed full step sizes the per-step sample so the run stays short
+    t0 = time.perf_counter()
+    lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
+    oracle.statistics_of_labelled_pixels(f, lab)
+    t_full = time.perf_counter() - t0
+    budget = 150.0
+    if f.ndim == 3 and t_full * (args.steps + args.warmup) > budget:
+        planes = max(8, int(f.shape[0] * budget / (t_full * (args.steps + args.warmup))))
+        f = np.ascontiguousarray(f[:planes])
+    sample = f"{f.shape} slab of the workload per step" if f.shape != host.shape else "full workload per step"
+    for _ in range(args.warmup):
+        lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
+        oracle.statistics_of_labelled_pixels(f, lab)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
+        oracle.statistics_of_labelled_pixels(f, lab)
+        ts.append(time.perf_counter() - t0)
+    total = sum(ts)
+    v = f.size * args.steps / total / 1e6
+    print(json.dumps({
+        "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference", "config": {"workload": w["desc"], "voxels_per_step": int(f.size)},
+        "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU OpenCL path unavailable (no pyopencl / CPU OpenCL runtime / kernel sources); "
+                "its C restatement runs on all host threads"}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="nuclei", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,214 @@
+/*
+ * cle_b200.h -- C ABI of libcle_b200.so, the sm_100a implementation of
+ * pyclesperanto_prototype's voronoi_otsu_labeling + statistics path.
+ *
+ * Conventions
+ *   - Every image is a cle_tensor: a device pointer plus numpy-order shape
+ *     (z, y, x) for 3D or (y, x) for 2D, C-contiguous (strides are element
+ *     strides and are validated), dtype code and CUDA device ordinal.
+ *   - Every compute entry point is asynchronous on the given CUDA stream
+ *     (a cudaStream_t passed as void*; NULL = the legacy default stream) and
+ *     returns a cle_status.  On failure cle_last_error_message() (thread
+ *     local) holds a description.
+ *   - Entry points never allocate device memory.  Scratch comes from a
+ *     caller-provided workspace; its size is returned by the matching
+ *     *_workspace_bytes() query (0 means none needed).  Workspaces must be
+ *     256-byte aligned and must not be shared by calls that may overlap.
+ *   - Output dtypes follow the reference's output creators
+ *     (_tier0/_create.py:26-52): float32 (create_like), uint8
+ *     (create_binary_like), uint32 (create_labels_like).  Where the
+ *     reference also accepts a caller destination of another type the
+ *     entry point converts the way the reference's WRITE_IMAGE does.
+ *
+ * The "replaces" line on each entry point names the reference function
+ * (pyclesperanto_prototype/<file>:<line>) whose behaviour it implements.
+ */
+#ifndef CLE_B200_H
+#define CLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLE_B200_ABI_VERSION 1
+
+typedef enum cle_dtype {
+    CLE_U8 = 1,
+    CLE_U16 = 2,
+    CLE_U32 = 3,
+    CLE_I32 = 4,
+    CLE_F32 = 5
+} cle_dtype;
+
+typedef enum cle_status {
+    CLE_OK = 0,
+    CLE_ERR_DTYPE = 1,      /* unsupported dtype              -> KeyError   */
+    CLE_ERR_SHAPE = 2,      /* shapes disagree / not 2D or 3D -> ValueError */
+    CLE_ERR_ARG = 3,        /* bad scalar argument            -> ValueError */
+    CLE_ERR_WORKSPACE = 4,  /* workspace missing or too small -> RuntimeError */
+    CLE_ERR_ITER_LIMIT = 5, /* device loop hit its step/time limit          */
+    CLE_ERR_CUDA = 6,       /* CUDA runtime error             -> RuntimeError */
+    CLE_ERR_TOO_LARGE = 7   /* image exceeds the 2^31-2 voxel index range   */
+} cle_status;
+
+typedef struct cle_tensor {
+    void *data;         /* device pointer                                   */
+    int32_t ndim;       /* 1, 2 or 3                                        */
+    int32_t dtype;      /* cle_dtype                                        */
+    int64_t shape[3];   /* numpy order; unused trailing entries ignored     */
+    int64_t strides[3]; /* element strides, must be C-contiguous            */
+    int32_t device;     /* CUDA device ordinal                              */
+} cle_tensor;
+
+/* Number of float32 columns of the statistics table (see
+ * cle_statistics_of_labelled_pixels). */
+#define CLE_STATS_NCOLS 35
+
+/* ---- library ---------------------------------------------------------- */
+int cle_abi_version(void);
+const char *cle_version(void);
+const char *cle_last_error_message(void);
+/* Number of kernel launches this library has issued in this process. */
+unsigned long long cle_kernel_launches(void);
+/* Stage timing for profiling: when enabled on the calling thread, the
+ * composite ops record a CUDA event at each stage boundary on their stream.
+ * cle_profile_stage_ms() waits for the last recorded event and writes the
+ * elapsed milliseconds between consecutive events (returns how many).
+ * Events 0-7 (voronoi_otsu_labeling): blur(spot) | detect_maxima |
+ * blur(outline) | min/max+histogram+Otsu | threshold+seeds | seed CCL |
+ * Voronoi growth; events 8-12 (statistics): pass 1 | finalise 1 | pass 2 |
+ * finalise 2.  Interval 7 (between the two ops) is host time. */
+int cle_profile_enable(int on);
+int cle_profile_stage_ms(float *out, int max);
+
+/* ---- gaussian_blur -----------------------------------------------------
+ * replaces _tier1/_gaussian_blur.py:6-58 (+ _tier1/_execute_separable_kernel.py:7-76,
+ * _tier0/_sigma_to_kernel_size.py:1-4).  src: u8/u16/f32; dst: f32.
+ * Kernel size per axis int(8*sigma)|1; sigma <= 0 leaves that axis as is;
+ * sigma_z is ignored for 2D images. */
+size_t cle_gaussian_blur_workspace_bytes(const cle_tensor *src);
+int cle_gaussian_blur(const cle_tensor *src, const cle_tensor *dst, double sigma_x,
+                      double sigma_y, double sigma_z, void *workspace, size_t workspace_bytes,
+                      void *stream);
+
+/* ---- minimum_of_all_pixels / maximum_of_all_pixels ----------------------
+ * replaces _tier2/_minimum_of_all_pixels.py:7-60 and
+ * _tier2/_maximum_of_all_pixels.py:7-60.  Writes {min, max} as two float32
+ * to the device pointer d_minmax.  src: u8/u16/u32/f32. */
+size_t cle_minimum_maximum_workspace_bytes(const cle_tensor *src);
+int cle_minimum_maximum(const cle_tensor *src, float *d_minmax, void *workspace,
+                        size_t workspace_bytes, void *stream);
+
+/* ---- histogram -----------------------------------------------------------
+ * replaces _tier3/_histogram.py:26-130.  dst: f32[num_bins].  With
+ * determine_min_max != 0 the range is computed on the device (no host
+ * round trip); otherwise [minimum, maximum] is used. */
+size_t cle_histogram_workspace_bytes(const cle_tensor *src, int num_bins);
+int cle_histogram(const cle_tensor *src, const cle_tensor *dst, int num_bins, float minimum,
+                  float maximum, int determine_min_max, void *workspace,
+                  size_t workspace_bytes, void *stream);
+
+/* ---- threshold_otsu ----------------------------------------------------
+ * replaces _tier9/_threshold_otsu.py:11-54 (and the host Otsu of
+ * scikit_image_threshold_otsu, :64-106, now on the device in float64).
+ * dst: u8 or f32 (1/0).  d_threshold (may be NULL) receives the float64
+ * threshold. */
+size_t cle_threshold_otsu_workspace_bytes(const cle_tensor *src);
+int cle_threshold_otsu(const cle_tensor *src, const cle_tensor *dst, double *d_threshold,
+                       void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- element-wise ops --------------------------------------------------
+ * greater_constant replaces _tier1/_greater_constant.py:6-40 (constant as float32);
+ * binary_and       replaces _tier1/_binary_and.py:6-47;
+ * mask             replaces _tier1/_mask.py:6-44 (f32 -> u32 saturating like
+ *                  clij_convert_uint_sat, _tier0/preamble.cl:548-556). */
+int cle_greater_constant(const cle_tensor *src, const cle_tensor *dst, float constant,
+                         void *stream);
+int cle_binary_and(const cle_tensor *a, const cle_tensor *b, const cle_tensor *dst, void *stream);
+int cle_mask(const cle_tensor *src, const cle_tensor *mask, const cle_tensor *dst, void *stream);
+
+/* ---- detect_maxima_box ---------------------------------------------------
+ * replaces _tier1/_detect_maxima_box.py:5-48 with kernels
+ * _tier1/detect_maxima_3d_x.cl:1-49, _tier1/detect_maxima_2d_x.cl:1-35.
+ * Radii > 0 apply mean_box first (as the reference does); dst: u8 or f32. */
+size_t cle_detect_maxima_box_workspace_bytes(const cle_tensor *src, int rx, int ry, int rz);
+int cle_detect_maxima_box(const cle_tensor *src, const cle_tensor *dst, int rx, int ry, int rz,
+                          void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- connected_components_labeling_box ---------------------------------
+ * replaces _tier4/_connected_components_labeling_box.py:15-66 (+ relabel,
+ * _tier3/_relabel_sequential.py:12-58).  binary: u8/u32/f32 (nonzero =
+ * foreground); dst: u32 or f32.  Labels are the ranks of each component's
+ * float32 pixel-index key (x-major), as in the reference. */
+size_t cle_connected_components_labeling_box_workspace_bytes(const cle_tensor *binary);
+int cle_connected_components_labeling_box(const cle_tensor *binary, const cle_tensor *dst,
+                                          void *workspace, size_t workspace_bytes,
+                                          void *stream);
+
+/* ---- relabel_sequential --------------------------------------------------
+ * replaces _tier3/_relabel_sequential.py:12-58.  src: u32 or f32 labels;
+ * dst: u32 or f32.  max_label is the maximum of src (the reference also
+ * reads it first, :42). */
+size_t cle_relabel_sequential_workspace_bytes(const cle_tensor *src, uint32_t max_label);
+int cle_relabel_sequential(const cle_tensor *src, const cle_tensor *dst, uint32_t max_label,
+                           void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- masked_voronoi_labeling -------------------------------------------
+ * replaces _tier5/_masked_voronoi_labeling.py:7-76.  binary: seeds (u8/u32/f32,
+ * nonzero); mask: u8/f32; dst: u32 or f32.  General form: any mask values,
+ * seeds anywhere (dense Jacobi on the device, exact reference semantics). */
+size_t cle_masked_voronoi_labeling_workspace_bytes(const cle_tensor *binary);
+int cle_masked_voronoi_labeling(const cle_tensor *binary, const cle_tensor *mask,
+                                const cle_tensor *dst, void *workspace, size_t workspace_bytes,
+                                void *stream);
+
+/* ---- voronoi_otsu_labeling ---------------------------------------------
+ * replaces _tier9/_voronoi_otsu_labeling.py:11-73.  src: u8/u16/f32 (u8 and
+ * u16 are converted on the fly, exactly as push's float32 cast would);
+ * dst: u32 (or f32).  No host synchronisation inside. */
+size_t cle_voronoi_otsu_labeling_workspace_bytes(const cle_tensor *src);
+int cle_voronoi_otsu_labeling(const cle_tensor *src, const cle_tensor *dst, double spot_sigma,
+                              double outline_sigma, void *workspace, size_t workspace_bytes,
+                              void *stream);
+
+/* Device status word of the last voronoi_otsu_labeling / masked Voronoi
+ * call that used this workspace: 0 = finished, else a cle_status.  Reads
+ * 4 bytes (synchronises the stream). */
+int cle_workspace_status(const void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- maximum label -------------------------------------------------------
+ * Maximum value of a label image (u32 or f32 read as (int)), written as one
+ * uint32 to d_max (device).  Used to size the statistics table
+ * (_tier9/_statistics_of_labelled_pixels.py:56). */
+size_t cle_label_maximum_workspace_bytes(const cle_tensor *labels);
+int cle_label_maximum(const cle_tensor *labels, uint32_t *d_max, void *workspace,
+                      size_t workspace_bytes, void *stream);
+
+/* ---- statistics_of_labelled_pixels -------------------------------------
+ * replaces _tier9/_statistics_of_labelled_pixels.py:7-293 (kernels
+ * _tier9/statistics_per_label_x.cl, _tier9/standard_deviation_per_label_x.cl).
+ * Writes a float32 table of CLE_STATS_NCOLS rows x num_labels columns
+ * (row-major) to d_table, rows in the reference's dict order after 'label'
+ * and 'original_label':
+ *   bbox_min_x/y/z, bbox_max_x/y/z, bbox_width/height/depth, min_intensity,
+ *   max_intensity, sum_intensity, area, mean_intensity,
+ *   sum_intensity_times_x, mass_center_x, (y), (z), sum_x, centroid_x, (y),
+ *   (z), sum_distance_to_centroid, mean_distance_to_centroid,
+ *   sum_distance_to_mass_center, mean_distance_to_mass_center,
+ *   standard_deviation_intensity, max_distance_to_centroid,
+ *   max_distance_to_mass_center, mean_max_distance_to_centroid_ratio,
+ *   mean_max_distance_to_mass_center_ratio.
+ * Labels 1..num_labels; values above num_labels are ignored. */
+size_t cle_statistics_workspace_bytes(const cle_tensor *labels, int64_t num_labels);
+int cle_statistics_of_labelled_pixels(const cle_tensor *intensity, const cle_tensor *labels,
+                                      int64_t num_labels, float *d_table, void *workspace,
+                                      size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLE_B200_H */

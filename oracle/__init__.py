@@ -1,0 +1,253 @@
+"""CPU oracle for the voronoi_otsu_labeling + statistics path.
+
+TEST INFRASTRUCTURE ONLY: the parity checker for the CUDA library and the
+timed CPU baseline.  Only ``tests/``, ``__graft_entry__.smoke()`` and
+``bench.py`` (its ``cpu_baseline`` leg and ``--impl reference``) import this
+package; the product package never does.
+
+The arithmetic lives in ``cle_oracle.c`` (a C restatement of the reference's
+algorithm, citing the reference file:line for each step); this module is a
+thin numpy/ctypes wrapper.  ``build()`` compiles it with the committed
+Makefile.
+
+Parity status: pinned against every golden vector the reference's own tests
+hold for this path (tests/test_oracle_golden.py) and the demo known answers on
+``blobs.tif`` (tests/golden/).  Unpinned by any reference fixture: the z term
+of the 3D CCL key (x-major ``(x*H + y)*D + z`` assumed), the choice between
+histogram bin rules (``floor((v-min)*255/range + 0.5)`` used), the float32
+operation order inside a Gaussian pass (fused multiply-add chain used).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libcle_oracle.so")
+_lib = None
+
+NCOLS = 35
+STAT_KEYS = [
+    "bbox_min_x", "bbox_min_y", "bbox_min_z", "bbox_max_x", "bbox_max_y", "bbox_max_z",
+    "bbox_width", "bbox_height", "bbox_depth", "min_intensity", "max_intensity",
+    "sum_intensity", "area", "mean_intensity",
+    "sum_intensity_times_x", "mass_center_x", "sum_intensity_times_y", "mass_center_y",
+    "sum_intensity_times_z", "mass_center_z",
+    "sum_x", "centroid_x", "sum_y", "centroid_y", "sum_z", "centroid_z",
+    "sum_distance_to_centroid", "mean_distance_to_centroid",
+    "sum_distance_to_mass_center", "mean_distance_to_mass_center",
+    "standard_deviation_intensity", "max_distance_to_centroid", "max_distance_to_mass_center",
+    "mean_max_distance_to_centroid_ratio", "mean_max_distance_to_mass_center_ratio",
+]
+
+
+def build() -> str:
+    """Compile libcle_oracle.so in place (idempotent)."""
+    src = os.path.join(_HERE, "cle_oracle.c")
+    if (not os.path.exists(_LIB_PATH)) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        I64 = ctypes.c_int64
+        D = ctypes.c_double
+        I = ctypes.c_int
+        F = ctypes.c_float
+        L.orc_num_threads.restype = I
+        L.orc_set_num_threads.argtypes = [I]
+        L.orc_sigma_to_kernel_size.argtypes = [D]
+        L.orc_sigma_to_kernel_size.restype = I
+        L.orc_gauss_weights.argtypes = [D, I, P]
+        L.orc_gaussian_blur.argtypes = [P, P, I64, I64, I64, I, D, D, D]
+        L.orc_detect_maxima.argtypes = [P, P, I64, I64, I64, I]
+        L.orc_minmax.argtypes = [P, I64, P, P]
+        L.orc_histogram.argtypes = [P, I64, I64, I64, I, F, F, P]
+        L.orc_otsu_threshold.argtypes = [P, I, F, F]
+        L.orc_otsu_threshold.restype = D
+        L.orc_greater_constant.argtypes = [P, P, I64, F]
+        L.orc_binary_and.argtypes = [P, P, P, I64]
+        L.orc_threshold_otsu.argtypes = [P, P, I64, I64, I64]
+        L.orc_threshold_otsu.restype = D
+        L.orc_ccl_box.argtypes = [P, P, I64, I64, I64]
+        L.orc_ccl_box.restype = I64
+        L.orc_relabel_sequential.argtypes = [P, P, I64]
+        L.orc_masked_voronoi.argtypes = [P, P, P, P, I64, I64, I64, I]
+        L.orc_masked_voronoi.restype = I64
+        L.orc_voronoi_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, D, D, P, P, P]
+        L.orc_voronoi_otsu_labeling.restype = I64
+        L.orc_statistics.argtypes = [P, P, I64, I64, I64, I64, P]
+        L.orc_stats_ncols.restype = I
+        assert L.orc_stats_ncols() == NCOLS
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _dhw(shape):
+    if len(shape) == 2:
+        return 1, shape[0], shape[1]
+    if len(shape) == 3:
+        return shape
+    raise ValueError(f"2D or 3D image expected, got shape {shape}")
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a), dtype=np.float32)
+
+
+def _u8(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a) != 0, dtype=np.uint8)
+
+
+def set_num_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def sigma_to_kernel_size(sigma: float) -> int:
+    return lib().orc_sigma_to_kernel_size(float(sigma))
+
+
+def gauss_weights(sigma: float) -> np.ndarray:
+    n = sigma_to_kernel_size(sigma)
+    w = np.empty(n, np.float32)
+    lib().orc_gauss_weights(float(sigma), n, _p(w))
+    return w
+
+
+def gaussian_blur(img, sigma_x=0.0, sigma_y=0.0, sigma_z=0.0) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty_like(a)
+    D, H, W = _dhw(a.shape)
+    lib().orc_gaussian_blur(_p(a), _p(out), D, H, W, a.ndim, float(sigma_x), float(sigma_y),
+                            float(sigma_z))
+    return out
+
+
+def detect_maxima(img) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint8)
+    D, H, W = _dhw(a.shape)
+    lib().orc_detect_maxima(_p(a), _p(out), D, H, W, a.ndim)
+    return out
+
+
+def minmax(img):
+    a = _f32(img)
+    mn = np.zeros(1, np.float32)
+    mx = np.zeros(1, np.float32)
+    lib().orc_minmax(_p(a), a.size, _p(mn), _p(mx))
+    return mn[0], mx[0]
+
+
+def histogram(img, num_bins=256, minimum_intensity=None, maximum_intensity=None) -> np.ndarray:
+    a = _f32(img)
+    if minimum_intensity is None or maximum_intensity is None:
+        minimum_intensity, maximum_intensity = minmax(a)
+    out = np.empty(num_bins, np.float32)
+    D, H, W = _dhw(a.shape)
+    lib().orc_histogram(_p(a), D, H, W, int(num_bins), float(minimum_intensity),
+                        float(maximum_intensity), _p(out))
+    return out
+
+
+def otsu_threshold_from_histogram(hist, mn, mx) -> float:
+    h = _f32(hist)
+    return lib().orc_otsu_threshold(_p(h), h.size, float(mn), float(mx))
+
+
+def threshold_otsu(img):
+    """Returns (binary u8, float64 threshold)."""
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint8)
+    D, H, W = _dhw(a.shape)
+    t = lib().orc_threshold_otsu(_p(a), _p(out), D, H, W)
+    return out, t
+
+
+def greater_constant(img, constant) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint8)
+    lib().orc_greater_constant(_p(a), _p(out), a.size, float(constant))
+    return out
+
+
+def binary_and(a, b) -> np.ndarray:
+    x, y = _u8(a), _u8(b)
+    out = np.empty(x.shape, np.uint8)
+    lib().orc_binary_and(_p(x), _p(y), _p(out), x.size)
+    return out
+
+
+def connected_components_labeling_box(binary) -> np.ndarray:
+    fg = _u8(binary)
+    out = np.empty(fg.shape, np.uint32)
+    D, H, W = _dhw(fg.shape)
+    lib().orc_ccl_box(_p(fg), _p(out), D, H, W)
+    return out
+
+
+def relabel_sequential(labels) -> np.ndarray:
+    a = np.asarray(labels)
+    if a.dtype.kind == "f":
+        a = a.astype(np.int64)
+    a = np.ascontiguousarray(np.clip(a, 0, None), dtype=np.uint32)
+    out = np.empty_like(a)
+    lib().orc_relabel_sequential(_p(a), _p(out), a.size)
+    return out
+
+
+def masked_voronoi_labeling(seeds, mask, return_steps=False):
+    s = _u8(seeds)
+    m = _f32(mask)
+    out = np.empty(s.shape, np.uint32)
+    D, H, W = _dhw(s.shape)
+    steps = lib().orc_masked_voronoi(_p(s), _p(m), None, _p(out), D, H, W, s.ndim)
+    return (out, steps) if return_steps else out
+
+
+def voronoi_otsu_labeling(img, spot_sigma=2.0, outline_sigma=2.0, debug=False):
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint32)
+    D, H, W = _dhw(a.shape)
+    spots = np.empty(a.shape, np.uint8)
+    seg = np.empty(a.shape, np.uint8)
+    thr = np.zeros(1, np.float64)
+    steps = lib().orc_voronoi_otsu_labeling(_p(a), _p(out), D, H, W, a.ndim, float(spot_sigma),
+                                            float(outline_sigma), _p(spots), _p(seg), _p(thr))
+    if debug:
+        return out, dict(seeds=spots, segmentation=seg, threshold=float(thr[0]), steps=steps)
+    return out
+
+
+def statistics_of_labelled_pixels(intensity, labels) -> dict:
+    lab = np.asarray(labels)
+    if lab.dtype.kind == "f":
+        lab = lab.astype(np.int64)
+    lab = np.ascontiguousarray(np.clip(lab, 0, None), dtype=np.uint32)
+    inten = _f32(intensity)
+    L = int(lab.max()) if lab.size else 0
+    table = np.empty((NCOLS, max(L, 1)), np.float32)
+    D, H, W = _dhw(lab.shape)
+    if L > 0:
+        lib().orc_statistics(_p(inten), _p(lab), D, H, W, L, _p(table))
+    table = table[:, :L]
+    out = {"label": np.arange(1, L + 1), "original_label": np.arange(1, L + 1)}
+    for i, k in enumerate(STAT_KEYS):
+        out[k] = table[i].copy()
+    return out

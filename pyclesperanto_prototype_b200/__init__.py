@@ -1,0 +1,58 @@
+"""pyclesperanto_prototype_b200 -- the voronoi_otsu_labeling +
+statistics_of_labelled_pixels path of pyclesperanto_prototype, as hand-written
+sm_100a CUDA kernels behind the reference's cle.* signatures.
+
+    import pyclesperanto_prototype_b200 as cle
+    labels = cle.voronoi_otsu_labeling(image, spot_sigma=2, outline_sigma=1)
+    stats = cle.statistics_of_labelled_pixels(image, labels)
+
+Device images are torch CUDA tensors wrapped in B200Array; the kernels live in
+libcle_b200.so (C ABI, include/cle_b200.h), reached through ctypes.  Without
+the library or a CUDA device the ops raise; there is no CPU fallback.
+"""
+from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, create_binary_like,
+                     create_labels_like, create_like, create_none, create_zyx, is_image, nparray,
+                     plugin_function, pull, pull_zyx, push, push_native, push_zyx)
+from ._ops import (binary_and, connected_components_labeling_box, detect_maxima_box,
+                   gaussian_blur, greater_constant, histogram, mask, masked_voronoi_labeling,
+                   maximum_of_all_pixels, minimum_of_all_pixels, radius_to_kernel_size,
+                   relabel_sequential, scikit_image_threshold_otsu, sigma_to_kernel_size,
+                   statistics_of_labeled_pixels, statistics_of_labelled_pixels, statistics_table,
+                   threshold_otsu, voronoi_otsu_labeling, workspaces, STAT_KEYS)
+
+__version__ = "0.1.0"
+__common_alias__ = "cle"
+
+
+def get_device():
+    import torch
+    from . import _lib
+    _lib.load()
+    return torch.cuda.get_device_name(torch.cuda.current_device())
+
+
+def select_device(name: str = "", dev_type: str = "all", score_key=None, device_index: int = None):
+    """Selects the CUDA device whose name contains `name` (or device_index),
+    like the reference's select_device (_tier0/_device.py:48-84)."""
+    import torch
+    from . import _lib
+    _lib.load()
+    if device_index is not None:
+        torch.cuda.set_device(int(device_index))
+        return get_device()
+    for i in range(torch.cuda.device_count()):
+        if name.lower() in torch.cuda.get_device_name(i).lower():
+            torch.cuda.set_device(i)
+            return get_device()
+    return get_device()
+
+
+def available_device_names(dev_type: str = None, score_key=None):
+    import torch
+    return [torch.cuda.get_device_name(i) for i in range(torch.cuda.device_count())]
+
+
+def set_wait_for_kernel_finish(wait: bool = None):
+    """Kept for API compatibility: launches are stream-ordered; synchronise
+    with torch.cuda.synchronize() when timing."""
+    return None

@@ -1,0 +1,80 @@
+// kernels.cuh -- internal (C++) interface between the op files and the C ABI.
+#pragma once
+
+#include "common.cuh"
+
+namespace cle {
+
+// blur.cu
+size_t separable_workspace_bytes(const Img &im);
+int separable_filter(const Img &src, float *dst, const Taps *tx, const Taps *ty, const Taps *tz,
+                     Arena &ws, cudaStream_t st);
+int gaussian_blur(const Img &src, float *dst, double sx, double sy, double sz, Arena &ws,
+                  cudaStream_t st);
+
+// reduce.cu
+struct MinMaxScratch {
+    float *partial;   // 2 * blocks
+    int blocks;
+};
+size_t minmax_workspace_bytes(const Img &im);
+// Writes {min, max} to d_out (device) without host synchronisation.
+int minmax(const Img &im, float *d_out, Arena &ws, cudaStream_t st);
+size_t histogram_workspace_bytes(const Img &im, int bins);
+// Row-partial histogram + float32 row sum (reference order); d_minmax holds {min,max}.
+int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Arena &ws,
+              cudaStream_t st);
+// Otsu on a 256-bin float32 histogram, device float64.  Writes the float64
+// threshold to d_thr (may be null) and its float32 cast to d_thr32.
+int otsu(const float *d_hist, const float *d_minmax, double *d_thr, float *d_thr32,
+         cudaStream_t st);
+int greater_constant(const Img &src, const Img &dst, float c, const float *d_c, cudaStream_t st);
+int binary_and(const Img &a, const Img &b, const Img &dst, cudaStream_t st);
+int mask_op(const Img &src, const Img &mask, const Img &dst, cudaStream_t st);
+int label_max(const Img &labels, uint32_t *d_max, Arena &ws, cudaStream_t st);
+size_t label_max_workspace_bytes(const Img &im);
+
+// maxima.cu
+int detect_maxima(const Img &src, const Img &dst, cudaStream_t st);
+
+// ccl.cu
+size_t ccl_workspace_bytes(const Img &im);
+// Dense CCL of (binary != 0) into u32 labels (x-major float32 key ranks).
+int ccl_dense(const Img &binary, uint32_t *labels, Arena &ws, cudaStream_t st);
+// CCL restricted to a device list of voxel indices whose entries in `labels`
+// already hold (own x-major key + 1); on return those entries hold labels.
+// d_count: device count of list entries; cap: list capacity.
+int ccl_list(const Geo &g, int64_t n, uint32_t *labels, const uint32_t *list,
+             const uint32_t *d_count, int64_t cap, Arena &ws, cudaStream_t st);
+int ccl_to_dst(const uint32_t *lab, const Img &dst, cudaStream_t st);
+size_t relabel_workspace_bytes(uint32_t max_label);
+int relabel_sequential(const Img &src, const Img &dst, uint32_t max_label, Arena &ws,
+                       cudaStream_t st);
+size_t rank_workspace_bytes(uint64_t bits);
+
+// voronoi.cu
+size_t voronoi_frontier_workspace_bytes(const Img &im);
+// Frontier-queued Jacobi growth.  labels: u32 with seed labels, 0 elsewhere;
+// seg: u8 mask (0/1); seeds: device list of seed memory indices (count in
+// d_seed_count).  d_status receives 0 or an error.
+int voronoi_frontier(const Img &shape, uint32_t *labels, const uint8_t *seg,
+                     const uint32_t *seeds, const uint32_t *d_seed_count, int *d_status,
+                     Arena &ws, cudaStream_t st);
+size_t voronoi_dense_workspace_bytes(const Img &im);
+int masked_voronoi_dense(const Img &binary, const Img &mask, const Img &dst, int *d_status,
+                         Arena &ws, cudaStream_t st);
+
+// stats.cu
+size_t stats_workspace_bytes(const Img &labels, int64_t L);
+int statistics(const Img &inten, const Img &labels, int64_t L, float *d_table, Arena &ws,
+               cudaStream_t st);
+
+// pipeline.cu
+size_t vol_workspace_bytes(const Img &im);
+int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma,
+                          double outline_sigma, Arena &ws, cudaStream_t st);
+
+// Status word at a fixed offset of every composite workspace (first 256 B).
+int *workspace_status_ptr(void *ws);
+
+}  // namespace cle

@@ -1,0 +1,136 @@
+// maxima.cu -- detect_maxima_box with radius 1 (_tier1/detect_maxima_3d_x.cl:1-49,
+// _tier1/detect_maxima_2d_x.cl:1-35).
+//
+// The reference kernel walks the 3^d box in order dx (outer), dy, dz (inner),
+// starting from localMax = v(p) - 1, skipping positions with a negative
+// coordinate, reading clamp-to-edge and keeping the first strict maximum;
+// p is flagged iff that arg-max is p itself.  For v(p) - 1 < v(p) this is
+// exactly:  v(p) > max(in-bounds neighbours preceding p in walk order)  and
+// v(p) >= max(in-bounds neighbours following p)  -- clamped re-reads of the
+// upper border only repeat voxels whose constraint is already implied.  When
+// v(p) - 1 == v(p) (|v| >= 2^24, inf) both comparisons are >=; a NaN centre
+// always wins and NaN neighbours never do.
+//
+// The preceding set is {dx=-1: all} + {dx=0, dy=-1: all dz} + {(0,0,-1)}, so
+// with T(x,y) = max_dz v and S(x,y) = max_dy T:
+//   A = max(S(x-1,y), T(x,y-1), v(z-1)),  B = max(S(x+1,y), T(x,y+1), v(z+1)).
+// Each thread owns 4 consecutive rows of one x column and marches along z
+// with a 3-plane x 6-row register window; x neighbours come from warp
+// shuffles (a warp covers 30 output columns plus one halo lane each side).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace cle {
+
+namespace {
+
+constexpr int kRows = 4;          // output rows per thread
+constexpr int kWin = kRows + 2;   // rows held (halo above and below)
+constexpr int kOutX = 30;         // output columns per warp
+constexpr int kGroups = 4;        // y-groups (warps) per block
+
+template <typename Ts, typename Td>
+__global__ void __launch_bounds__(32 * kGroups)
+maxima_kernel(const Ts *__restrict__ src, Td *__restrict__ dst, int D, int H, int W, int zchunk) {
+    const int lane = threadIdx.x;
+    const int x = (int)blockIdx.x * kOutX + lane - 1;
+    const int y0 = ((int)blockIdx.y * kGroups + threadIdx.y) * kRows;
+    const int z0 = (int)blockIdx.z * zchunk;
+    const int z1 = min(D, z0 + zchunk);
+    if (y0 >= H) return;   // whole warp leaves together (y0 is warp-uniform)
+    const bool xin = (x >= 0 && x < W);
+    const float NEG = -INFINITY;
+
+    auto load = [&](int z, int j) -> float {
+        int y = y0 - 1 + j;
+        if (!xin || z < 0 || z >= D || y < 0 || y >= H) return NEG;
+        return to_f32(src[((int64_t)z * H + y) * W + x]);
+    };
+
+    float vm[kWin], vc[kWin], vp[kWin];
+#pragma unroll
+    for (int j = 0; j < kWin; ++j) {
+        vm[j] = load(z0 - 1, j);
+        vc[j] = load(z0, j);
+    }
+    for (int z = z0; z < z1; ++z) {
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) vp[j] = load(z + 1, j);
+        float T[kWin];
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) T[j] = fmaxf(fmaxf(vm[j], vc[j]), vp[j]);
+        float S[kRows];
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) S[j] = fmaxf(fmaxf(T[j], T[j + 1]), T[j + 2]);
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) {
+            const float sl = __shfl_up_sync(0xffffffffu, S[j], 1);
+            const float sr = __shfl_down_sync(0xffffffffu, S[j], 1);
+            const int y = y0 + j;
+            if (lane >= 1 && lane <= kOutX && xin && y < H) {
+                const float v = vc[j + 1];
+                const float A = fmaxf(fmaxf(sl, T[j]), vm[j + 1]);
+                const float B = fmaxf(fmaxf(sr, T[j + 2]), vp[j + 1]);
+                bool win;
+                if (v != v) {
+                    win = true;
+                } else if (__fsub_rn(v, 1.0f) < v) {
+                    win = (v > A) && (v >= B);
+                } else {
+                    win = (v >= A) && (v >= B);
+                }
+                dst[((int64_t)z * H + y) * W + x] = (Td)(win ? 1 : 0);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) {
+            vm[j] = vc[j];
+            vc[j] = vp[j];
+        }
+    }
+}
+
+template <typename Ts, typename Td>
+int launch_maxima(const Img &src, const Img &dst, cudaStream_t st) {
+    const int D = (int)src.D, H = (int)src.H, W = (int)src.W;
+    const int gx = (W + kOutX - 1) / kOutX;
+    const int gy = (H + kRows * kGroups - 1) / (kRows * kGroups);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int64_t target = (int64_t)num_sms(dev) * 12;   // blocks
+    int64_t zchunks = (target + (int64_t)gx * gy - 1) / ((int64_t)gx * gy);
+    if (zchunks > D) zchunks = D;
+    if (zchunks < 1) zchunks = 1;
+    int zchunk = (int)((D + zchunks - 1) / zchunks);
+    if (zchunk < 4 && D >= 4) zchunk = 4;
+    zchunks = (D + zchunk - 1) / zchunk;
+    if (gy > 65535 || zchunks > 65535) { set_error("detect_maxima: image too large"); return CLE_ERR_TOO_LARGE; }
+    dim3 grid(gx, gy, (unsigned)zchunks), block(32, kGroups);
+    maxima_kernel<Ts, Td><<<grid, block, 0, st>>>((const Ts *)src.data, (Td *)dst.data, D, H, W, zchunk);
+    CLE_LAUNCH_CHECK("detect_maxima");
+    return CLE_OK;
+}
+
+template <typename Ts>
+int maxima_dst(const Img &src, const Img &dst, cudaStream_t st) {
+    switch (dst.dtype) {
+        case CLE_U8: return launch_maxima<Ts, uint8_t>(src, dst, st);
+        case CLE_F32: return launch_maxima<Ts, float>(src, dst, st);
+        case CLE_U32: return launch_maxima<Ts, uint32_t>(src, dst, st);
+        default: set_error("detect_maxima_box: unsupported destination dtype %d", dst.dtype); return CLE_ERR_DTYPE;
+    }
+}
+
+}  // namespace
+
+int detect_maxima(const Img &src, const Img &dst, cudaStream_t st) {
+    CLE_TRY(same_shape(src, dst, "source", "destination"));
+    switch (src.dtype) {
+        case CLE_F32: return maxima_dst<float>(src, dst, st);
+        case CLE_U16: return maxima_dst<uint16_t>(src, dst, st);
+        case CLE_U8: return maxima_dst<uint8_t>(src, dst, st);
+        default: set_error("detect_maxima_box: unsupported source dtype %d", src.dtype); return CLE_ERR_DTYPE;
+    }
+}
+
+}  // namespace cle

@@ -1,0 +1,176 @@
+// pipeline.cu -- voronoi_otsu_labeling (_tier9/_voronoi_otsu_labeling.py:49-73) as one
+// stream-ordered sequence with no host round trip:
+//   T = gaussian_blur(src, spot_sigma)            (blur.cu)
+//   spots = detect_maxima_box(T)                  (maxima.cu; mean_box r=0 is a copy)
+//   T = gaussian_blur(src, outline_sigma)
+//   {min,max} -> histogram -> Otsu -> t32         (reduce.cu, all on the device)
+//   seg = T > t32; seeds = spots & seg            (seed kernel below; emits the seed list
+//                                                  and the seeds' initial CCL keys)
+//   labels(seeds) = CCL                           (ccl.cu, list form)
+//   labels = masked Voronoi growth inside seg     (voronoi.cu, frontier form)
+// The label output buffer is the CCL parent store and the Voronoi state, so
+// the only full-size scratch is T (f32), spots/seg (u8), the seed list and
+// the two frontier arrays (which also serve as the blur's temporaries).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace cle {
+
+namespace {
+
+struct Scalars {
+    int status;
+    uint32_t seed_count;
+    float minmax[2];
+    float thr32;
+    float pad;
+    double thr;
+    float hist[256];
+};
+
+__global__ void seeds_kernel(const float *__restrict__ T, const uint8_t *__restrict__ spots,
+                             const float *__restrict__ d_thr32, Geo g, int64_t n,
+                             uint8_t *__restrict__ seg, uint32_t *__restrict__ lab,
+                             uint32_t *__restrict__ seeds, uint32_t *__restrict__ d_count) {
+    const float t = *d_thr32;
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n;
+         base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool s = false, seed = false;
+        uint32_t key = 0;
+        if (i < n) {
+            s = T[i] > t;
+            seed = s && spots[i] != 0;
+            if (seed) {
+                uint32_t x, y, z;
+                m2xyz(g, (uint32_t)i, x, y, z);
+                key = xyz2k(g, x, y, z) + 1u;
+            }
+            seg[i] = s ? 1 : 0;
+            lab[i] = key;
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, seed);
+        if (b) {
+            uint32_t base_pos = 0;
+            const int leader = __ffs(b) - 1;
+            if (lane == leader) base_pos = atomicAdd(d_count, (uint32_t)__popc(b));
+            base_pos = __shfl_sync(0xffffffffu, base_pos, leader);
+            if (seed) seeds[base_pos + __popc(b & ((1u << lane) - 1u))] = (uint32_t)i;
+        }
+    }
+}
+
+__global__ void u32_to_f32(const uint32_t *__restrict__ s, float *__restrict__ d, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = (float)s[i];
+}
+
+struct Layout {
+    Scalars *sc;
+    float *T;
+    uint8_t *spots, *seg;
+    uint32_t *seeds;
+    size_t fixed_end;
+};
+
+Layout take_layout(Arena &a, const Img &im) {
+    Layout l;
+    l.sc = a.take<Scalars>(1);
+    l.T = a.take<float>(im.n());
+    l.spots = a.take<uint8_t>(im.n());
+    l.seg = a.take<uint8_t>(im.n());
+    l.seeds = a.take<uint32_t>(im.n());
+    l.fixed_end = a.off;
+    return l;
+}
+
+}  // namespace
+
+int *workspace_status_ptr(void *ws) { return &reinterpret_cast<Scalars *>(ws)->status; }
+
+size_t vol_workspace_bytes(const Img &im) {
+    Arena a(nullptr, 0);
+    take_layout(a, im);
+    const size_t base = a.off;
+    // phase-dependent tail (max over the phases that use it)
+    size_t tail = 0;
+    tail = std::max(tail, separable_workspace_bytes(im));
+    tail = std::max(tail, minmax_workspace_bytes(im) + histogram_workspace_bytes(im, 256));
+    tail = std::max(tail, rank_workspace_bytes(fkey_bits_for(im.n())));
+    tail = std::max(tail, voronoi_frontier_workspace_bytes(im));
+    return base + tail;
+}
+
+int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, double outline_sigma,
+                          Arena &ws, cudaStream_t st) {
+    CLE_TRY(same_shape(src, dst, "source", "label_image_destination"));
+    if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
+        set_error("voronoi_otsu_labeling: destination must be uint32 or float32 (got %d)", dst.dtype);
+        return CLE_ERR_DTYPE;
+    }
+    Layout l = take_layout(ws, src);
+    const size_t tail_off = ws.off;
+    if (!ws.ok() || (!ws.measuring && ws.cap < vol_workspace_bytes(src))) {
+        set_error("voronoi_otsu_labeling: workspace too small (%zu < %zu)", ws.cap, vol_workspace_bytes(src));
+        return CLE_ERR_WORKSPACE;
+    }
+    const int64_t n = src.n();
+    stage_mark(0, st);
+    CLE_CUDA(cudaMemsetAsync(l.sc, 0, sizeof(Scalars), st));
+
+    // 1-3: blurs and maxima (the blur's temporaries live in the tail)
+    CLE_TRY(gaussian_blur(src, l.T, spot_sigma, spot_sigma, spot_sigma, ws, st));
+    stage_mark(1, st);
+    ws.off = tail_off;
+    Img Ti = src;
+    Ti.data = l.T;
+    Ti.dtype = CLE_F32;
+    Img Si = src;
+    Si.data = l.spots;
+    Si.dtype = CLE_U8;
+    CLE_TRY(detect_maxima(Ti, Si, st));
+    stage_mark(2, st);
+    CLE_TRY(gaussian_blur(src, l.T, outline_sigma, outline_sigma, outline_sigma, ws, st));
+    ws.off = tail_off;
+    stage_mark(3, st);
+
+    // 4-6: threshold on the device
+    CLE_TRY(minmax(Ti, l.sc->minmax, ws, st));
+    CLE_TRY(histogram(Ti, 256, l.sc->minmax, l.sc->hist, ws, st));
+    ws.off = tail_off;
+    CLE_TRY(otsu(l.sc->hist, l.sc->minmax, &l.sc->thr, &l.sc->thr32, st));
+    stage_mark(4, st);
+
+    // 7: segmentation, seeds, seed keys
+    uint32_t *lab = (dst.dtype == CLE_U32) ? (uint32_t *)dst.data : (uint32_t *)l.T;
+    const Geo g = make_geo(src);
+    if (dst.dtype == CLE_F32) {
+        // T is still needed by the seed kernel; use dst as the blurred copy
+        CLE_CUDA(cudaMemcpyAsync(dst.data, l.T, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+        seeds_kernel<<<launch_blocks(n, 256), 256, 0, st>>>((const float *)dst.data, l.spots, &l.sc->thr32, g, n, l.seg, lab, l.seeds, &l.sc->seed_count);
+    } else {
+        seeds_kernel<<<launch_blocks(n, 256), 256, 0, st>>>(l.T, l.spots, &l.sc->thr32, g, n, l.seg, lab, l.seeds, &l.sc->seed_count);
+    }
+    CLE_LAUNCH_CHECK("seeds");
+    stage_mark(5, st);
+
+    // 8: label the seeds
+    CLE_TRY(ccl_list(g, n, lab, l.seeds, &l.sc->seed_count, n, ws, st));
+    ws.off = tail_off;
+    stage_mark(6, st);
+
+    // 9: grow inside the segmentation
+    CLE_TRY(voronoi_frontier(src, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st));
+    ws.off = tail_off;
+    stage_mark(7, st);
+
+    if (dst.dtype == CLE_F32) {
+        u32_to_f32<<<launch_blocks(n, 256), 256, 0, st>>>(lab, (float *)dst.data, n);
+        CLE_LAUNCH_CHECK("labels to f32");
+    }
+    return CLE_OK;
+}
+
+}  // namespace cle
