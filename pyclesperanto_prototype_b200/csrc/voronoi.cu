@@ -33,6 +33,7 @@ constexpr int kVT = 512;
 constexpr int kBuf = 4096;                 // block-local append buffer
 constexpr uint32_t kSkip = 0xFFFFFFFFu;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;   // 4 s per barrier wait
+constexpr uint64_t kKernelLimitNs = 20000000000ull;   // 20 s per launch
 
 struct VorState {
     GridBarrier bar;
@@ -131,9 +132,11 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
     ap.flush(L0, &S->sizes[0]);
     bool ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
 
+    const uint64_t t_start = global_ns();
     uint32_t t = 0;
     bool done = false;
     while (ok && t < max_steps) {
+        if (gtid == 0 && global_ns() - t_start > kKernelLimitNs) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
         uint32_t *F = (t & 1) ? L1 : L0;
         uint32_t *Fn = (t & 1) ? L0 : L1;
         const uint32_t nF = __ldcg(&S->sizes[t & 3]);
@@ -235,7 +238,9 @@ vor_dense_kernel(float *A, float *B, Geo g, int is3d, int64_t n, DenseState *S, 
     const int zr = is3d ? 1 : 0;
     bool ok = true, done = false;
     uint32_t t = 0;
+    const uint64_t t_start = global_ns();
     while (ok && t < max_steps) {
+        if (gtid == 0 && global_ns() - t_start > kKernelLimitNs) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
         const float *cur = (t & 1) ? B : A;
         float *nxt = (t & 1) ? A : B;
         const bool box = (t & 1) == 0;
@@ -325,7 +330,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(VorState), st));
     Geo g = make_geo(im);
     int is3d = im.ndim == 3 ? 1 : 0;
-    uint32_t max_steps = 0x7FFFFFF0u;
+    uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
     const int grid = coop_grid((const void *)voronoi_frontier_kernel, kVT, 0, im.n() / 8 + 1);
     void *args[] = {&lab, (void *)&seg, &g, &is3d, (void *)&seeds, (void *)&d_seed_count, &L0, &L1,
                     &Mv, &S, &d_status, &max_steps};
@@ -378,7 +383,7 @@ int masked_voronoi_dense(const Img &bin, const Img &mask, const Img &dst, int *d
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(DenseState), st));
     Geo g = make_geo(bin);
     int is3d = bin.ndim == 3 ? 1 : 0;
-    uint32_t max_steps = 0x7FFFFFF0u;
+    uint32_t max_steps = (uint32_t)bin.n() + 16u;
     int64_t nn = n;
     const int grid = coop_grid((const void *)vor_dense_kernel, kVT, 0, n);
     void *args[] = {&A, &B, &g, &is3d, &nn, &S, &d_status, &par, &max_steps};
