@@ -220,14 +220,16 @@ def run_b200(args):
 
     # correctness of the loop status once (not timed)
     cle._ops._vol(src, labels, w["spot"], w["outline"], check=True)
+    # clocks are sampled from the start of the warm-up (under load) through
+    # the timed region; short runs add untimed steps until 3 samples exist
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     lib.cle_profile_enable(1)
     stage_buf = (ctypes.c_float * 16)()
     barrier(world)
-    clocks = ClockSampler(local)
-    clocks.start()
     n0 = lib.cle_kernel_launches()
     times, stage_ms = [], []
     for _ in range(args.steps):
@@ -242,6 +244,10 @@ def run_b200(args):
         stage_ms.append([stage_buf[i] for i in range(k)])
     launches = lib.cle_kernel_launches() - n0
     barrier(world)
+    t_pad = time.perf_counter()
+    while len(clocks.lines) < 3 and time.perf_counter() - t_pad < 3.0:
+        step()
+        torch.cuda.synchronize()
     clk = clocks.stop()
     lib.cle_profile_enable(0)
     total_ms = max_over_ranks(sum(times), world)
