@@ -1,0 +1,243 @@
+// blur_fused.cu -- one-launch separable Gaussian blur for isotropic sigma.
+//
+// Same arithmetic as the three-pass path in blur.cu (x pass, then y, then z,
+// float32 intermediates, clamp-to-edge, acc = fma(w_i, v_i, acc) for
+// i = -R..R from 0), fused so the source is read once and the result written
+// once:
+//   * a CTA owns a kTX x kTY output tile in (x, y) and marches along z over a
+//     chunk of planes (plus R halo planes at each end, clamped);
+//   * per input plane it stages the clamped (kTY+2R) x (kTX+2R) tile in
+//     shared memory -- the next plane's values are loaded into registers
+//     while the current one is computed;
+//   * x pass: each thread produces 4 consecutive x outputs from 128-bit
+//     shared loads, for all kTY+2R rows (the y halo);
+//   * y pass: each thread produces kRY consecutive rows of one column from a
+//     register window;
+//   * z pass: a register ring of 2R+1 planes per owned column; the plane loop
+//     is unrolled by 2R+1 so every ring slot is a static register.
+// Radius R (= sigma_to_kernel_size(sigma)/2) is a template parameter; radii
+// above kMaxFusedR or anisotropic sigmas use the three-pass path.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace cle {
+
+namespace {
+
+constexpr int kTX = 32;          // output columns per CTA
+constexpr int kTY = 32;          // output rows per CTA
+constexpr int kRY = 4;           // output rows per thread (y and z passes)
+constexpr int kThreads = kTX * (kTY / kRY);   // 256
+constexpr int kWarps = kThreads / 32;
+
+template <int R>
+struct Geom {
+    static constexpr int ROWS = kTY + 2 * R;                     // staged rows
+    static constexpr int COLS = kTX + 2 * R;                     // staged columns
+    static constexpr int QUADS = (4 + 2 * R + 3) / 4;            // float4 per x-pass thread
+    static constexpr int STRIDE = ((COLS + 3) / 4) * 4 + 4;      // In row stride (floats)
+    static constexpr int ROWS_PER_WARP = (ROWS + kWarps - 1) / kWarps;
+    static constexpr int COL_LOADS = (COLS + 31) / 32;
+    static constexpr int LOADS = ROWS_PER_WARP * COL_LOADS;
+    static constexpr int XO_STRIDE = kTX;                        // Xo row stride
+    static constexpr size_t SMEM = sizeof(float) * (ROWS * STRIDE + ROWS * kTX);
+};
+
+template <typename Tin, int R, bool Z>
+__global__ void __launch_bounds__(kThreads, 1)
+blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, int H, int W,
+                  int zchunk, const __grid_constant__ Taps taps) {
+    using G = Geom<R>;
+    constexpr int WIN = 2 * R + 1;
+    extern __shared__ __align__(16) float smem[];
+    float *In = smem;                          // [ROWS][STRIDE]
+    float *Xo = smem + G::ROWS * G::STRIDE;    // [ROWS][kTX]
+
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * kTX;
+    const int y0 = blockIdx.y * kTY;
+    const int z0 = Z ? (int)blockIdx.z * zchunk : 0;
+    const int z1 = Z ? min(D, z0 + zchunk) : 1;
+    // virtual planes z0-R .. z1-1+R (clamped); 2D: the single plane
+    const int nvirt = Z ? (z1 - z0) + 2 * R : 1;
+    const int zbase = Z ? z0 - R : 0;
+    const int64_t plane = (int64_t)H * W;
+
+    // staging: warp w loads rows w, w+kWarps, ...; lane loads columns
+    // lane, lane+32, ... (clamped to the image)
+    const int lane = tid & 31, warp = tid >> 5;
+    int gx[G::COL_LOADS];
+#pragma unroll
+    for (int c = 0; c < G::COL_LOADS; ++c) gx[c] = clampi(x0 - R + lane + 32 * c, 0, W - 1);
+    float pre[G::LOADS];
+    auto load_plane = [&](int v) {
+        const int zi = Z ? clampi(zbase + v, 0, D - 1) : 0;
+        const Tin *p = src + (int64_t)zi * plane;
+#pragma unroll
+        for (int rr = 0; rr < G::ROWS_PER_WARP; ++rr) {
+            const int r = warp + rr * kWarps;
+            const Tin *row = p + (int64_t)clampi(y0 - R + r, 0, H - 1) * W;
+#pragma unroll
+            for (int c = 0; c < G::COL_LOADS; ++c) {
+                const bool ok = r < G::ROWS && lane + 32 * c < G::COLS;
+                pre[rr * G::COL_LOADS + c] = ok ? to_f32(__ldg(row + gx[c])) : 0.0f;
+            }
+        }
+    };
+    auto store_plane = [&]() {
+#pragma unroll
+        for (int rr = 0; rr < G::ROWS_PER_WARP; ++rr) {
+            const int r = warp + rr * kWarps;
+#pragma unroll
+            for (int c = 0; c < G::COL_LOADS; ++c)
+                if (r < G::ROWS && lane + 32 * c < G::COLS) In[r * G::STRIDE + lane + 32 * c] = pre[rr * G::COL_LOADS + c];
+        }
+    };
+
+    // y/z ownership: column tx, rows ry0 .. ry0+kRY-1
+    const int tx = tid % kTX;
+    const int ry0 = (tid / kTX) * kRY;
+    const bool col_ok = (x0 + tx) < W;
+
+    float ring[kRY][WIN];
+#pragma unroll
+    for (int j = 0; j < kRY; ++j)
+#pragma unroll
+        for (int i = 0; i < WIN; ++i) ring[j][i] = 0.0f;
+
+    load_plane(0);
+    for (int vb = 0; vb < nvirt; vb += WIN) {
+#pragma unroll
+        for (int k = 0; k < WIN; ++k) {
+            const int v = vb + k;
+            if (v < nvirt) {
+                __syncthreads();   // previous plane fully consumed
+                store_plane();
+                if (v + 1 < nvirt) load_plane(v + 1);
+                __syncthreads();
+                // x pass: rows 0..ROWS-1, 4 outputs per item
+                for (int it = tid; it < G::ROWS * (kTX / 4); it += kThreads) {
+                    const int r = it / (kTX / 4);
+                    const int xq = (it - r * (kTX / 4)) * 4;
+                    float in[G::QUADS * 4];
+                    const float4 *rp = reinterpret_cast<const float4 *>(In + r * G::STRIDE + xq);
+#pragma unroll
+                    for (int q = 0; q < G::QUADS; ++q) {
+                        float4 f = rp[q];
+                        in[4 * q] = f.x; in[4 * q + 1] = f.y; in[4 * q + 2] = f.z; in[4 * q + 3] = f.w;
+                    }
+                    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+                    for (int i = 0; i < WIN; ++i) {
+                        const float w = taps.w[i];
+                        a0 = __fmaf_rn(w, in[i], a0);
+                        a1 = __fmaf_rn(w, in[i + 1], a1);
+                        a2 = __fmaf_rn(w, in[i + 2], a2);
+                        a3 = __fmaf_rn(w, in[i + 3], a3);
+                    }
+                    *reinterpret_cast<float4 *>(Xo + r * kTX + xq) = make_float4(a0, a1, a2, a3);
+                }
+                __syncthreads();
+                // y pass: kRY rows of column tx into ring slot k
+                float col[kRY + 2 * R];
+#pragma unroll
+                for (int j = 0; j < kRY + 2 * R; ++j) col[j] = Xo[(ry0 + j) * kTX + tx];
+#pragma unroll
+                for (int j = 0; j < kRY; ++j) {
+                    float a = 0.f;
+#pragma unroll
+                    for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], col[j + i], a);
+                    if constexpr (Z) ring[j][k] = a;
+                    else ring[j][0] = a;
+                }
+                // z pass: output plane z0 + v - 2R once 2R+1 planes are held
+                if constexpr (Z) {
+                    if (v >= 2 * R) {
+                        const int zo = z0 + v - 2 * R;
+#pragma unroll
+                        for (int j = 0; j < kRY; ++j) {
+                            float a = 0.f;
+#pragma unroll
+                            for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], ring[j][(k + 1 + i) % WIN], a);
+                            const int y = y0 + ry0 + j;
+                            if (col_ok && y < H) dst[(int64_t)zo * plane + (int64_t)y * W + x0 + tx] = a;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < kRY; ++j) {
+                        const int y = y0 + ry0 + j;
+                        if (col_ok && y < H) dst[(int64_t)y * W + x0 + tx] = ring[j][0];
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <typename Tin, int R, bool Z>
+int launch_fused_r(const Img &src, float *dst, const Taps &t, cudaStream_t st) {
+    using G = Geom<R>;
+    auto kern = blur_fused_kernel<Tin, R, Z>;
+    static bool attr_set = false;   // per instantiation
+    if (!attr_set) {
+        CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+        attr_set = true;
+    }
+    const int gx = (int)((src.W + kTX - 1) / kTX);
+    const int gy = (int)((src.H + kTY - 1) / kTY);
+    int zchunk = 1, gz = 1;
+    if (Z) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const int64_t target = (int64_t)num_sms(dev) * 2;   // CTAs
+        int64_t chunks = (target + (int64_t)gx * gy - 1) / ((int64_t)gx * gy);
+        // keep the halo overhead (2R planes per chunk) below ~1/2
+        const int64_t max_chunks = std::max<int64_t>(1, src.D / std::max(2 * R, 1));
+        chunks = std::min(chunks, max_chunks);
+        chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, src.D));
+        zchunk = (int)((src.D + chunks - 1) / chunks);
+        gz = (int)((src.D + zchunk - 1) / zchunk);
+    }
+    if (gy > 65535 || gz > 65535) { set_error("gaussian_blur: image too large for the fused path"); return CLE_ERR_TOO_LARGE; }
+    kern<<<dim3(gx, gy, gz), kThreads, G::SMEM, st>>>((const Tin *)src.data, dst, (int)src.D, (int)src.H,
+                                                       (int)src.W, zchunk, t);
+    CLE_LAUNCH_CHECK("gaussian_blur fused");
+    return CLE_OK;
+}
+
+template <typename Tin, bool Z, int R = 1>
+int dispatch_r(const Img &src, float *dst, const Taps &t, int r, cudaStream_t st) {
+    if constexpr (R > kMaxFusedR) {
+        set_error("internal: fused radius out of range");
+        return CLE_ERR_ARG;
+    } else {
+        if (r == R) return launch_fused_r<Tin, R, Z>(src, dst, t, st);
+        return dispatch_r<Tin, Z, R + 1>(src, dst, t, r, st);
+    }
+}
+
+}  // namespace
+
+bool fused_blur_applies(const Img &src, double sx, double sy, double sz) {
+    if (!(sx > 0) || sx != sy) return false;
+    if (src.ndim == 3 && sz != sx) return false;
+    if (src.dtype != CLE_F32 && src.dtype != CLE_U16 && src.dtype != CLE_U8) return false;
+    const int r = (sigma_to_kernel_size(sx) - 1) / 2;
+    return r >= 1 && r <= kMaxFusedR && src.W < (1 << 30) && src.H < (1 << 30);
+}
+
+int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st) {
+    Taps t;
+    CLE_TRY(make_gauss_taps(sigma, t));
+    const int r = (t.n - 1) / 2;
+    const bool z = src.ndim == 3;
+    switch (src.dtype) {
+        case CLE_F32: return z ? dispatch_r<float, true>(src, dst, t, r, st) : dispatch_r<float, false>(src, dst, t, r, st);
+        case CLE_U16: return z ? dispatch_r<uint16_t, true>(src, dst, t, r, st) : dispatch_r<uint16_t, false>(src, dst, t, r, st);
+        case CLE_U8: return z ? dispatch_r<uint8_t, true>(src, dst, t, r, st) : dispatch_r<uint8_t, false>(src, dst, t, r, st);
+        default: set_error("gaussian_blur: unsupported source dtype"); return CLE_ERR_DTYPE;
+    }
+}
+
+}  // namespace cle

@@ -12,6 +12,11 @@ int separable_filter(const Img &src, float *dst, const Taps *tx, const Taps *ty,
 int gaussian_blur(const Img &src, float *dst, double sx, double sy, double sz, Arena &ws,
                   cudaStream_t st);
 
+// blur_fused.cu (isotropic sigma, radius <= kMaxFusedR, one launch)
+constexpr int kMaxFusedR = 14;
+bool fused_blur_applies(const Img &src, double sx, double sy, double sz);
+int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st);
+
 // reduce.cu
 struct MinMaxScratch {
     float *partial;   // 2 * blocks

@@ -114,7 +114,8 @@ constexpr int kHistThreads = 256;
 template <typename T>
 __global__ void __launch_bounds__(kHistThreads)
 hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int bins,
-                 int zchunk, const float *__restrict__ d_minmax, uint32_t *__restrict__ part) {
+                 int zchunk, const float *__restrict__ d_minmax, uint32_t *__restrict__ part,
+                 FastDiv fw) {
     extern __shared__ uint32_t sh[];   // (warps x bins) when private, else bins
     const int nwarps = kHistThreads / 32;
     const bool priv = bins <= 512;
@@ -129,11 +130,22 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
     const int64_t z1 = min(D, z0 + zchunk);
     uint32_t *mine = sh + (priv ? (threadIdx.x >> 5) * bins : 0);
     const unsigned lane = threadIdx.x & 31;
-    for (int64_t z = z0; z < z1; ++z) {
-        const T *row = src + (z * H + y) * W;
-        for (int64_t x0 = 0; x0 < W; x0 += kHistThreads) {
-            int64_t x = x0 + threadIdx.x;
-            int b = (x < W) ? hist_bin(to_f32(row[x]), mn, range, bm1, bins) : -1;
+    // the block's voxels, (z0..z1) x W, visited 4 per thread per round with
+    // all loads issued before the binning
+    const uint32_t span = (uint32_t)((z1 - z0) * W);
+    for (uint32_t base = 0; base < span; base += 4 * kHistThreads) {
+        float v[4];
+        bool ok[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t j = base + k * kHistThreads + threadIdx.x;
+            ok[k] = j < span;
+            const uint32_t zz = fw.div(j), xx = j - zz * (uint32_t)W;
+            v[k] = ok[k] ? to_f32(src[((z0 + zz) * H + y) * W + xx]) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int b = ok[k] ? hist_bin(v[k], mn, range, bm1, bins) : -1;
             // warp-aggregated increment: one shared atomic per distinct bin
             unsigned peers = __match_any_sync(0xffffffffu, b);
             if (b >= 0 && (__ffs(peers) - 1) == (int)lane) atomicAdd(&mine[b], (uint32_t)__popc(peers));
@@ -151,7 +163,15 @@ __global__ void hist_rowsum_kernel(const uint32_t *__restrict__ part, int64_t H,
                                    float *__restrict__ hist) {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bins; b += gridDim.x * blockDim.x) {
         float acc = 0.0f;
-        for (int64_t y = 0; y < H; ++y) acc = __fadd_rn(acc, (float)part[y * bins + b]);
+        int64_t y = 0;
+        for (; y + 8 <= H; y += 8) {   // 8 loads in flight, then the ordered sum
+            uint32_t c[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) c[k] = part[(y + k) * bins + b];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc = __fadd_rn(acc, (float)c[k]);
+        }
+        for (; y < H; ++y) acc = __fadd_rn(acc, (float)part[y * bins + b]);
         hist[b] = acc;
     }
 }
@@ -319,15 +339,15 @@ int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Are
     switch (im.dtype) {
         case CLE_F32:
             if (smem > 48 * 1024) CLE_CUDA(cudaFuncSetAttribute(hist_rows_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            hist_rows_kernel<float><<<grid, kHistThreads, smem, st>>>((const float *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part);
+            hist_rows_kernel<float><<<grid, kHistThreads, smem, st>>>((const float *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W));
             break;
         case CLE_U16:
             if (smem > 48 * 1024) CLE_CUDA(cudaFuncSetAttribute(hist_rows_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            hist_rows_kernel<uint16_t><<<grid, kHistThreads, smem, st>>>((const uint16_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part);
+            hist_rows_kernel<uint16_t><<<grid, kHistThreads, smem, st>>>((const uint16_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W));
             break;
         case CLE_U8:
             if (smem > 48 * 1024) CLE_CUDA(cudaFuncSetAttribute(hist_rows_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            hist_rows_kernel<uint8_t><<<grid, kHistThreads, smem, st>>>((const uint8_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part);
+            hist_rows_kernel<uint8_t><<<grid, kHistThreads, smem, st>>>((const uint8_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W));
             break;
         default: set_error("histogram: unsupported dtype %d", im.dtype); return CLE_ERR_DTYPE;
     }

@@ -149,22 +149,22 @@ __device__ __forceinline__ Seg make_seg(uint32_t l) {
 template <typename TL, typename TI>
 __global__ void __launch_bounds__(kST)
 stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t L, Acc1 a) {
+            int64_t W, int64_t L, Acc1 a, FastDiv fc, FastDiv fh) {
     const int lane = threadIdx.x & 31;
-    const int64_t chunks = (W + 31) / 32;
-    const int64_t tasks = D * H * chunks;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t t = warp; t < tasks; t += nwarps) {
-        const int64_t row = t / chunks;
-        const int64_t c = t - row * chunks;
-        const int64_t x = c * 32 + lane;
+    const uint32_t chunks = (uint32_t)((W + 31) / 32);
+    const uint32_t tasks = (uint32_t)(D * H) * chunks;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = warp; t < tasks; t += nwarps) {
+        const uint32_t row = fc.div(t);
+        const uint32_t c = t - row * chunks;
+        const int64_t x = (int64_t)c * 32 + lane;
         const bool valid = x < W;
-        const int64_t m = row * W + x;
+        const int64_t m = (int64_t)row * W + x;
         uint32_t l = valid ? lab_of(lab[m]) : 0u;
         if (l > (uint32_t)L) l = 0u;
         if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
-        const int64_t z = row / H, y = row - z * H;
+        const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
         const float v = l ? to_f32(inten[m]) : 0.0f;
         const Seg s = make_seg(l);
         const double dv = (double)v;
@@ -247,22 +247,22 @@ __global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T) {
 template <typename TL, typename TI>
 __global__ void __launch_bounds__(kST)
 stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t L, Acc2 b) {
+            int64_t W, int64_t L, Acc2 b, FastDiv fc, FastDiv fh) {
     const int lane = threadIdx.x & 31;
-    const int64_t chunks = (W + 31) / 32;
-    const int64_t tasks = D * H * chunks;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t t = warp; t < tasks; t += nwarps) {
-        const int64_t row = t / chunks;
-        const int64_t c = t - row * chunks;
-        const int64_t x = c * 32 + lane;
+    const uint32_t chunks = (uint32_t)((W + 31) / 32);
+    const uint32_t tasks = (uint32_t)(D * H) * chunks;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = warp; t < tasks; t += nwarps) {
+        const uint32_t row = fc.div(t);
+        const uint32_t c = t - row * chunks;
+        const int64_t x = (int64_t)c * 32 + lane;
         const bool valid = x < W;
-        const int64_t m = row * W + x;
+        const int64_t m = (int64_t)row * W + x;
         uint32_t l = valid ? lab_of(lab[m]) : 0u;
         if (l > (uint32_t)L) l = 0u;
         if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
-        const int64_t z = row / H, y = row - z * H;
+        const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
         double dc = 0.0, dm = 0.0, sq = 0.0;
         if (l) {
             const uint32_t i = l - 1;
@@ -314,14 +314,15 @@ int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc
                 const Acc2 &b, cudaStream_t st) {
     const int64_t tasks = lab.D * lab.H * ((lab.W + 31) / 32);
     const int blocks = launch_blocks(tasks * 32, kST, 8);
+    const FastDiv fc((uint32_t)((lab.W + 31) / 32)), fh((uint32_t)lab.H);
     stage_mark(8, st);
     stats_pass1<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, a);
+                                                lab.H, lab.W, L, a, fc, fh);
     stage_mark(9, st);
     stats_final1<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, T);
     stage_mark(10, st);
     stats_pass2<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, b);
+                                                lab.H, lab.W, L, b, fc, fh);
     stage_mark(11, st);
     stats_final2<<<launch_blocks(L, 256), 256, 0, st>>>(b, L, T);
     stage_mark(12, st);

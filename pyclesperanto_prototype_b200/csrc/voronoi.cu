@@ -30,6 +30,7 @@ namespace cle {
 namespace {
 
 constexpr int kVT = 512;
+constexpr int kFT = 256;                   // frontier kernel block
 constexpr int kBuf = 4096;                 // block-local append buffer
 constexpr uint32_t kSkip = 0xFFFFFFFFu;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;   // 4 s per barrier wait
@@ -71,10 +72,10 @@ struct Appender {
     }
 };
 
-__device__ __forceinline__ void try_mark(uint32_t *lab, uint32_t q, uint32_t step, Appender &ap,
-                                         uint32_t *dst, uint32_t *dst_size) {
+// Claims voxel q (whose label word was read as v) for the frontier of `step`.
+__device__ __forceinline__ void try_mark_from(uint32_t *lab, uint32_t q, uint32_t v, uint32_t step,
+                                              Appender &ap, uint32_t *dst, uint32_t *dst_size) {
     const uint32_t mark = kMarkBit | step;
-    uint32_t v = ld_cg(lab + q);
     for (;;) {
         if (v != 0u && !(v & kMarkBit)) return;   // already labelled
         if (v == mark) return;                     // already queued for this step
@@ -85,6 +86,10 @@ __device__ __forceinline__ void try_mark(uint32_t *lab, uint32_t q, uint32_t ste
         }
         v = old;
     }
+}
+
+__device__ __forceinline__ bool needs_mark(uint32_t v, uint32_t step) {
+    return v == 0u || ((v & kMarkBit) && v != (kMarkBit | step));
 }
 
 __device__ __forceinline__ uint32_t block_sum(uint32_t v) {
@@ -100,7 +105,64 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v) {
     return s;   // valid in thread 0
 }
 
-__global__ void __launch_bounds__(kVT)
+// Clamped neighbour coordinates: reading the clamp-to-edge neighbourhood
+// (the reference's own read semantics) only repeats voxels of the stencil,
+// so no per-neighbour bounds test is needed and every load can be in flight.
+struct Nbr {
+    uint32_t xs[3], ys[3], zs[3];
+};
+
+__device__ __forceinline__ Nbr nbr_of(const Geo &g, uint32_t m, bool is3d) {
+    uint32_t x, y, z;
+    m2xyz(g, m, x, y, z);
+    Nbr n;
+    n.xs[0] = x ? x - 1 : 0; n.xs[1] = x; n.xs[2] = (x + 1 < g.W) ? x + 1 : x;
+    n.ys[0] = y ? y - 1 : 0; n.ys[1] = y; n.ys[2] = (y + 1 < g.H) ? y + 1 : y;
+    if (is3d) {
+        n.zs[0] = z ? z - 1 : 0; n.zs[1] = z; n.zs[2] = (z + 1 < g.D) ? z + 1 : z;
+    } else {
+        n.zs[0] = n.zs[1] = n.zs[2] = z;
+    }
+    return n;
+}
+
+// Maximum label (mark bits read as 0) over the box or the face stencil.
+__device__ __forceinline__ uint32_t stencil_max(const uint32_t *lab, const Geo &g, const Nbr &n,
+                                                bool box) {
+    uint32_t v[27];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) {
+        const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
+        const bool face = (abs(dx - 1) + abs(dy - 1) + abs(dz - 1)) <= 1;
+        v[k] = (box || face) ? ld_cg(lab + xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz])) : 0u;
+    }
+    uint32_t mx = 0;
+#pragma unroll
+    for (int k = 0; k < 27; ++k)
+        if (!(v[k] & kMarkBit)) mx = max(mx, v[k]);
+    return mx;
+}
+
+// Queues the zero mask voxels of the box neighbourhood of p for `step`.
+__device__ __forceinline__ void mark_neighbours(uint32_t *lab, const uint8_t *seg, const Geo &g,
+                                                const Nbr &n, uint32_t step, Appender &ap,
+                                                uint32_t *dst, uint32_t *dst_size) {
+    uint32_t q[27];
+    uint32_t v[27];
+    uint8_t s[27];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) {
+        const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
+        q[k] = xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]);
+        s[k] = seg[q[k]];
+        v[k] = ld_cg(lab + q[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 27; ++k)
+        if (k != 13 && s[k] && needs_mark(v[k], step)) try_mark_from(lab, q[k], v[k], step, ap, dst, dst_size);
+}
+
+__global__ void __launch_bounds__(kFT)
 voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, int is3d,
                         const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *L0,
                         uint32_t *L1, uint32_t *Mv, VorState *S, int *d_status,
@@ -112,22 +174,12 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
     Appender ap{s_buf, &s_cnt};
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t gstride = gridDim.x * blockDim.x;
-    const int zr = is3d ? 1 : 0;
 
     // frontier 0: zero mask voxels in the box neighbourhood of the seeds
     const uint32_t ns = __ldcg(d_seed_count);
     for (uint32_t i = gtid; i < ns; i += gstride) {
-        const uint32_t m = __ldcg(seeds + i);
-        uint32_t x, y, z;
-        m2xyz(g, m, x, y, z);
-        for (int dz = -zr; dz <= zr; ++dz)
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int qx = (int)x + dx, qy = (int)y + dy, qz = (int)z + dz;
-                    if (qx < 0 || qy < 0 || qz < 0 || qx >= (int)g.W || qy >= (int)g.H || qz >= (int)g.D) continue;
-                    const uint32_t q = xyz2m(g, qx, qy, qz);
-                    if (seg[q]) try_mark(lab, q, 0u, ap, L0, &S->sizes[0]);
-                }
+        const Nbr n = nbr_of(g, __ldcg(seeds + i), is3d);
+        mark_neighbours(lab, seg, g, n, 0u, ap, L0, &S->sizes[0]);
     }
     ap.flush(L0, &S->sizes[0]);
     bool ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
@@ -147,18 +199,7 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
             const uint32_t p = __ldcg(F + i);
             const uint32_t v = ld_cg(lab + p);
             if (v != 0u && !(v & kMarkBit)) { Mv[i] = kSkip; continue; }
-            uint32_t x, y, z;
-            m2xyz(g, p, x, y, z);
-            uint32_t mx = 0;
-            for (int dz = -zr; dz <= zr; ++dz)
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        if (!box && (abs(dx) + abs(dy) + abs(dz)) != 1) continue;
-                        const int qx = (int)x + dx, qy = (int)y + dy, qz = (int)z + dz;
-                        if (qx < 0 || qy < 0 || qz < 0 || qx >= (int)g.W || qy >= (int)g.H || qz >= (int)g.D) continue;
-                        const uint32_t w = ld_cg(lab + xyz2m(g, qx, qy, qz));
-                        if (!(w & kMarkBit) && w > mx) mx = w;
-                    }
+            const uint32_t mx = stencil_max(lab, g, nbr_of(g, p, is3d), box);
             Mv[i] = mx;
             changed += (mx != 0u);
         }
@@ -178,20 +219,11 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
             if (mv == kSkip) continue;
             const uint32_t p = __ldcg(F + i);
             if (mv == 0u) {
-                try_mark(lab, p, t + 1, ap, Fn, nsize);
+                try_mark_from(lab, p, ld_cg(lab + p), t + 1, ap, Fn, nsize);
                 continue;
             }
             st_cg(lab + p, mv);
-            uint32_t x, y, z;
-            m2xyz(g, p, x, y, z);
-            for (int dz = -zr; dz <= zr; ++dz)
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        const int qx = (int)x + dx, qy = (int)y + dy, qz = (int)z + dz;
-                        if (qx < 0 || qy < 0 || qz < 0 || qx >= (int)g.W || qy >= (int)g.H || qz >= (int)g.D) continue;
-                        const uint32_t q = xyz2m(g, qx, qy, qz);
-                        if (seg[q]) try_mark(lab, q, t + 1, ap, Fn, nsize);
-                    }
+            mark_neighbours(lab, seg, g, nbr_of(g, p, is3d), t + 1, ap, Fn, nsize);
         }
         ap.flush(Fn, nsize);
         ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
@@ -295,13 +327,14 @@ __global__ void vor_dense_out(const float *__restrict__ A, const float *__restri
     }
 }
 
-int coop_grid(const void *func, int threads, size_t smem, int64_t work) {
+int coop_grid(const void *func, int threads, size_t smem, int64_t work, int max_per_sm = 64) {
     int dev = 0;
     cudaGetDevice(&dev);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
+    if (per_sm > max_per_sm) per_sm = max_per_sm;
     int64_t cap = (int64_t)per_sm * num_sms(dev);
     int64_t want = (work + threads * 4 - 1) / (threads * 4);
     if (want < 1) want = 1;
@@ -331,10 +364,10 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     Geo g = make_geo(im);
     int is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    const int grid = coop_grid((const void *)voronoi_frontier_kernel, kVT, 0, im.n() / 8 + 1);
+    const int grid = coop_grid((const void *)voronoi_frontier_kernel, kFT, 0, im.n() / 16 + 1, 4);
     void *args[] = {&lab, (void *)&seg, &g, &is3d, (void *)&seeds, (void *)&d_seed_count, &L0, &L1,
                     &Mv, &S, &d_status, &max_steps};
-    CLE_CUDA(cudaLaunchCooperativeKernel((const void *)voronoi_frontier_kernel, dim3(grid), dim3(kVT),
+    CLE_CUDA(cudaLaunchCooperativeKernel((const void *)voronoi_frontier_kernel, dim3(grid), dim3(kFT),
                                          args, 0, st));
     count_launches(1);
     return CLE_OK;

@@ -37,6 +37,15 @@ def test_gaussian_blur_bit_exact(cle, oracle, shape, sig):
     assert got.dtype == np.float32 and np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("shape", [(3, 70, 33), (40, 130, 97), (1, 33, 31), (17, 64, 64), (250, 260), (5, 3)])
+@pytest.mark.parametrize("sigma", [0.3, 1.0, 1.7, 2.0, 3.5])
+def test_gaussian_blur_fused_bit_exact(cle, oracle, shape, sigma):
+    # isotropic sigma with radius 1..14 takes the one-launch fused kernel
+    a = rng(21).uniform(0, 5000, size=shape).astype(np.float32)
+    got = cle.pull(cle.gaussian_blur(a, None, sigma, sigma, sigma))
+    assert np.array_equal(got, oracle.gaussian_blur(a, sigma, sigma, sigma))
+
+
 @pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
 def test_gaussian_blur_narrow_input(cle, oracle, dtype):
     a = rng(2).integers(0, np.iinfo(dtype).max, size=(9, 40, 37)).astype(dtype)
