@@ -243,6 +243,10 @@ def run_b200(args):
         k = lib.cle_profile_stage_ms(stage_buf, 16)
         stage_ms.append([stage_buf[i] for i in range(k)])
     launches = lib.cle_kernel_launches() - n0
+    trace = (ctypes.c_uint64 * (3 * 256))()
+    lib.cle_profile_trace(trace, ctypes.sizeof(trace))
+    vor_trace = [(int(trace[3 * i]), int(trace[3 * i + 1]), int(trace[3 * i + 2])) for i in range(256)
+                 if trace[3 * i] or trace[3 * i + 1]]
     barrier(world)
     t_pad = time.perf_counter()
     while len(clocks.lines) < 3 and time.perf_counter() - t_pad < 3.0:
@@ -306,7 +310,7 @@ def run_b200(args):
                           "input_dtype": str(src.dtype)},
                "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                               "p99": round(float(np.percentile(lat, 99)), 4)},
-               "stages_ms": stages, "e2e": e2e, "gpu_launches": int(launches),
+               "stages_ms": stages, "voronoi_trace": vor_trace if args.trace else None, "e2e": e2e, "gpu_launches": int(launches),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -369,6 +373,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="nuclei", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--trace", action="store_true", help="include the Voronoi per-step trace")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

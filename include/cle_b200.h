@@ -83,6 +83,12 @@ unsigned long long cle_kernel_launches(void);
  * finalise 2.  Interval 7 (between the two ops) is host time. */
 int cle_profile_enable(int on);
 int cle_profile_stage_ms(float *out, int max);
+/* Per-step trace of the last device loop (Voronoi growth) while profiling is
+ * enabled: triples of uint64 (ns since the loop started, frontier size,
+ * voxels changed) per step, zero after the last step.  Synchronous; returns
+ * the bytes copied.  Profiling allocates its own trace buffer (outside any
+ * workspace). */
+int cle_profile_trace(void *host, size_t bytes);
 
 /* ---- gaussian_blur -----------------------------------------------------
  * replaces _tier1/_gaussian_blur.py:6-58 (+ _tier1/_execute_separable_kernel.py:7-76,

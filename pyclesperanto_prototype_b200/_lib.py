@@ -61,6 +61,7 @@ _SIGS = {
     "cle_kernel_launches": (ctypes.c_ulonglong, []),
     "cle_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "cle_profile_stage_ms": (ctypes.c_int, [_P, ctypes.c_int]),
+    "cle_profile_trace": (ctypes.c_int, [_P, _SZ]),
     "cle_gaussian_blur_workspace_bytes": (_SZ, [_T]),
     "cle_gaussian_blur": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
     "cle_minimum_maximum_workspace_bytes": (_SZ, [_T]),

@@ -38,6 +38,7 @@ const char *cle_last_error_message(void) { return last_error(); }
 unsigned long long cle_kernel_launches(void) { return launches_issued(); }
 int cle_profile_enable(int on) { return profile_enable(on); }
 int cle_profile_stage_ms(float *out, int max) { return stage_ms(out, max); }
+int cle_profile_trace(void *host, size_t bytes) { return profile_trace_read(host, bytes); }
 
 // ---- gaussian_blur -------------------------------------------------------
 size_t cle_gaussian_blur_workspace_bytes(const cle_tensor *src) {

@@ -29,6 +29,30 @@ static thread_local cudaEvent_t g_ev[kMaxStages];
 static thread_local bool g_prof = false;
 static thread_local int g_marks = 0;
 
+static thread_local void *g_trace = nullptr;
+static thread_local size_t g_trace_bytes = 0;
+
+void *profile_trace_buffer(size_t bytes) {
+    if (!g_prof) return nullptr;
+    if (g_trace_bytes < bytes) {
+        if (g_trace) cudaFree(g_trace);
+        g_trace = nullptr;
+        g_trace_bytes = 0;
+        if (cudaMalloc(&g_trace, bytes) != cudaSuccess) return nullptr;
+        g_trace_bytes = bytes;
+    }
+    cudaMemset(g_trace, 0, g_trace_bytes);
+    return g_trace;
+}
+
+int profile_trace_read(void *host, size_t bytes) {
+    if (!g_trace) return 0;
+    if (bytes > g_trace_bytes) bytes = g_trace_bytes;
+    cudaError_t e = cudaMemcpy(host, g_trace, bytes, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return -cuda_error(e, "trace copy");
+    return (int)bytes;
+}
+
 int profile_enable(int on) {
     if (on && !g_prof) {
         for (int i = 0; i < kMaxStages; ++i) {
@@ -38,6 +62,9 @@ int profile_enable(int on) {
         g_prof = true;
     } else if (!on && g_prof) {
         for (int i = 0; i < kMaxStages; ++i) cudaEventDestroy(g_ev[i]);
+        if (g_trace) cudaFree(g_trace);
+        g_trace = nullptr;
+        g_trace_bytes = 0;
         g_prof = false;
     }
     return CLE_OK;

@@ -24,6 +24,10 @@ unsigned long long launches_issued();
 void stage_mark(int i, cudaStream_t st);
 int stage_ms(float *out, int max);
 int profile_enable(int on);
+// Device buffer for per-step traces of device loops while profiling is
+// enabled (null otherwise); cle_profile_trace() copies it out.
+void *profile_trace_buffer(size_t bytes);
+int profile_trace_read(void *host, size_t bytes);
 int cuda_error(cudaError_t e, const char *where);
 
 #define CLE_CUDA(call)                                                        \

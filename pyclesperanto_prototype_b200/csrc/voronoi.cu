@@ -33,6 +33,7 @@ constexpr int kVT = 512;
 constexpr int kFT = 256;                   // frontier kernel block
 constexpr int kBuf = 4096;                 // block-local append buffer
 constexpr uint32_t kSkip = 0xFFFFFFFFu;
+constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;   // 4 s per barrier wait
 constexpr uint64_t kKernelLimitNs = 20000000000ull;   // 20 s per launch
 
@@ -166,7 +167,7 @@ __global__ void __launch_bounds__(kFT)
 voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, int is3d,
                         const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *L0,
                         uint32_t *L1, uint32_t *Mv, VorState *S, int *d_status,
-                        uint32_t max_steps) {
+                        uint32_t max_steps, unsigned long long *trace) {
     __shared__ uint32_t s_buf[kBuf];
     __shared__ uint32_t s_cnt;
     if (threadIdx.x == 0) s_cnt = 0;
@@ -207,6 +208,11 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
         if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
         ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
         if (!ok) break;
+        if (trace && gtid == 0 && t < kTraceSteps) {
+            trace[3 * t] = global_ns() - t_start;
+            trace[3 * t + 1] = nF;
+            trace[3 * t + 2] = __ldcg(&S->changes[t & 3]);
+        }
         if (__ldcg(&S->changes[t & 3]) == 0u) { done = true; break; }
         // phase B: write, then build the next frontier
         if (gtid == 0) {
@@ -365,8 +371,9 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     int is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
     const int grid = coop_grid((const void *)voronoi_frontier_kernel, kFT, 0, im.n() / 16 + 1, 4);
+    unsigned long long *trace = (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long));
     void *args[] = {&lab, (void *)&seg, &g, &is3d, (void *)&seeds, (void *)&d_seed_count, &L0, &L1,
-                    &Mv, &S, &d_status, &max_steps};
+                    &Mv, &S, &d_status, &max_steps, &trace};
     CLE_CUDA(cudaLaunchCooperativeKernel((const void *)voronoi_frontier_kernel, dim3(grid), dim3(kFT),
                                          args, 0, st));
     count_launches(1);
