@@ -213,9 +213,9 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, int *err, uint64_t lim
             atomicAdd(&b->gen, 1u);
         } else {
             uint64_t t0 = global_ns();
+            uint32_t spins = 0;
             while (*vgen == g) {
-                __nanosleep(64);
-                if (global_ns() - t0 > limit_ns) {
+                if ((++spins & 1023u) == 0u && global_ns() - t0 > limit_ns) {
                     atomicExch(err, (int)CLE_ERR_ITER_LIMIT);
                     break;
                 }

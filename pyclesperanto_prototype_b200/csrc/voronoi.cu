@@ -30,7 +30,7 @@ namespace cle {
 namespace {
 
 constexpr int kVT = 512;
-constexpr int kFT = 256;                   // frontier kernel block
+constexpr int kFT = 512;                   // frontier kernel block (one per SM)
 constexpr int kBuf = 4096;                 // block-local append buffer
 constexpr uint32_t kSkip = 0xFFFFFFFFu;
 constexpr uint32_t kTraceSteps = 256;
@@ -135,7 +135,7 @@ __device__ __forceinline__ uint32_t stencil_max(const uint32_t *lab, const Geo &
     for (int k = 0; k < 27; ++k) {
         const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
         const bool face = (abs(dx - 1) + abs(dy - 1) + abs(dz - 1)) <= 1;
-        v[k] = (box || face) ? ld_cg(lab + xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz])) : 0u;
+        v[k] = (box || face) ? lab[xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz])] : 0u;
     }
     uint32_t mx = 0;
 #pragma unroll
@@ -156,14 +156,17 @@ __device__ __forceinline__ void mark_neighbours(uint32_t *lab, const uint8_t *se
         const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
         q[k] = xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]);
         s[k] = seg[q[k]];
-        v[k] = ld_cg(lab + q[k]);
+        v[k] = lab[q[k]];
     }
 #pragma unroll
     for (int k = 0; k < 27; ++k)
         if (k != 13 && s[k] && needs_mark(v[k], step)) try_mark_from(lab, q[k], v[k], step, ap, dst, dst_size);
 }
 
-__global__ void __launch_bounds__(kFT)
+// Loads of the label buffer go through L1: every phase starts after a grid
+// barrier whose gpu-scope acquire invalidates the SM's L1, and within phase
+// B a stale neighbour value can only be older, which the CAS corrects.
+__global__ void __launch_bounds__(kFT, 1)
 voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, int is3d,
                         const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *L0,
                         uint32_t *L1, uint32_t *Mv, VorState *S, int *d_status,
@@ -197,8 +200,8 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
         // phase A: new values from the current state
         uint32_t changed = 0;
         for (uint32_t i = gtid; i < nF; i += gstride) {
-            const uint32_t p = __ldcg(F + i);
-            const uint32_t v = ld_cg(lab + p);
+            const uint32_t p = F[i];
+            const uint32_t v = lab[p];
             if (v != 0u && !(v & kMarkBit)) { Mv[i] = kSkip; continue; }
             const uint32_t mx = stencil_max(lab, g, nbr_of(g, p, is3d), box);
             Mv[i] = mx;
@@ -223,12 +226,12 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
         for (uint32_t i = gtid; i < nF; i += gstride) {
             const uint32_t mv = Mv[i];
             if (mv == kSkip) continue;
-            const uint32_t p = __ldcg(F + i);
+            const uint32_t p = F[i];
             if (mv == 0u) {
-                try_mark_from(lab, p, ld_cg(lab + p), t + 1, ap, Fn, nsize);
+                try_mark_from(lab, p, lab[p], t + 1, ap, Fn, nsize);
                 continue;
             }
-            st_cg(lab + p, mv);
+            lab[p] = mv;
             mark_neighbours(lab, seg, g, nbr_of(g, p, is3d), t + 1, ap, Fn, nsize);
         }
         ap.flush(Fn, nsize);
@@ -370,7 +373,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     Geo g = make_geo(im);
     int is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    const int grid = coop_grid((const void *)voronoi_frontier_kernel, kFT, 0, im.n() / 16 + 1, 4);
+    const int grid = coop_grid((const void *)voronoi_frontier_kernel, kFT, 0, im.n() / 16 + 1, 1);
     unsigned long long *trace = (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long));
     void *args[] = {&lab, (void *)&seg, &g, &is3d, (void *)&seeds, (void *)&d_seed_count, &L0, &L1,
                     &Mv, &S, &d_status, &max_steps, &trace};
