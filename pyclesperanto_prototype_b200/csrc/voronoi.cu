@@ -30,7 +30,7 @@ namespace cle {
 namespace {
 
 constexpr int kVT = 512;
-constexpr int kFT = 512;                   // frontier kernel block (one per SM)
+constexpr int kFT = 384;                   // frontier kernel block (one per SM)
 constexpr int kBuf = 4096;                 // block-local append buffer
 constexpr uint32_t kSkip = 0xFFFFFFFFu;
 constexpr uint32_t kTraceSteps = 256;
@@ -144,23 +144,52 @@ __device__ __forceinline__ uint32_t stencil_max(const uint32_t *lab, const Geo &
     return mx;
 }
 
+// Predicated compare-and-swap: issued only when `pred`; returns `cmp` when
+// not issued.  Written as one predicated instruction so that a thread's CAS
+// attempts on several neighbours are all in flight together instead of each
+// waiting behind a divergent branch.
+__device__ __forceinline__ uint32_t cas_if(uint32_t *addr, uint32_t cmp, uint32_t val, bool pred) {
+    uint32_t old = cmp;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %4, 0;\n\t"
+        "@p atom.global.cas.b32 %0, [%1], %2, %3;\n\t}"
+        : "+r"(old)
+        : "l"(addr), "r"(cmp), "r"(val), "r"((uint32_t)pred)
+        : "memory");
+    return old;
+}
+
 // Queues the zero mask voxels of the box neighbourhood of p for `step`.
 __device__ __forceinline__ void mark_neighbours(uint32_t *lab, const uint8_t *seg, const Geo &g,
                                                 const Nbr &n, uint32_t step, Appender &ap,
                                                 uint32_t *dst, uint32_t *dst_size) {
-    uint32_t q[27];
+    const uint32_t mark = kMarkBit | step;
     uint32_t v[27];
-    uint8_t s[27];
+    uint32_t segbits = 0;
 #pragma unroll
     for (int k = 0; k < 27; ++k) {
         const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
-        q[k] = xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]);
-        s[k] = seg[q[k]];
-        v[k] = lab[q[k]];
+        const uint32_t q = xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]);
+        segbits |= (seg[q] ? 1u : 0u) << k;
+        v[k] = lab[q];
+    }
+    uint32_t old[27];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) {
+        const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
+        const bool c = k != 13 && ((segbits >> k) & 1u) && needs_mark(v[k], step);
+        old[k] = cas_if(lab + xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]), v[k], mark, c);
     }
 #pragma unroll
-    for (int k = 0; k < 27; ++k)
-        if (k != 13 && s[k] && needs_mark(v[k], step)) try_mark_from(lab, q[k], v[k], step, ap, dst, dst_size);
+    for (int k = 0; k < 27; ++k) {
+        const int dz = k / 9, dy = (k / 3) % 3, dx = k % 3;
+        const bool c = k != 13 && ((segbits >> k) & 1u) && needs_mark(v[k], step);
+        if (!c) continue;
+        const uint32_t q = xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]);
+        if (old[k] == v[k]) ap.push(q, dst, dst_size);                 // claimed
+        else try_mark_from(lab, q, old[k], step, ap, dst, dst_size);   // lost a race: re-check
+    }
 }
 
 // Loads of the label buffer go through L1: every phase starts after a grid
