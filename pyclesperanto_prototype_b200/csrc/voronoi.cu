@@ -31,7 +31,9 @@ namespace {
 
 constexpr int kVT = 512;
 constexpr int kFT = 384;                   // frontier kernel block (one per SM)
-constexpr int kBuf = 4096;                 // block-local append buffer
+constexpr int kBuf = 16384;                // block-local append buffer (entries)
+constexpr int kFlushAt = kBuf - 27 * kFT;  // flush threshold
+constexpr size_t kBufBytes = sizeof(uint32_t) * kBuf;
 constexpr uint32_t kSkip = 0xFFFFFFFFu;
 constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;   // 4 s per barrier wait
@@ -47,29 +49,34 @@ struct VorState {
     uint32_t pad[3];
 };
 
+// Block-local append buffer in shared memory.  Loops that push run with a
+// block-uniform trip count and call maybe_flush() after each round, which
+// moves the buffer to the global list (one atomicAdd per flush) once it is
+// past kFlushAt; a round pushes at most 27 entries per thread, so the buffer
+// never overflows.
 struct Appender {
-    uint32_t *buf;      // shared
+    uint32_t *buf;      // shared, kBuf entries
     uint32_t *cnt;      // shared
-    __device__ __forceinline__ void push(uint32_t v, uint32_t *dst, uint32_t *dst_size) {
-        uint32_t pos = atomicAdd(cnt, 1u);
-        if (pos < (uint32_t)kBuf) {
-            buf[pos] = v;
-        } else {
-            uint32_t g = atomicAdd(dst_size, 1u);
-            __stcg(dst + g, v);
-        }
+    __device__ __forceinline__ void push(uint32_t v) {
+        const uint32_t pos = atomicAdd(cnt, 1u);
+        buf[pos] = v;
     }
     // All threads of the block must call.
     __device__ __forceinline__ void flush(uint32_t *dst, uint32_t *dst_size) {
         __shared__ uint32_t base;
         __syncthreads();
-        const uint32_t n = min(*cnt, (uint32_t)kBuf);
+        const uint32_t n = *cnt;
         if (threadIdx.x == 0) base = n ? atomicAdd(dst_size, n) : 0u;
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) __stcg(dst + base + i, buf[i]);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[base + i] = buf[i];
         __syncthreads();
         if (threadIdx.x == 0) *cnt = 0;
         __syncthreads();
+    }
+    // All threads of the block must call (after a round of pushes).
+    __device__ __forceinline__ void maybe_flush(uint32_t *dst, uint32_t *dst_size) {
+        __syncthreads();
+        if (*cnt >= (uint32_t)kFlushAt) flush(dst, dst_size);
     }
 };
 
@@ -82,7 +89,7 @@ __device__ __forceinline__ void try_mark_from(uint32_t *lab, uint32_t q, uint32_
         if (v == mark) return;                     // already queued for this step
         uint32_t old = atomicCAS(lab + q, v, mark);
         if (old == v) {
-            ap.push(q, dst, dst_size);
+            ap.push(q);
             return;
         }
         v = old;
@@ -187,7 +194,7 @@ __device__ __forceinline__ void mark_neighbours(uint32_t *lab, const uint8_t *se
         const bool c = k != 13 && ((segbits >> k) & 1u) && needs_mark(v[k], step);
         if (!c) continue;
         const uint32_t q = xyz2m(g, n.xs[dx], n.ys[dy], n.zs[dz]);
-        if (old[k] == v[k]) ap.push(q, dst, dst_size);                 // claimed
+        if (old[k] == v[k]) ap.push(q);                                // claimed
         else try_mark_from(lab, q, old[k], step, ap, dst, dst_size);   // lost a race: re-check
     }
 }
@@ -200,7 +207,7 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
                         const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *L0,
                         uint32_t *L1, uint32_t *Mv, VorState *S, int *d_status,
                         uint32_t max_steps, unsigned long long *trace) {
-    __shared__ uint32_t s_buf[kBuf];
+    extern __shared__ uint32_t s_buf[];   // kBuf entries
     __shared__ uint32_t s_cnt;
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
@@ -210,9 +217,10 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
 
     // frontier 0: zero mask voxels in the box neighbourhood of the seeds
     const uint32_t ns = __ldcg(d_seed_count);
-    for (uint32_t i = gtid; i < ns; i += gstride) {
-        const Nbr n = nbr_of(g, __ldcg(seeds + i), is3d);
-        mark_neighbours(lab, seg, g, n, 0u, ap, L0, &S->sizes[0]);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < ns; base += gstride) {
+        const uint32_t i = base + threadIdx.x;
+        if (i < ns) mark_neighbours(lab, seg, g, nbr_of(g, __ldcg(seeds + i), is3d), 0u, ap, L0, &S->sizes[0]);
+        ap.maybe_flush(L0, &S->sizes[0]);
     }
     ap.flush(L0, &S->sizes[0]);
     bool ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
@@ -252,16 +260,19 @@ voronoi_frontier_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, Geo g, i
             S->sizes[(t + 2) & 3] = 0u;
         }
         uint32_t *nsize = &S->sizes[(t + 1) & 3];
-        for (uint32_t i = gtid; i < nF; i += gstride) {
-            const uint32_t mv = Mv[i];
-            if (mv == kSkip) continue;
-            const uint32_t p = F[i];
-            if (mv == 0u) {
-                try_mark_from(lab, p, lab[p], t + 1, ap, Fn, nsize);
-                continue;
+        for (uint32_t base = blockIdx.x * blockDim.x; base < nF; base += gstride) {
+            const uint32_t i = base + threadIdx.x;
+            const uint32_t mv = (i < nF) ? Mv[i] : kSkip;
+            if (mv != kSkip) {
+                const uint32_t p = F[i];
+                if (mv == 0u) {
+                    try_mark_from(lab, p, lab[p], t + 1, ap, Fn, nsize);
+                } else {
+                    lab[p] = mv;
+                    mark_neighbours(lab, seg, g, nbr_of(g, p, is3d), t + 1, ap, Fn, nsize);
+                }
             }
-            lab[p] = mv;
-            mark_neighbours(lab, seg, g, nbr_of(g, p, is3d), t + 1, ap, Fn, nsize);
+            ap.maybe_flush(Fn, nsize);
         }
         ap.flush(Fn, nsize);
         ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
@@ -402,12 +413,18 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     Geo g = make_geo(im);
     int is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    const int grid = coop_grid((const void *)voronoi_frontier_kernel, kFT, 0, im.n() / 16 + 1, 1);
+    static bool attr = false;
+    if (!attr) {
+        CLE_CUDA(cudaFuncSetAttribute((const void *)voronoi_frontier_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBufBytes));
+        attr = true;
+    }
+    const int grid = coop_grid((const void *)voronoi_frontier_kernel, kFT, kBufBytes, im.n() / 16 + 1, 1);
     unsigned long long *trace = (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long));
     void *args[] = {&lab, (void *)&seg, &g, &is3d, (void *)&seeds, (void *)&d_seed_count, &L0, &L1,
                     &Mv, &S, &d_status, &max_steps, &trace};
     CLE_CUDA(cudaLaunchCooperativeKernel((const void *)voronoi_frontier_kernel, dim3(grid), dim3(kFT),
-                                         args, 0, st));
+                                         args, kBufBytes, st));
     count_launches(1);
     return CLE_OK;
 }
