@@ -171,6 +171,17 @@ int cle_masked_voronoi_labeling(const cle_tensor *binary, const cle_tensor *mask
                                 const cle_tensor *dst, void *workspace, size_t workspace_bytes,
                                 void *stream);
 
+/* Fast form of masked_voronoi_labeling for the case voronoi_otsu_labeling
+ * produces: mask values in {0, 1} and every seed inside the mask (then the
+ * reference's -1/0/label state reduces to labels in the mask).  Growth visits
+ * only the active part of the front (row bricks).  For other masks or seeds
+ * outside the mask use cle_masked_voronoi_labeling.  The status word of the
+ * workspace (cle_workspace_status) reports the loop outcome. */
+size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *binary);
+int cle_masked_voronoi_labeling_binary(const cle_tensor *binary, const cle_tensor *mask,
+                                       const cle_tensor *dst, void *workspace,
+                                       size_t workspace_bytes, void *stream);
+
 /* ---- voronoi_otsu_labeling ---------------------------------------------
  * replaces _tier9/_voronoi_otsu_labeling.py:11-73.  src: u8/u16/f32 (u8 and
  * u16 are converted on the fly, exactly as push's float32 cast would);

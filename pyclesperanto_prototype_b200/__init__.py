@@ -15,6 +15,7 @@ from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, cr
                      plugin_function, pull, pull_zyx, push, push_native, push_zyx)
 from ._ops import (binary_and, connected_components_labeling_box, detect_maxima_box,
                    gaussian_blur, greater_constant, histogram, mask, masked_voronoi_labeling,
+                   masked_voronoi_labeling_binary,
                    maximum_of_all_pixels, minimum_of_all_pixels, radius_to_kernel_size,
                    relabel_sequential, scikit_image_threshold_otsu, sigma_to_kernel_size,
                    statistics_of_labeled_pixels, statistics_of_labelled_pixels, statistics_table,

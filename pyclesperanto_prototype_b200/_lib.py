@@ -81,6 +81,8 @@ _SIGS = {
     "cle_relabel_sequential": (ctypes.c_int, [_T, _T, ctypes.c_uint32, _P, _SZ, _P]),
     "cle_masked_voronoi_labeling_workspace_bytes": (_SZ, [_T]),
     "cle_masked_voronoi_labeling": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
+    "cle_masked_voronoi_labeling_binary_workspace_bytes": (_SZ, [_T]),
+    "cle_masked_voronoi_labeling_binary": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
     "cle_voronoi_otsu_labeling_workspace_bytes": (_SZ, [_T]),
     "cle_voronoi_otsu_labeling": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
     "cle_workspace_status": (ctypes.c_int, [_P, _SZ, _P]),

@@ -264,6 +264,25 @@ int cle_masked_voronoi_labeling(const cle_tensor *bin, const cle_tensor *msk, co
     return masked_voronoi_dense(a, m, d, status, ar, S(stream));
 }
 
+size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *bin) {
+    Img im;
+    if (to_img(bin, im, "binary_source")) return 0;
+    return masked_voronoi_binary_workspace_bytes(im);
+}
+
+int cle_masked_voronoi_labeling_binary(const cle_tensor *bin, const cle_tensor *msk,
+                                       const cle_tensor *dst, void *ws, size_t ws_bytes,
+                                       void *stream) {
+    Img a, m, d;
+    CLE_TRY(to_img(bin, a, "binary_source"));
+    CLE_TRY(to_img(msk, m, "mask_image"));
+    CLE_TRY(to_img(dst, d, "labeling_destination"));
+    CLE_TRY(ws_check(ws, ws_bytes, masked_voronoi_binary_workspace_bytes(a), "masked_voronoi_labeling"));
+    CLE_TRY(set_device_of(a, bin));
+    Arena ar(ws, ws_bytes);
+    return masked_voronoi_binary(a, m, d, ar, S(stream));
+}
+
 // ---- voronoi_otsu_labeling ----------------------------------------------------------
 size_t cle_voronoi_otsu_labeling_workspace_bytes(const cle_tensor *src) {
     Img im;

@@ -79,6 +79,11 @@ size_t vol_workspace_bytes(const Img &im);
 int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma,
                           double outline_sigma, Arena &ws, cudaStream_t st);
 
+// masked_voronoi_labeling for a 0/1 mask with every seed inside it (the
+// composite's case), on the active-brick growth.
+size_t masked_voronoi_binary_workspace_bytes(const Img &im);
+int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st);
+
 // Status word at a fixed offset of every composite workspace (first 256 B).
 int *workspace_status_ptr(void *ws);
 

@@ -61,6 +61,40 @@ __global__ void seeds_kernel(const float *__restrict__ T, const uint8_t *__restr
     }
 }
 
+// Seeds of masked_voronoi_labeling with a 0/1 mask: seg = mask != 0,
+// seed = binary != 0 inside the mask; seeds get their CCL key and are listed.
+template <typename Tb, typename Tm>
+__global__ void mask_seeds_kernel(const Tb *__restrict__ bin, const Tm *__restrict__ mask, Geo g,
+                                  int64_t n, uint8_t *__restrict__ seg, uint32_t *__restrict__ lab,
+                                  uint32_t *__restrict__ seeds, uint32_t *__restrict__ d_count) {
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n;
+         base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        bool seed = false;
+        if (i < n) {
+            const bool s = mask[i] != (Tm)0;
+            seed = s && bin[i] != (Tb)0;
+            uint32_t key = 0;
+            if (seed) {
+                uint32_t x, y, z;
+                m2xyz(g, (uint32_t)i, x, y, z);
+                key = xyz2k(g, x, y, z) + 1u;
+            }
+            seg[i] = s ? 1 : 0;
+            lab[i] = key;
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, seed);
+        if (b) {
+            uint32_t base_pos = 0;
+            const int leader = __ffs(b) - 1;
+            if (lane == leader) base_pos = atomicAdd(d_count, (uint32_t)__popc(b));
+            base_pos = __shfl_sync(0xffffffffu, base_pos, leader);
+            if (seed) seeds[base_pos + __popc(b & ((1u << lane) - 1u))] = (uint32_t)i;
+        }
+    }
+}
+
 __global__ void u32_to_f32(const uint32_t *__restrict__ s, float *__restrict__ d, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
@@ -86,7 +120,77 @@ Layout take_layout(Arena &a, const Img &im) {
     return l;
 }
 
+struct BinLayout {
+    Scalars *sc;
+    uint8_t *seg;
+    uint32_t *seeds;
+    uint32_t *lab;   // used when the destination is float32
+};
+
+BinLayout take_bin_layout(Arena &a, const Img &im) {
+    BinLayout l;
+    l.sc = a.take<Scalars>(1);
+    l.seg = a.take<uint8_t>(im.n());
+    l.seeds = a.take<uint32_t>(im.n());
+    l.lab = a.take<uint32_t>(im.n());
+    return l;
+}
+
+template <typename Tb>
+int launch_mask_seeds(const Img &bin, const Img &mask, const Geo &g, const BinLayout &l,
+                      uint32_t *lab, cudaStream_t st) {
+    const int64_t n = bin.n();
+    const int b = launch_blocks(n, 256);
+    switch (mask.dtype) {
+        case CLE_U8: mask_seeds_kernel<Tb, uint8_t><<<b, 256, 0, st>>>((const Tb *)bin.data, (const uint8_t *)mask.data, g, n, l.seg, lab, l.seeds, &l.sc->seed_count); break;
+        case CLE_F32: mask_seeds_kernel<Tb, float><<<b, 256, 0, st>>>((const Tb *)bin.data, (const float *)mask.data, g, n, l.seg, lab, l.seeds, &l.sc->seed_count); break;
+        case CLE_U32: mask_seeds_kernel<Tb, uint32_t><<<b, 256, 0, st>>>((const Tb *)bin.data, (const uint32_t *)mask.data, g, n, l.seg, lab, l.seeds, &l.sc->seed_count); break;
+        default: set_error("masked_voronoi_labeling: unsupported mask dtype %d", mask.dtype); return CLE_ERR_DTYPE;
+    }
+    CLE_LAUNCH_CHECK("mask seeds");
+    return CLE_OK;
+}
+
 }  // namespace
+
+size_t masked_voronoi_binary_workspace_bytes(const Img &im) {
+    Arena a(nullptr, 0);
+    take_bin_layout(a, im);
+    size_t tail = std::max(rank_workspace_bytes(fkey_bits_for(im.n())), voronoi_frontier_workspace_bytes(im));
+    return a.off + tail;
+}
+
+int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st) {
+    CLE_TRY(same_shape(bin, mask, "binary_source", "mask_image"));
+    CLE_TRY(same_shape(bin, dst, "binary_source", "labeling_destination"));
+    if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
+        set_error("masked_voronoi_labeling: destination must be uint32 or float32");
+        return CLE_ERR_DTYPE;
+    }
+    BinLayout l = take_bin_layout(ws, bin);
+    const size_t tail_off = ws.off;
+    if (!ws.measuring && ws.cap < masked_voronoi_binary_workspace_bytes(bin)) {
+        set_error("masked_voronoi_labeling: workspace too small");
+        return CLE_ERR_WORKSPACE;
+    }
+    CLE_CUDA(cudaMemsetAsync(l.sc, 0, sizeof(Scalars), st));
+    uint32_t *lab = dst.dtype == CLE_U32 ? (uint32_t *)dst.data : l.lab;
+    const Geo g = make_geo(bin);
+    switch (bin.dtype) {
+        case CLE_U8: CLE_TRY(launch_mask_seeds<uint8_t>(bin, mask, g, l, lab, st)); break;
+        case CLE_F32: CLE_TRY(launch_mask_seeds<float>(bin, mask, g, l, lab, st)); break;
+        case CLE_U32: CLE_TRY(launch_mask_seeds<uint32_t>(bin, mask, g, l, lab, st)); break;
+        default: set_error("masked_voronoi_labeling: unsupported binary dtype %d", bin.dtype); return CLE_ERR_DTYPE;
+    }
+    CLE_TRY(ccl_list(g, bin.n(), lab, l.seeds, &l.sc->seed_count, bin.n(), ws, st));
+    ws.off = tail_off;
+    CLE_TRY(voronoi_frontier(bin, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st));
+    if (dst.dtype == CLE_F32) {
+        u32_to_f32<<<launch_blocks(dst.n(), 256), 256, 0, st>>>(lab, (float *)dst.data, dst.n());
+        CLE_LAUNCH_CHECK("labels to f32");
+    }
+    return CLE_OK;
+}
 
 int *workspace_status_ptr(void *ws) { return &reinterpret_cast<Scalars *>(ws)->status; }
 

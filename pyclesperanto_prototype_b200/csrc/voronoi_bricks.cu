@@ -1,0 +1,316 @@
+// voronoi_bricks.cu -- the masked Voronoi growth of voronoi_otsu_labeling
+// (_tier5/_masked_voronoi_labeling.py:44-76, with a 0/1 mask and seeds inside it).
+//
+// The reference's Jacobi steps (box stencil on even steps, face stencil on odd
+// steps, a voxel rewritten only while 0 with the maximum over the stencil
+// including itself, stop at the first step that changes nothing) run on
+// "row bricks": 32 consecutive x voxels of one (z, y) row, one warp each.
+// Only active bricks are visited -- those that may hold a voxel able to change
+// in this step -- so the work per step follows the growth front, and a warp's
+// neighbour reads are 9 coalesced row segments (x +- 1 by warp shuffles).
+//
+// A step is two phases separated by grid barriers:
+//   A  every active brick computes its candidates' new values from the state
+//      of the previous step (candidates: mask voxels still 0);
+//   B  new labels are written, and the bricks of the next step are queued:
+//      the 3x3x3 brick neighbourhood of every brick that changed, plus any
+//      brick with a voxel that the face stencil could not reach but the box
+//      stencil will (it changes at the next step).
+// Queueing deduplicates with an atomicMax on a per-brick step tag, so the
+// label buffer holds labels only.  Every voxel that can change at a step lies
+// in a queued brick (a voxel whose labelled neighbour is older was already
+// visited and either changed or was re-queued), so the result equals the
+// reference's dense iteration.  Once few bricks remain active, one CTA
+// finishes the remaining steps with block barriers instead of grid barriers.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace cle {
+
+namespace {
+
+constexpr int kBT = 1024;                       // threads per CTA (one CTA per SM)
+constexpr int kWPB = kBT / 32;                  // warps per CTA
+constexpr int kBBuf = 8192;                     // CTA append buffer (entries)
+constexpr int kBFlushAt = kBBuf - 27 * kWPB;    // a round queues <= 27 bricks per warp
+constexpr size_t kBBufBytes = sizeof(uint32_t) * kBBuf;
+constexpr uint32_t kTailBricks = 1024;          // single-CTA finish at or below this
+constexpr uint32_t kPend = 0x80000000u;         // Mv: face stencil missed, box will hit
+constexpr uint32_t kTraceSteps = 256;
+constexpr uint64_t kBarrierLimitNs = 4000000000ull;
+constexpr uint64_t kKernelLimitNs = 20000000000ull;
+
+struct BState {
+    GridBarrier bar;
+    int err;
+    int done;
+    uint32_t sizes[4];
+    uint32_t changes[4];
+    uint32_t steps;
+    uint32_t pad[3];
+};
+
+struct BGeo {
+    Geo g;
+    uint32_t WB;        // bricks per row
+    FastDiv fWB;
+    int is3d;
+};
+
+struct BAppender {
+    uint32_t *buf;
+    uint32_t *cnt;
+    __device__ __forceinline__ void push(uint32_t v) { buf[atomicAdd(cnt, 1u)] = v; }
+    __device__ __forceinline__ void flush(uint32_t *dst, uint32_t *dst_size) {
+        __shared__ uint32_t base;
+        __syncthreads();
+        const uint32_t n = *cnt;
+        if (threadIdx.x == 0) base = n ? atomicAdd(dst_size, n) : 0u;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[base + i] = buf[i];
+        __syncthreads();
+        if (threadIdx.x == 0) *cnt = 0;
+        __syncthreads();
+    }
+    __device__ __forceinline__ void maybe_flush(uint32_t *dst, uint32_t *dst_size) {
+        __syncthreads();
+        if (*cnt >= (uint32_t)kBFlushAt) flush(dst, dst_size);
+    }
+};
+
+__device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t s = 0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < kWPB; ++i) s += red[i];
+    return s;   // thread 0
+}
+
+// Queues bricks (z+dz, y+dy, xb+dxb) for the step tagged `tag`; lane k of the
+// warp handles offset k of the 3x3x3 neighbourhood when want(k).
+__device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint32_t y, uint32_t xb,
+                                                 bool want, uint32_t tag, uint32_t *bstep,
+                                                 BAppender &ap) {
+    const int lane = threadIdx.x & 31;
+    if (!want || lane >= 27) return;
+    const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+    const int zz = (int)z + dz, yy = (int)y + dy, xx = (int)xb + dxb;
+    if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)G.g.D || yy >= (int)G.g.H || xx >= (int)G.WB) return;
+    const uint32_t nb = ((uint32_t)zz * G.g.H + (uint32_t)yy) * G.WB + (uint32_t)xx;
+    if (atomicMax(bstep + nb, tag) < tag) ap.push(nb);
+}
+
+__global__ void __launch_bounds__(kBT, 1)
+voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
+                      const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
+                      uint32_t *B1, uint32_t *Mv, uint32_t *bstep, BState *S, int *d_status,
+                      uint32_t max_steps, unsigned long long *trace) {
+    extern __shared__ uint32_t s_buf[];
+    __shared__ uint32_t s_cnt;
+    __shared__ uint32_t s_red[kWPB];
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    BAppender ap{s_buf, &s_cnt};
+    const Geo &g = G.g;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gstride = gridDim.x * blockDim.x;
+
+    // step 0's bricks: the brick neighbourhoods of the seeds (tag 1)
+    const uint32_t ns = __ldcg(d_seed_count);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < ns; base += gstride) {
+        const uint32_t i = base + threadIdx.x;
+        if (i < ns) {
+            uint32_t x, y, z;
+            m2xyz(g, __ldcg(seeds + i), x, y, z);
+            const uint32_t xb = x >> 5;
+            for (int k = 0; k < 27; ++k) {
+                const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dxb = k % 3 - 1;
+                if (!G.is3d && dz) continue;
+                const int zz = (int)z + dz, yy = (int)y + dy, xx = (int)xb + dxb;
+                if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)g.D || yy >= (int)g.H || xx >= (int)G.WB) continue;
+                const uint32_t nb = ((uint32_t)zz * g.H + (uint32_t)yy) * G.WB + (uint32_t)xx;
+                if (atomicMax(bstep + nb, 1u) < 1u) ap.push(nb);
+            }
+        }
+        ap.maybe_flush(B0, &S->sizes[0]);
+    }
+    ap.flush(B0, &S->sizes[0]);
+    bool ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
+
+    const uint64_t t_start = global_ns();
+    uint32_t t = 0;
+    bool done = false, tail = false;
+    const int zr = G.is3d ? 1 : 0;
+    while (ok && t < max_steps) {
+        if (gtid == 0 && global_ns() - t_start > kKernelLimitNs) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
+        const uint32_t *F = (t & 1) ? B1 : B0;
+        uint32_t *Fn = (t & 1) ? B0 : B1;
+        const uint32_t nB = __ldcg(&S->sizes[t & 3]);
+        if (!tail && nB <= kTailBricks) {
+            tail = true;                      // uniform: nB was read after a barrier
+            if (blockIdx.x != 0) break;       // CTA 0 finishes alone
+        }
+        const uint32_t wstride = tail ? kWPB : gridDim.x * kWPB;
+        const uint32_t wbase = tail ? 0 : blockIdx.x * kWPB;
+        const bool box = (t & 1) == 0;
+        // ---- phase A ---------------------------------------------------
+        uint32_t changed = 0;
+        for (uint32_t base = wbase; base < nB; base += wstride) {
+            const uint32_t idx = base + warp;
+            if (idx >= nB) continue;
+            const uint32_t b = __ldcg(F + idx);
+            const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
+            const uint32_t z = g.fH.div(r), y = r - z * g.H;
+            const int x = (int)(xb * 32u) + lane;
+            const int xc = min(x, (int)g.W - 1);
+            const uint32_t p = r * g.W + (uint32_t)xc;
+            const bool cand = x < (int)g.W && seg[p] != 0 && ld_cg(lab + p) == 0u;
+            uint32_t out = 0;
+            if (__any_sync(0xffffffffu, cand)) {
+                uint32_t bm = 0, dm = 0;
+                for (int dz = -zr; dz <= zr; ++dz)
+#pragma unroll
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
+                        const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
+                        const uint32_t *row = lab + (zz * g.H + yy) * g.W;
+                        const uint32_t c = ld_cg(row + xc);
+                        uint32_t lft = __shfl_up_sync(0xffffffffu, c, 1);
+                        uint32_t rgt = __shfl_down_sync(0xffffffffu, c, 1);
+                        if (lane == 0) lft = ld_cg(row + max(x - 1, 0));
+                        if (lane == 31) rgt = ld_cg(row + min(x + 1, (int)g.W - 1));
+                        bm = max(bm, max(c, max(lft, rgt)));
+                        if (dz == 0 && dy == 0) dm = max(dm, max(lft, rgt));
+                        else if (dz == 0 || dy == 0) dm = max(dm, c);
+                    }
+                if (cand) {
+                    const uint32_t m = box ? bm : dm;
+                    out = m ? m : ((bm != 0u) ? kPend : 0u);
+                    changed += (m != 0u);
+                }
+            }
+            Mv[(size_t)idx * 32 + lane] = out;
+        }
+        if (!tail) {
+            const uint32_t bs = block_total(changed, s_red);
+            if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
+            ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
+        } else {
+            const uint32_t bs = block_total(changed, s_red);
+            if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
+            __syncthreads();
+        }
+        if (!ok) break;
+        const uint32_t nchanged = __ldcg(&S->changes[t & 3]);
+        if (trace && gtid == 0 && t < kTraceSteps) {
+            trace[3 * t] = global_ns() - t_start;
+            trace[3 * t + 1] = nB;
+            trace[3 * t + 2] = nchanged;
+        }
+        if (nchanged == 0u) { done = true; break; }
+        // ---- phase B ---------------------------------------------------
+        if (gtid == 0) {
+            S->changes[(t + 2) & 3] = 0u;
+            S->sizes[(t + 2) & 3] = 0u;
+        }
+        uint32_t *nsize = &S->sizes[(t + 1) & 3];
+        const uint32_t tag = t + 2;
+        for (uint32_t base = wbase; base < nB; base += wstride) {
+            const uint32_t idx = base + warp;
+            if (idx < nB) {
+                const uint32_t b = __ldcg(F + idx);
+                const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
+                const uint32_t z = g.fH.div(r), y = r - z * g.H;
+                const uint32_t mv = Mv[(size_t)idx * 32 + lane];
+                const uint32_t m = (mv & kPend) ? 0u : mv;
+                if (m) st_cg(lab + r * g.W + xb * 32u + (uint32_t)lane, m);
+                const unsigned ch = __ballot_sync(0xffffffffu, m != 0u);
+                const bool pend = __any_sync(0xffffffffu, mv == kPend);
+                bool want = false;
+                if (lane < 27) {
+                    const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+                    if (G.is3d || dz == 0) {
+                        if (ch) want = dxb == 0 || (dxb < 0 && (ch & 1u)) || (dxb > 0 && (ch >> 31));
+                        if (pend && dz == 0 && dy == 0 && dxb == 0) want = true;
+                    }
+                }
+                queue_neighbours(G, z, y, xb, want, tag, bstep, ap);
+            }
+            ap.maybe_flush(Fn, nsize);
+        }
+        ap.flush(Fn, nsize);
+        if (!tail) ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
+        else __syncthreads();
+        ++t;
+    }
+    if (gtid == 0) {
+        S->steps = t + 1;
+        S->done = done ? 1 : 0;
+        const int e = *(volatile int *)&S->err;
+        *d_status = done ? CLE_OK : (e ? e : (int)CLE_ERR_ITER_LIMIT);
+    }
+}
+
+uint32_t bricks_per_row(const Img &im) { return (uint32_t)((im.W + 31) / 32); }
+uint32_t brick_count(const Img &im) { return (uint32_t)(im.D * im.H) * bricks_per_row(im); }
+
+}  // namespace
+
+size_t voronoi_frontier_workspace_bytes(const Img &im) {
+    const size_t nb = brick_count(im);
+    Arena a(nullptr, 0);
+    a.take<BState>(1);
+    a.take<uint32_t>(nb);        // list 0
+    a.take<uint32_t>(nb);        // list 1
+    a.take<uint32_t>(nb);        // per-brick step tags
+    a.take<uint32_t>(nb * 32);   // per-voxel phase-A results
+    return a.off;
+}
+
+int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uint32_t *seeds,
+                     const uint32_t *d_seed_count, int *d_status, Arena &ws, cudaStream_t st) {
+    const size_t nb = brick_count(im);
+    BState *S = ws.take<BState>(1);
+    uint32_t *B0 = ws.take<uint32_t>(nb);
+    uint32_t *B1 = ws.take<uint32_t>(nb);
+    uint32_t *bstep = ws.take<uint32_t>(nb);
+    uint32_t *Mv = ws.take<uint32_t>(nb * 32);
+    if (!ws.ok()) { set_error("masked_voronoi_labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
+    CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(BState), st));
+    CLE_CUDA(cudaMemsetAsync(bstep, 0, sizeof(uint32_t) * nb, st));
+    BGeo G;
+    G.g = make_geo(im);
+    G.WB = bricks_per_row(im);
+    G.fWB = FastDiv(G.WB);
+    G.is3d = im.ndim == 3 ? 1 : 0;
+    uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
+    static bool attr = false;
+    if (!attr) {
+        CLE_CUDA(cudaFuncSetAttribute((const void *)voronoi_bricks_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
+        attr = true;
+    }
+    int dev = 0;
+    CLE_CUDA(cudaGetDevice(&dev));
+    int per_sm = 0;
+    CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)voronoi_bricks_kernel,
+                                                           kBT, kBBufBytes));
+    if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
+    const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
+    const int grid = (int)std::min<int64_t>(want, num_sms(dev));
+    unsigned long long *trace =
+        (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long));
+    void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv,
+                    &bstep, &S, &d_status, &max_steps, &trace};
+    CLE_CUDA(cudaLaunchCooperativeKernel((const void *)voronoi_bricks_kernel, dim3(grid), dim3(kBT),
+                                         args, kBBufBytes, st));
+    count_launches(1);
+    return CLE_OK;
+}
+
+}  // namespace cle

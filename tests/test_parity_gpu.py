@@ -294,3 +294,45 @@ def test_statistics_on_vol_labels(cle, oracle, blobs):
     ref = oracle.statistics_of_labelled_pixels(blobs, cle.pull(lab))
     _assert_stats(got, ref)
     assert len(got["label"]) == 65
+
+
+# ------------------------------------------ active-front (brick) growth -----
+def _binary_case(shape, seed, density, seed_density):
+    r = rng(seed)
+    mask = (r.uniform(size=shape) < density).astype(np.uint8)
+    seeds = ((r.uniform(size=shape) < seed_density) & (mask == 1)).astype(np.uint8)
+    return seeds, mask
+
+
+@pytest.mark.parametrize("shape", [(1, 1), (3, 40), (45, 70), (130, 97), (1, 33, 31), (9, 30, 31),
+                                   (20, 65, 67), (33, 64, 96)])
+@pytest.mark.parametrize("density", [0.35, 0.8, 1.0])
+def test_masked_voronoi_binary_exact(cle, oracle, shape, density):
+    seeds, mask = _binary_case(shape, 31, density, 0.002)
+    got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
+    ref = oracle.masked_voronoi_labeling(seeds, mask)
+    assert np.array_equal(got, ref)
+    # the general dense path agrees as well
+    assert np.array_equal(cle.pull(cle.masked_voronoi_labeling(seeds, mask)), ref)
+
+
+def test_masked_voronoi_binary_diagonal_stop(cle, oracle):
+    # a diagonal-only mask path: a face step changes nothing before the next
+    # box step would, so the reference stops and the rest stays 0
+    n = 40
+    mask = np.zeros((n, n), np.uint8)
+    for i in range(n):
+        mask[i, i] = 1
+    mask[0, 1] = 1
+    seeds = np.zeros_like(mask)
+    seeds[0, 0] = 1
+    ref, steps = oracle.masked_voronoi_labeling(seeds, mask, return_steps=True)
+    got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
+    assert np.array_equal(got, ref)
+    assert (ref > 0).sum() < mask.sum()      # growth stopped early, as in the reference
+
+
+def test_masked_voronoi_binary_many_seeds_3d(cle, oracle):
+    seeds, mask = _binary_case((24, 100, 70), 32, 0.6, 0.02)
+    got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
+    assert np.array_equal(got, oracle.masked_voronoi_labeling(seeds, mask))
