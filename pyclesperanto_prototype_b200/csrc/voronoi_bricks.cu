@@ -60,11 +60,18 @@ struct BGeo {
 struct BAppender {
     uint32_t *buf;
     uint32_t *cnt;
-    __device__ __forceinline__ void push(uint32_t v) { buf[atomicAdd(cnt, 1u)] = v; }
+    int *err;
+    // Rounds are sized so the buffer cannot fill; the check turns a broken
+    // bound into an error status instead of an out-of-range write.
+    __device__ __forceinline__ void push(uint32_t v) {
+        const uint32_t pos = atomicAdd(cnt, 1u);
+        if (pos < (uint32_t)kBBuf) buf[pos] = v;
+        else atomicExch(err, (int)CLE_ERR_ITER_LIMIT);
+    }
     __device__ __forceinline__ void flush(uint32_t *dst, uint32_t *dst_size) {
         __shared__ uint32_t base;
         __syncthreads();
-        const uint32_t n = *cnt;
+        const uint32_t n = min(*cnt, (uint32_t)kBBuf);
         if (threadIdx.x == 0) base = n ? atomicAdd(dst_size, n) : 0u;
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[base + i] = buf[i];
@@ -114,28 +121,21 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
     __shared__ uint32_t s_red[kWPB];
     if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
-    BAppender ap{s_buf, &s_cnt};
+    BAppender ap{s_buf, &s_cnt, &S->err};
     const Geo &g = G.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t gstride = gridDim.x * blockDim.x;
 
-    // step 0's bricks: the brick neighbourhoods of the seeds (tag 1)
+    // step 0's bricks: the brick neighbourhoods of the seeds (tag 1), one
+    // seed per warp per round so a round queues at most 27 bricks per warp
     const uint32_t ns = __ldcg(d_seed_count);
-    for (uint32_t base = blockIdx.x * blockDim.x; base < ns; base += gstride) {
-        const uint32_t i = base + threadIdx.x;
+    for (uint32_t base = blockIdx.x * kWPB; base < ns; base += gridDim.x * kWPB) {
+        const uint32_t i = base + warp;
         if (i < ns) {
             uint32_t x, y, z;
             m2xyz(g, __ldcg(seeds + i), x, y, z);
-            const uint32_t xb = x >> 5;
-            for (int k = 0; k < 27; ++k) {
-                const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dxb = k % 3 - 1;
-                if (!G.is3d && dz) continue;
-                const int zz = (int)z + dz, yy = (int)y + dy, xx = (int)xb + dxb;
-                if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)g.D || yy >= (int)g.H || xx >= (int)G.WB) continue;
-                const uint32_t nb = ((uint32_t)zz * g.H + (uint32_t)yy) * G.WB + (uint32_t)xx;
-                if (atomicMax(bstep + nb, 1u) < 1u) ap.push(nb);
-            }
+            const bool want = lane < 27 && (G.is3d || (lane / 9) == 1);
+            queue_neighbours(G, z, y, x >> 5, want, 1u, bstep, ap);
         }
         ap.maybe_flush(B0, &S->sizes[0]);
     }

@@ -336,3 +336,11 @@ def test_masked_voronoi_binary_many_seeds_3d(cle, oracle):
     seeds, mask = _binary_case((24, 100, 70), 32, 0.6, 0.02)
     got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
     assert np.array_equal(got, oracle.masked_voronoi_labeling(seeds, mask))
+
+
+def test_masked_voronoi_binary_dense_seeds(cle, oracle):
+    # tens of thousands of seeds: many per CTA in the seed queueing round
+    seeds, mask = _binary_case((32, 256, 256), 33, 0.7, 0.01)
+    assert seeds.sum() > 10000
+    got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
+    assert np.array_equal(got, oracle.masked_voronoi_labeling(seeds, mask))
