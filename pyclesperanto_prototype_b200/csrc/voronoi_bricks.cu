@@ -17,7 +17,8 @@
 //      brick with a voxel that the face stencil could not reach but the box
 //      stencil will (it changes at the next step).
 // Queueing deduplicates with an atomicMax on a per-brick step tag, so the
-// label buffer holds labels only.  Every voxel that can change at a step lies
+// label buffer holds labels only; a brick left without unlabelled mask voxels
+// gets the maximal tag and is never queued again.  Every voxel that can change at a step lies
 // in a queued brick (a voxel whose labelled neighbour is older was already
 // visited and either changed or was re-queued), so the result equals the
 // reference's dense iteration.  Once few bricks remain active, one CTA
@@ -34,7 +35,7 @@ constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kBBuf = 8192;                     // CTA append buffer (entries)
 constexpr int kBFlushAt = kBBuf - 27 * kWPB;    // a round queues <= 27 bricks per warp
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kBBuf;
-constexpr uint32_t kTailBricks = 1024;          // single-CTA finish at or below this
+constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
 constexpr uint32_t kPend = 0x80000000u;         // Mv: face stencil missed, box will hit
 constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
@@ -111,6 +112,7 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint
     if (atomicMax(bstep + nb, tag) < tag) ap.push(nb);
 }
 
+template <bool IS3D>
 __global__ void __launch_bounds__(kBT, 1)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
@@ -125,6 +127,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
     const Geo &g = G.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int ZR = IS3D ? 1 : 0;
 
     // step 0's bricks: the brick neighbourhoods of the seeds (tag 1), one
     // seed per warp per round so a round queues at most 27 bricks per warp
@@ -134,7 +137,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
         if (i < ns) {
             uint32_t x, y, z;
             m2xyz(g, __ldcg(seeds + i), x, y, z);
-            const bool want = lane < 27 && (G.is3d || (lane / 9) == 1);
+            const bool want = lane < 27 && (IS3D || (lane / 9) == 1);
             queue_neighbours(G, z, y, x >> 5, want, 1u, bstep, ap);
         }
         ap.maybe_flush(B0, &S->sizes[0]);
@@ -145,7 +148,6 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
     const uint64_t t_start = global_ns();
     uint32_t t = 0;
     bool done = false, tail = false;
-    const int zr = G.is3d ? 1 : 0;
     while (ok && t < max_steps) {
         if (gtid == 0 && global_ns() - t_start > kKernelLimitNs) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
         const uint32_t *F = (t & 1) ? B1 : B0;
@@ -168,43 +170,53 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const uint32_t z = g.fH.div(r), y = r - z * g.H;
             const int x = (int)(xb * 32u) + lane;
             const int xc = min(x, (int)g.W - 1);
-            const uint32_t p = r * g.W + (uint32_t)xc;
-            const bool cand = x < (int)g.W && seg[p] != 0 && ld_cg(lab + p) == 0u;
+            const bool inmask = x < (int)g.W && seg[r * g.W + (uint32_t)xc] != 0;
+            uint32_t rows[3 * (2 * ZR + 1)], lft[3 * (2 * ZR + 1)], rgt[3 * (2 * ZR + 1)];
+#pragma unroll
+            for (int dz = -ZR; dz <= ZR; ++dz)
+#pragma unroll
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int k = (dz + ZR) * 3 + (dy + 1);
+                    const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
+                    const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
+                    const uint32_t *row = lab + (zz * g.H + yy) * g.W;
+                    rows[k] = ld_cg(row + xc);
+                    lft[k] = (lane == 0) ? ld_cg(row + max(x - 1, 0)) : 0u;
+                    rgt[k] = (lane == 31) ? ld_cg(row + min(x + 1, (int)g.W - 1)) : 0u;
+                }
+            const int kc = ZR * 3 + 1;          // centre row
+            const bool cand = inmask && rows[kc] == 0u;
             uint32_t out = 0;
+            bool remain = false;
             if (__any_sync(0xffffffffu, cand)) {
                 uint32_t bm = 0, dm = 0;
-                for (int dz = -zr; dz <= zr; ++dz)
 #pragma unroll
-                    for (int dy = -1; dy <= 1; ++dy) {
-                        const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
-                        const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
-                        const uint32_t *row = lab + (zz * g.H + yy) * g.W;
-                        const uint32_t c = ld_cg(row + xc);
-                        uint32_t lft = __shfl_up_sync(0xffffffffu, c, 1);
-                        uint32_t rgt = __shfl_down_sync(0xffffffffu, c, 1);
-                        if (lane == 0) lft = ld_cg(row + max(x - 1, 0));
-                        if (lane == 31) rgt = ld_cg(row + min(x + 1, (int)g.W - 1));
-                        bm = max(bm, max(c, max(lft, rgt)));
-                        if (dz == 0 && dy == 0) dm = max(dm, max(lft, rgt));
-                        else if (dz == 0 || dy == 0) dm = max(dm, c);
-                    }
+                for (int k = 0; k < 3 * (2 * ZR + 1); ++k) {
+                    const uint32_t c = rows[k];
+                    const uint32_t up = __shfl_up_sync(0xffffffffu, c, 1);
+                    const uint32_t dn = __shfl_down_sync(0xffffffffu, c, 1);
+                    const uint32_t l = (lane == 0) ? lft[k] : up;
+                    const uint32_t rr = (lane == 31) ? rgt[k] : dn;
+                    bm = max(bm, max(c, max(l, rr)));
+                    const int dz = k / 3 - ZR, dy = k % 3 - 1;
+                    if (dz == 0 && dy == 0) dm = max(dm, max(l, rr));
+                    else if (dz == 0 || dy == 0) dm = max(dm, c);
+                }
                 if (cand) {
                     const uint32_t m = box ? bm : dm;
                     out = m ? m : ((bm != 0u) ? kPend : 0u);
                     changed += (m != 0u);
+                    remain = (m == 0u);
                 }
             }
             Mv[(size_t)idx * 32 + lane] = out;
+            // no unlabelled mask voxel left after this step: never queue it again
+            if (!__any_sync(0xffffffffu, remain) && lane == 0) atomicExch(bstep + b, 0xFFFFFFFFu);
         }
-        if (!tail) {
-            const uint32_t bs = block_total(changed, s_red);
-            if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
-            ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
-        } else {
-            const uint32_t bs = block_total(changed, s_red);
-            if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
-            __syncthreads();
-        }
+        const uint32_t bs = block_total(changed, s_red);
+        if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
+        if (!tail) ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
+        else __syncthreads();
         if (!ok) break;
         const uint32_t nchanged = __ldcg(&S->changes[t & 3]);
         if (trace && gtid == 0 && t < kTraceSteps) {
@@ -224,9 +236,9 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const uint32_t idx = base + warp;
             if (idx < nB) {
                 const uint32_t b = __ldcg(F + idx);
+                const uint32_t mv = Mv[(size_t)idx * 32 + lane];
                 const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
                 const uint32_t z = g.fH.div(r), y = r - z * g.H;
-                const uint32_t mv = Mv[(size_t)idx * 32 + lane];
                 const uint32_t m = (mv & kPend) ? 0u : mv;
                 if (m) st_cg(lab + r * g.W + xb * 32u + (uint32_t)lane, m);
                 const unsigned ch = __ballot_sync(0xffffffffu, m != 0u);
@@ -234,7 +246,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                 bool want = false;
                 if (lane < 27) {
                     const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
-                    if (G.is3d || dz == 0) {
+                    if (IS3D || dz == 0) {
                         if (ch) want = dxb == 0 || (dxb < 0 && (ch & 1u)) || (dxb > 0 && (ch >> 31));
                         if (pend && dz == 0 && dy == 0 && dxb == 0) want = true;
                     }
@@ -289,17 +301,17 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     G.fWB = FastDiv(G.WB);
     G.is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    static bool attr = false;
-    if (!attr) {
-        CLE_CUDA(cudaFuncSetAttribute((const void *)voronoi_bricks_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
-        attr = true;
+    const void *kern = G.is3d ? (const void *)voronoi_bricks_kernel<true>
+                              : (const void *)voronoi_bricks_kernel<false>;
+    static bool attr[2] = {false, false};
+    if (!attr[G.is3d]) {
+        CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
+        attr[G.is3d] = true;
     }
     int dev = 0;
     CLE_CUDA(cudaGetDevice(&dev));
     int per_sm = 0;
-    CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)voronoi_bricks_kernel,
-                                                           kBT, kBBufBytes));
+    CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, kBBufBytes));
     if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
     const int grid = (int)std::min<int64_t>(want, num_sms(dev));
@@ -307,8 +319,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
         (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long));
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv,
                     &bstep, &S, &d_status, &max_steps, &trace};
-    CLE_CUDA(cudaLaunchCooperativeKernel((const void *)voronoi_bricks_kernel, dim3(grid), dim3(kBT),
-                                         args, kBBufBytes, st));
+    CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
     count_launches(1);
     return CLE_OK;
 }
