@@ -227,7 +227,7 @@ def run_b200(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    lib.cle_profile_enable(1)
+    lib.cle_profile_enable(3 if args.trace else 1)
     stage_buf = (ctypes.c_float * 16)()
     barrier(world)
     n0 = lib.cle_kernel_launches()

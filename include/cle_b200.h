@@ -73,21 +73,23 @@ const char *cle_version(void);
 const char *cle_last_error_message(void);
 /* Number of kernel launches this library has issued in this process. */
 unsigned long long cle_kernel_launches(void);
-/* Stage timing for profiling: when enabled on the calling thread, the
- * composite ops record a CUDA event at each stage boundary on their stream.
+/* Profiling (off by default).  flags bit 0: the composite ops record a CUDA
+ * event at each stage boundary on their stream; bit 1: the Voronoi loop also
+ * writes a per-step trace to a buffer allocated here (not in the compute
+ * calls).  0 turns profiling off.
  * cle_profile_stage_ms() waits for the last recorded event and writes the
  * elapsed milliseconds between consecutive events (returns how many).
  * Events 0-7 (voronoi_otsu_labeling): blur(spot) | detect_maxima |
  * blur(outline) | min/max+histogram+Otsu | threshold+seeds | seed CCL |
  * Voronoi growth; events 8-12 (statistics): pass 1 | finalise 1 | pass 2 |
  * finalise 2.  Interval 7 (between the two ops) is host time. */
-int cle_profile_enable(int on);
+int cle_profile_enable(int flags);
 int cle_profile_stage_ms(float *out, int max);
 /* Per-step trace of the last device loop (Voronoi growth) while profiling is
  * enabled: triples of uint64 (ns since the loop started, frontier size,
  * voxels changed) per step, zero after the last step.  Synchronous; returns
  * the bytes copied.  Profiling allocates its own trace buffer (outside any
- * workspace). */
+ * workspace; bit 1 of cle_profile_enable). */
 int cle_profile_trace(void *host, size_t bytes);
 
 /* ---- gaussian_blur -----------------------------------------------------

@@ -36,7 +36,7 @@ int cle_abi_version(void) { return CLE_B200_ABI_VERSION; }
 const char *cle_version(void) { return "cle_b200 1.0 (sm_100a)"; }
 const char *cle_last_error_message(void) { return last_error(); }
 unsigned long long cle_kernel_launches(void) { return launches_issued(); }
-int cle_profile_enable(int on) { return profile_enable(on); }
+int cle_profile_enable(int flags) { return profile_enable(flags); }
 int cle_profile_stage_ms(float *out, int max) { return stage_ms(out, max); }
 int cle_profile_trace(void *host, size_t bytes) { return profile_trace_read(host, bytes); }
 

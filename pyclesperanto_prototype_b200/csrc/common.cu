@@ -31,17 +31,13 @@ static thread_local int g_marks = 0;
 
 static thread_local void *g_trace = nullptr;
 static thread_local size_t g_trace_bytes = 0;
+static constexpr size_t kTraceBytes = 1 << 16;
 
-void *profile_trace_buffer(size_t bytes) {
-    if (!g_prof) return nullptr;
-    if (g_trace_bytes < bytes) {
-        if (g_trace) cudaFree(g_trace);
-        g_trace = nullptr;
-        g_trace_bytes = 0;
-        if (cudaMalloc(&g_trace, bytes) != cudaSuccess) return nullptr;
-        g_trace_bytes = bytes;
-    }
-    cudaMemset(g_trace, 0, g_trace_bytes);
+// Trace buffer of the current profiling session (allocated when tracing is
+// enabled, never on a compute call); cleared on the caller's stream.
+void *profile_trace_buffer(size_t bytes, cudaStream_t st) {
+    if (!g_trace || bytes > g_trace_bytes) return nullptr;
+    cudaMemsetAsync(g_trace, 0, bytes, st);
     return g_trace;
 }
 
@@ -53,18 +49,28 @@ int profile_trace_read(void *host, size_t bytes) {
     return (int)bytes;
 }
 
-int profile_enable(int on) {
+// flags: bit 0 stage events, bit 1 per-step loop trace; 0 turns both off.
+int profile_enable(int flags) {
+    const bool on = flags != 0;
     if (on && !g_prof) {
         for (int i = 0; i < kMaxStages; ++i) {
             cudaError_t e = cudaEventCreate(&g_ev[i]);
             if (e != cudaSuccess) return cuda_error(e, "cudaEventCreate");
         }
         g_prof = true;
-    } else if (!on && g_prof) {
-        for (int i = 0; i < kMaxStages; ++i) cudaEventDestroy(g_ev[i]);
-        if (g_trace) cudaFree(g_trace);
+    }
+    if ((flags & 2) && !g_trace) {
+        cudaError_t e = cudaMalloc(&g_trace, kTraceBytes);
+        if (e != cudaSuccess) return cuda_error(e, "trace buffer");
+        g_trace_bytes = kTraceBytes;
+    }
+    if (!(flags & 2) && g_trace) {
+        cudaFree(g_trace);
         g_trace = nullptr;
         g_trace_bytes = 0;
+    }
+    if (!on && g_prof) {
+        for (int i = 0; i < kMaxStages; ++i) cudaEventDestroy(g_ev[i]);
         g_prof = false;
     }
     return CLE_OK;

@@ -23,10 +23,10 @@ unsigned long long launches_issued();
 // per stage boundary on its stream; a no-op unless enabled on this thread.
 void stage_mark(int i, cudaStream_t st);
 int stage_ms(float *out, int max);
-int profile_enable(int on);
+int profile_enable(int flags);
 // Device buffer for per-step traces of device loops while profiling is
 // enabled (null otherwise); cle_profile_trace() copies it out.
-void *profile_trace_buffer(size_t bytes);
+void *profile_trace_buffer(size_t bytes, cudaStream_t st);
 int profile_trace_read(void *host, size_t bytes);
 int cuda_error(cudaError_t e, const char *where);
 

@@ -316,7 +316,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
     const int grid = (int)std::min<int64_t>(want, num_sms(dev));
     unsigned long long *trace =
-        (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long));
+        (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv,
                     &bstep, &S, &d_status, &max_steps, &trace};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
