@@ -128,6 +128,22 @@ size_t cle_threshold_otsu_workspace_bytes(const cle_tensor *src);
 int cle_threshold_otsu(const cle_tensor *src, const cle_tensor *dst, double *d_threshold,
                        void *workspace, size_t workspace_bytes, void *stream);
 
+/* threshold_otsu without a workspace.  No counterpart in the reference: it
+ * is for callers that can pass in the input and output buffers but cannot
+ * allocate device memory themselves (a host that owns a fixed device-memory
+ * budget and allows no allocation in its processing loop, a plugin that only
+ * passes on the buffers its host gives it).  Same result as
+ * cle_threshold_otsu; the scratch is an array built into the library
+ * (cle_threshold_otsu_noalloc_scratch_bytes(), about 4 MiB, held on every
+ * GPU that loads the library until the process exits), which limits the
+ * image to 4096 rows (y); larger images return CLE_ERR_TOO_LARGE.  The first
+ * call on each device looks up the array's device address -- make that call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (different streams or threads) race and must be serialised by
+ * the caller.  Allocates nothing. */
+int cle_threshold_otsu_noalloc(const cle_tensor *src, const cle_tensor *dst, void *stream);
+size_t cle_threshold_otsu_noalloc_scratch_bytes(void);
+
 /* ---- element-wise ops --------------------------------------------------
  * greater_constant replaces _tier1/_greater_constant.py:6-40 (constant as float32);
  * binary_and       replaces _tier1/_binary_and.py:6-47;

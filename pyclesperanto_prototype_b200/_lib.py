@@ -70,6 +70,8 @@ _SIGS = {
     "cle_histogram": (ctypes.c_int, [_T, _T, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int, _P, _SZ, _P]),
     "cle_threshold_otsu_workspace_bytes": (_SZ, [_T]),
     "cle_threshold_otsu": (ctypes.c_int, [_T, _T, _P, _P, _SZ, _P]),
+    "cle_threshold_otsu_noalloc": (ctypes.c_int, [_T, _T, _P]),
+    "cle_threshold_otsu_noalloc_scratch_bytes": (_SZ, []),
     "cle_greater_constant": (ctypes.c_int, [_T, _T, ctypes.c_float, _P]),
     "cle_binary_and": (ctypes.c_int, [_T, _T, _T, _P]),
     "cle_mask": (ctypes.c_int, [_T, _T, _T, _P]),

@@ -133,6 +133,16 @@ int cle_threshold_otsu(const cle_tensor *src, const cle_tensor *dst, double *d_t
     return greater_constant(a, b, 0.0f, mm + 2, S(stream));
 }
 
+int cle_threshold_otsu_noalloc(const cle_tensor *src, const cle_tensor *dst, void *stream) {
+    Img a, b;
+    CLE_TRY(to_img(src, a, "source"));
+    CLE_TRY(to_img(dst, b, "destination"));
+    CLE_TRY(set_device_of(a, src));
+    return threshold_otsu_noalloc(a, b, S(stream));
+}
+
+size_t cle_threshold_otsu_noalloc_scratch_bytes(void) { return threshold_otsu_noalloc_capacity(); }
+
 // ---- element-wise -----------------------------------------------------------
 int cle_greater_constant(const cle_tensor *src, const cle_tensor *dst, float c, void *stream) {
     Img a, b;

@@ -84,6 +84,10 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma,
 size_t masked_voronoi_binary_workspace_bytes(const Img &im);
 int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st);
 
+// noalloc.cu: threshold_otsu with a built-in scratch array
+size_t threshold_otsu_noalloc_capacity();
+int threshold_otsu_noalloc(const Img &src, const Img &dst, cudaStream_t st);
+
 // Status word at a fixed offset of every composite workspace (first 256 B).
 int *workspace_status_ptr(void *ws);
 
