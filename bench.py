@@ -65,7 +65,7 @@ STAGES = ["blur_spot", "detect_maxima", "blur_outline", "minmax_hist_otsu", "thr
           "stats_final2"]
 ALGO_BYTES = {"blur_spot": 2 + 4, "detect_maxima": 4 + 1, "blur_outline": 2 + 4,
               "minmax_hist_otsu": 4 + 4, "threshold_seeds": 4 + 1 + 1 + 4,
-              "stats_pass1": 4 + 2, "stats_pass2": 4 + 2}
+              "voronoi_growth": 1 + 1 + 4, "stats_pass1": 4 + 2, "stats_pass2": 4 + 2}
 
 
 def load_peaks():
@@ -293,6 +293,8 @@ def run_b200(args):
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_voxel": ALGO_BYTES[dom]}
     stages = {STAGES[i]: round(float(mean_stage[i]), 4) for i in range(12) if STAGES[i]}
+    stage_roofline = {name: round(ALGO_BYTES[name] * nvox / (stages[name] / 1e3) / 1e9 / peak, 4)
+                      for name in ALGO_BYTES if stages.get(name)}
     lat = np.array(times)
 
     cpu = None
@@ -310,7 +312,7 @@ def run_b200(args):
                           "input_dtype": str(src.dtype)},
                "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                               "p99": round(float(np.percentile(lat, 99)), 4)},
-               "stages_ms": stages, "voronoi_trace": vor_trace if args.trace else None, "e2e": e2e, "gpu_launches": int(launches),
+               "stages_ms": stages, "stage_roofline_frac": stage_roofline, "voronoi_trace": vor_trace if args.trace else None, "e2e": e2e, "gpu_launches": int(launches),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -43,8 +43,12 @@ struct Geom {
     static constexpr size_t SMEM = sizeof(float) * (ROWS * STRIDE + ROWS * kTX);
 };
 
+// Two CTAs per SM (<= 128 registers, no spills) while the z ring is small.
+template <int R>
+constexpr int min_ctas() { return R <= 8 ? 2 : 1; }
+
 template <typename Tin, int R, bool Z>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, min_ctas<R>())
 blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, int H, int W,
                   int zchunk, const __grid_constant__ Taps taps) {
     using G = Geom<R>;
@@ -190,7 +194,7 @@ int launch_fused_r(const Img &src, float *dst, const Taps &t, cudaStream_t st) {
     if (Z) {
         int dev = 0;
         cudaGetDevice(&dev);
-        const int64_t target = (int64_t)num_sms(dev) * 2;   // CTAs
+        const int64_t target = (int64_t)num_sms(dev) * 2 * min_ctas<R>();   // CTAs
         int64_t chunks = (target + (int64_t)gx * gy - 1) / ((int64_t)gx * gy);
         // keep the halo overhead (2R planes per chunk) below ~1/2
         const int64_t max_chunks = std::max<int64_t>(1, src.D / std::max(2 * R, 1));

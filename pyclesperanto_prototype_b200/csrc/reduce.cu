@@ -159,57 +159,70 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
     }
 }
 
-__global__ void hist_rowsum_kernel(const uint32_t *__restrict__ part, int64_t H, int bins,
-                                   float *__restrict__ hist) {
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bins; b += gridDim.x * blockDim.x) {
+// hist[b] = float32 running sum over rows y = 0..H-1 in order; row chunks
+// are staged in shared memory by all threads so the ordered sums read smem.
+__global__ void __launch_bounds__(1024)
+hist_rowsum_kernel(const uint32_t *__restrict__ part, int64_t H, int bins,
+                   float *__restrict__ hist) {
+    constexpr int kRowsPerChunk = 32;
+    extern __shared__ uint32_t tile[];   // kRowsPerChunk x bins
+    for (int b0 = 0; b0 < bins; b0 += blockDim.x) {
+        const int b = b0 + threadIdx.x;
         float acc = 0.0f;
-        int64_t y = 0;
-        for (; y + 8 <= H; y += 8) {   // 8 loads in flight, then the ordered sum
-            uint32_t c[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) c[k] = part[(y + k) * bins + b];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) acc = __fadd_rn(acc, (float)c[k]);
+        for (int64_t y0 = 0; y0 < H; y0 += kRowsPerChunk) {
+            const int rows = (int)((H - y0) < kRowsPerChunk ? (H - y0) : kRowsPerChunk);
+            const int span = min(bins - b0, (int)blockDim.x);
+            __syncthreads();
+            for (int i = threadIdx.x; i < rows * span; i += blockDim.x) {
+                const int r = i / span, j = i - r * span;
+                tile[r * blockDim.x + j] = part[(y0 + r) * bins + b0 + j];
+            }
+            __syncthreads();
+            if (b < bins)
+                for (int r = 0; r < rows; ++r) acc = __fadd_rn(acc, (float)tile[r * blockDim.x + threadIdx.x]);
         }
-        for (; y < H; ++y) acc = __fadd_rn(acc, (float)part[y * bins + b]);
-        hist[b] = acc;
+        if (b < bins) hist[b] = acc;
     }
 }
 
 // A7: scikit-image Otsu on the histogram, float64, no contraction, numpy's
 // sequential cumsum, first-occurrence argmax with NaN as maximum
-// (_tier9/_threshold_otsu.py:38-49, :83-106).
-__global__ void otsu_kernel(const float *__restrict__ hist, const float *__restrict__ d_minmax,
-                            double *__restrict__ d_thr, float *__restrict__ d_thr32) {
+// (_tier9/_threshold_otsu.py:38-49, :83-106).  Only the running sums are
+// sequential (numpy's cumsum order); the divisions and the between-class
+// variances are elementwise and run in parallel.
+__global__ void __launch_bounds__(256)
+otsu_kernel(const float *__restrict__ hist, const float *__restrict__ d_minmax,
+            double *__restrict__ d_thr, float *__restrict__ d_thr32) {
     constexpr int B = 256;
-    __shared__ double bc[B], w1[B], w2[B], m1[B], m2[B], var[B];
+    __shared__ double bc[B], c[B], w1[B], w2[B], s1[B], s2[B], var[B];
     const int t = threadIdx.x;
     const float mn = d_minmax[0];
     const float range32 = __fsub_rn(d_minmax[1], mn);
     bc[t] = __dadd_rn(__ddiv_rn(__dmul_rn((double)t, (double)range32), 255.0), (double)mn);
+    c[t] = (double)hist[t];
     __syncthreads();
     if (t == 0) {
         double acc = 0.0, accm = 0.0;
         for (int i = 0; i < B; ++i) {
-            double c = (double)hist[i];
-            acc = __dadd_rn(acc, c);
-            accm = __dadd_rn(accm, __dmul_rn(c, bc[i]));
+            acc = __dadd_rn(acc, c[i]);
+            accm = __dadd_rn(accm, __dmul_rn(c[i], bc[i]));
             w1[i] = acc;
-            m1[i] = __ddiv_rn(accm, acc);
+            s1[i] = accm;
         }
     } else if (t == 32) {
         double acc = 0.0, accm = 0.0;
         for (int i = B - 1; i >= 0; --i) {
-            double c = (double)hist[i];
-            acc = __dadd_rn(acc, c);
-            accm = __dadd_rn(accm, __dmul_rn(c, bc[i]));
+            acc = __dadd_rn(acc, c[i]);
+            accm = __dadd_rn(accm, __dmul_rn(c[i], bc[i]));
             w2[i] = acc;
-            m2[i] = __ddiv_rn(accm, acc);
+            s2[i] = accm;
         }
     }
     __syncthreads();
     if (t < B - 1) {
-        double d = __dsub_rn(m1[t], m2[t + 1]);
+        const double m1 = __ddiv_rn(s1[t], w1[t]);
+        const double m2 = __ddiv_rn(s2[t + 1], w2[t + 1]);
+        const double d = __dsub_rn(m1, m2);
         var[t] = __dmul_rn(__dmul_rn(w1[t], w2[t + 1]), __dmul_rn(d, d));
     }
     __syncthreads();
@@ -217,11 +230,11 @@ __global__ void otsu_kernel(const float *__restrict__ hist, const float *__restr
         int idx = 0;
         double best = 0.0;
         for (int i = 0; i < B - 1; ++i) {
-            double v = var[i];
+            const double v = var[i];
             if (v != v) { idx = i; break; }
             if (i == 0 || v > best) { best = v; idx = i; }
         }
-        double thr = bc[idx];
+        const double thr = bc[idx];
         if (d_thr) *d_thr = thr;
         if (d_thr32) *d_thr32 = __double2float_rn(thr);
     }
@@ -352,7 +365,11 @@ int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Are
         default: set_error("histogram: unsupported dtype %d", im.dtype); return CLE_ERR_DTYPE;
     }
     CLE_LAUNCH_CHECK("histogram rows");
-    hist_rowsum_kernel<<<(bins + 255) / 256, 256, 0, st>>>(part, im.H, bins, d_hist);
+    {
+        const int threads = bins < 1024 ? ((bins + 31) / 32) * 32 : 1024;
+        const size_t smem = sizeof(uint32_t) * 32 * threads;
+        hist_rowsum_kernel<<<1, threads, smem, st>>>(part, im.H, bins, d_hist);
+    }
     CLE_LAUNCH_CHECK("histogram rowsum");
     return CLE_OK;
 }

@@ -22,6 +22,7 @@ namespace cle {
 namespace {
 
 constexpr int kST = 256;
+constexpr int kBatch = 4;   // row segments per warp round
 
 struct Acc1 {
     uint32_t *cnt;
@@ -155,17 +156,35 @@ stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
     const uint32_t tasks = (uint32_t)(D * H) * chunks;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = warp; t < tasks; t += nwarps) {
+    // kBatch row segments per round: every load is issued before its use
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch];
+        float vb[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            const uint32_t l = (t < tasks && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
+            lb[k] = (l > (uint32_t)L) ? 0u : l;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+        const uint32_t l = lb[k];
+        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+        const uint32_t t = t0 + k * nwarps;
         const uint32_t row = fc.div(t);
         const uint32_t c = t - row * chunks;
         const int64_t x = (int64_t)c * 32 + lane;
-        const bool valid = x < W;
-        const int64_t m = (int64_t)row * W + x;
-        uint32_t l = valid ? lab_of(lab[m]) : 0u;
-        if (l > (uint32_t)L) l = 0u;
-        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
         const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
-        const float v = l ? to_f32(inten[m]) : 0.0f;
+        const float v = vb[k];
         const Seg s = make_seg(l);
         const double dv = (double)v;
         const double ssum = s.scan_add(dv);
@@ -192,6 +211,7 @@ stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
             atomicMax(a.ymax + i, (uint32_t)y);
             atomicMin(a.zmin + i, (uint32_t)z);
             atomicMax(a.zmax + i, (uint32_t)z);
+        }
         }
     }
 }
@@ -253,20 +273,38 @@ stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
     const uint32_t tasks = (uint32_t)(D * H) * chunks;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = warp; t < tasks; t += nwarps) {
+    // kBatch row segments per round: every load is issued before its use
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch];
+        float vb[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            const uint32_t l = (t < tasks && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
+            lb[k] = (l > (uint32_t)L) ? 0u : l;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+        const uint32_t l = lb[k];
+        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+        const uint32_t t = t0 + k * nwarps;
         const uint32_t row = fc.div(t);
         const uint32_t c = t - row * chunks;
         const int64_t x = (int64_t)c * 32 + lane;
-        const bool valid = x < W;
-        const int64_t m = (int64_t)row * W + x;
-        uint32_t l = valid ? lab_of(lab[m]) : 0u;
-        if (l > (uint32_t)L) l = 0u;
-        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
         const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
         double dc = 0.0, dm = 0.0, sq = 0.0;
         if (l) {
             const uint32_t i = l - 1;
-            const double v = (double)to_f32(inten[m]);
+            const double v = (double)vb[k];
             const double ex = (double)x - b.cx[i], ey = (double)y - b.cy[i], ez = (double)z - b.cz[i];
             const double fx = (double)x - b.mx[i], fy = (double)y - b.my[i], fz = (double)z - b.mz[i];
             dc = sqrt(ex * ex + ey * ey + ez * ez);
@@ -287,6 +325,7 @@ stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
             atomicAdd(b.ssq + i, ssq);
             atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong(mdc));
             atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong(mdm));
+        }
         }
     }
 }
