@@ -159,29 +159,59 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
     }
 }
 
-// hist[b] = float32 running sum over rows y = 0..H-1 in order; row chunks
-// are staged in shared memory by all threads so the ordered sums read smem.
+// hist[b] = float32 running sum of the row partials over y = 0..H-1 in order
+// (the reference's sum_z_projection).  Partials and their running sums are
+// integers, so while the running sum stays below 2^24 every float32 addition
+// is exact and the result is the exact integer total.  Bins whose total
+// reaches 2^24 (at most voxels / 2^24 of them) are summed in row order by one
+// warp each; the others take their exact total.
 __global__ void __launch_bounds__(1024)
 hist_rowsum_kernel(const uint32_t *__restrict__ part, int64_t H, int bins,
                    float *__restrict__ hist) {
-    constexpr int kRowsPerChunk = 32;
-    extern __shared__ uint32_t tile[];   // kRowsPerChunk x bins
-    for (int b0 = 0; b0 < bins; b0 += blockDim.x) {
-        const int b = b0 + threadIdx.x;
-        float acc = 0.0f;
-        for (int64_t y0 = 0; y0 < H; y0 += kRowsPerChunk) {
-            const int rows = (int)((H - y0) < kRowsPerChunk ? (H - y0) : kRowsPerChunk);
-            const int span = min(bins - b0, (int)blockDim.x);
-            __syncthreads();
-            for (int i = threadIdx.x; i < rows * span; i += blockDim.x) {
-                const int r = i / span, j = i - r * span;
-                tile[r * blockDim.x + j] = part[(y0 + r) * bins + b0 + j];
-            }
-            __syncthreads();
-            if (b < bins)
-                for (int r = 0; r < rows; ++r) acc = __fadd_rn(acc, (float)tile[r * blockDim.x + threadIdx.x]);
+    extern __shared__ unsigned long long tot[];   // bins x 4 partial totals
+    const int groups = blockDim.x / 256 > 0 ? (int)blockDim.x / 256 : 1;
+    for (int b0 = 0; b0 < bins; b0 += 256) {
+        // exact totals: 256 bins x `groups` row groups
+        const int b = b0 + (threadIdx.x & 255);
+        const int gidx = threadIdx.x >> 8;
+        unsigned long long acc = 0;
+        if (b < bins && gidx < groups)
+            for (int64_t y = gidx; y < H; y += groups) acc += part[y * bins + b];
+        __syncthreads();
+        if (gidx < groups) tot[(threadIdx.x & 255) * 4 + gidx] = acc;
+        __syncthreads();
+        if (threadIdx.x < 256 && b0 + (int)threadIdx.x < bins) {
+            unsigned long long t = 0;
+            for (int k = 0; k < groups; ++k) t += tot[threadIdx.x * 4 + k];
+            tot[threadIdx.x * 4] = t;
+            if (t < (1ull << 24)) hist[b0 + threadIdx.x] = (float)t;
         }
-        if (b < bins) hist[b] = acc;
+        __syncthreads();
+        // ordered float32 sums for the bins at or above 2^24
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        int seen = 0;
+        for (int j = 0; j < 256 && b0 + j < bins; ++j) {
+            if (tot[j * 4] < (1ull << 24)) continue;
+            if ((seen++ % nw) != warp) continue;
+            const int bb = b0 + j;
+            float acc32 = 0.0f;
+            for (int64_t y0 = 0; y0 < H; y0 += 128) {
+                uint32_t v[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int64_t y = y0 + q * 32 + lane;
+                    v[q] = (y < H) ? part[y * bins + bb] : 0u;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    for (int k = 0; k < 32; ++k) {
+                        const uint32_t x = __shfl_sync(0xffffffffu, v[q], k);
+                        if (y0 + q * 32 + k < H) acc32 = __fadd_rn(acc32, (float)x);
+                    }
+            }
+            if (lane == 0) hist[bb] = acc32;
+        }
+        __syncthreads();
     }
 }
 
@@ -365,11 +395,7 @@ int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Are
         default: set_error("histogram: unsupported dtype %d", im.dtype); return CLE_ERR_DTYPE;
     }
     CLE_LAUNCH_CHECK("histogram rows");
-    {
-        const int threads = bins < 1024 ? ((bins + 31) / 32) * 32 : 1024;
-        const size_t smem = sizeof(uint32_t) * 32 * threads;
-        hist_rowsum_kernel<<<1, threads, smem, st>>>(part, im.H, bins, d_hist);
-    }
+    hist_rowsum_kernel<<<1, 1024, sizeof(unsigned long long) * 256 * 4, st>>>(part, im.H, bins, d_hist);
     CLE_LAUNCH_CHECK("histogram rowsum");
     return CLE_OK;
 }
