@@ -73,6 +73,12 @@ const char *cle_version(void);
 const char *cle_last_error_message(void);
 /* Number of kernel launches this library has issued in this process. */
 unsigned long long cle_kernel_launches(void);
+/* Several pipelines on one GPU at once (batched and served forms): caps the
+ * CTAs of each cooperative launch (the growth loops) at max_ctas so that the
+ * concurrent grids fit on the GPU together; 0 restores one CTA per SM.
+ * Process-wide. */
+void cle_set_cooperative_ctas(int max_ctas);
+
 /* Profiling (off by default).  flags bit 0: the composite ops record a CUDA
  * event at each stage boundary on their stream; bit 1: the Voronoi loop also
  * writes a per-step trace to a buffer allocated here (not in the compute
@@ -209,6 +215,12 @@ int cle_voronoi_otsu_labeling(const cle_tensor *src, const cle_tensor *dst, doub
                               double outline_sigma, void *workspace, size_t workspace_bytes,
                               void *stream);
 
+/* Device pointer to the label count (= maximum label) written by the last
+ * voronoi_otsu_labeling / masked_voronoi_labeling_binary call that used this
+ * workspace; for stream-ordered consumers such as
+ * cle_statistics_of_labelled_pixels_device_count. */
+const uint32_t *cle_workspace_label_count(const void *workspace);
+
 /* Device status word of the last voronoi_otsu_labeling / masked Voronoi
  * call that used this workspace: 0 = finished, else a cle_status.  Reads
  * 4 bytes (synchronises the stream). */
@@ -241,6 +253,18 @@ size_t cle_statistics_workspace_bytes(const cle_tensor *labels, int64_t num_labe
 int cle_statistics_of_labelled_pixels(const cle_tensor *intensity, const cle_tensor *labels,
                                       int64_t num_labels, float *d_table, void *workspace,
                                       size_t workspace_bytes, void *stream);
+
+/* Statistics with the label count in device memory (no host round trip):
+ * d_num_labels points to the number of labels (e.g. from
+ * cle_workspace_label_count); the table has `capacity` columns (row stride
+ * capacity) and only the first min(count, capacity) are meaningful; labels
+ * above capacity are ignored.  Workspace: cle_statistics_workspace_bytes(labels,
+ * capacity).  Same results as cle_statistics_of_labelled_pixels. */
+int cle_statistics_of_labelled_pixels_device_count(const cle_tensor *intensity,
+                                                   const cle_tensor *labels,
+                                                   const uint32_t *d_num_labels, int64_t capacity,
+                                                   float *d_table, void *workspace,
+                                                   size_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,7 @@ _SIGS = {
     "cle_version": (ctypes.c_char_p, []),
     "cle_last_error_message": (ctypes.c_char_p, []),
     "cle_kernel_launches": (ctypes.c_ulonglong, []),
+    "cle_set_cooperative_ctas": (None, [ctypes.c_int]),
     "cle_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "cle_profile_stage_ms": (ctypes.c_int, [_P, ctypes.c_int]),
     "cle_profile_trace": (ctypes.c_int, [_P, _SZ]),
@@ -88,6 +89,8 @@ _SIGS = {
     "cle_voronoi_otsu_labeling_workspace_bytes": (_SZ, [_T]),
     "cle_voronoi_otsu_labeling": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
     "cle_workspace_status": (ctypes.c_int, [_P, _SZ, _P]),
+    "cle_workspace_label_count": (_P, [_P]),
+    "cle_statistics_of_labelled_pixels_device_count": (ctypes.c_int, [_T, _T, _P, ctypes.c_int64, _P, _P, _SZ, _P]),
     "cle_label_maximum_workspace_bytes": (_SZ, [_T]),
     "cle_label_maximum": (ctypes.c_int, [_T, _P, _P, _SZ, _P]),
     "cle_statistics_workspace_bytes": (_SZ, [_T, ctypes.c_int64]),

@@ -1,0 +1,155 @@
+"""Batched form: many independent volumes through voronoi_otsu_labeling as one
+CUDA graph.
+
+Tiles of any mix of 2D / 3D shapes are spread over K lanes (CUDA streams) by
+a longest-first greedy schedule on voxel count; tiles in a lane run one after
+another on that lane's workspace (sized for its largest tile, reused), lanes
+run concurrently.  The whole batch is captured into one CUDA graph after one
+uncaptured warm-up run, so a batch is a single graph launch with no host
+work per tile.  While several lanes run, each cooperative launch of the
+growth loop is capped at SMs / K CTAs so the concurrent grids always fit on
+the GPU together.  Results are the same labels as the per-call path, tile by
+tile (tests/test_batch_serve_gpu.py).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._tier0 import B200Array
+
+
+def _desc(t: torch.Tensor):
+    return _lib.tensor_desc(t)
+
+
+def vol_workspace_bytes(shape, dtype=torch.float32) -> int:
+    d = _lib.CleTensor()
+    d.data = 256
+    d.ndim = len(shape)
+    d.dtype = _lib._TORCH_TO_CODE[dtype]
+    acc = 1
+    strides = []
+    for s in reversed(shape):
+        strides.insert(0, acc)
+        acc *= int(s)
+    for i in range(3):
+        d.shape[i] = int(shape[i]) if i < len(shape) else 1
+        d.strides[i] = strides[i] if i < len(shape) else 1
+    d.device = 0
+    return int(_lib.load(require_gpu=False).cle_voronoi_otsu_labeling_workspace_bytes(_lib.ref(d)))
+
+
+def vol_into(src: torch.Tensor, dst: torch.Tensor, ws: torch.Tensor, spot_sigma: float,
+             outline_sigma: float, stream: int) -> None:
+    """One voronoi_otsu_labeling on `stream` with an explicit workspace."""
+    s, d = _desc(src), _desc(dst)
+    lib = _lib.load()
+    _lib.check(lib.cle_voronoi_otsu_labeling(_lib.ref(s), _lib.ref(d), float(spot_sigma),
+                                             float(outline_sigma), ws.data_ptr(), ws.numel(), stream),
+               "voronoi_otsu_labeling")
+
+
+def workspace_status(ws: torch.Tensor, stream: int) -> int:
+    return int(_lib.load().cle_workspace_status(ws.data_ptr(), ws.numel(), stream))
+
+
+def schedule(voxels, lanes: int):
+    """Longest-first greedy assignment of tiles to lanes (lists of indices)."""
+    order = sorted(range(len(voxels)), key=lambda i: -voxels[i])
+    load = [0] * lanes
+    out = [[] for _ in range(lanes)]
+    for i in order:
+        k = int(np.argmin(load))
+        out[k].append(i)
+        load[k] += voxels[i]
+    return out
+
+
+class VolBatch:
+    """voronoi_otsu_labeling over a fixed set of device volumes, replayed as
+    one CUDA graph.
+
+        batch = VolBatch(inputs, spot_sigma=3.5, outline_sigma=1.0, lanes=8)
+        batch.run()                 # labels in batch.outputs[i]
+    """
+
+    def __init__(self, inputs, spot_sigma: float = 2.0, outline_sigma: float = 2.0,
+                 lanes: int = 8, use_graph: bool = True):
+        _lib.load()
+        self.inputs = [x.tensor if isinstance(x, B200Array) else x for x in inputs]
+        for t in self.inputs:
+            if not t.is_cuda or not t.is_contiguous():
+                raise ValueError("VolBatch inputs must be contiguous CUDA tensors")
+        self.spot, self.outline = float(spot_sigma), float(outline_sigma)
+        self.device = self.inputs[0].device
+        self.outputs = [torch.empty(t.shape, dtype=torch.uint32, device=self.device) for t in self.inputs]
+        vox = [t.numel() for t in self.inputs]
+        self.lanes = max(1, min(int(lanes), len(self.inputs)))
+        self.plan = [p for p in schedule(vox, self.lanes) if p]
+        self.lanes = len(self.plan)
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in self.plan]
+        self.ws = []
+        for p in self.plan:
+            need = max(vol_workspace_bytes(tuple(self.inputs[i].shape), self.inputs[i].dtype) for i in p)
+            self.ws.append(torch.empty(need, dtype=torch.uint8, device=self.device))
+        # per-lane sticky status: max over every call's status word (offset 0
+        # of its workspace), so a limit hit by any tile is reported
+        self.status = torch.zeros(len(self.plan), dtype=torch.int32, device=self.device)
+        self.graph = None
+        self.use_graph = use_graph
+        self._coop = max(1, torch.cuda.get_device_properties(self.device).multi_processor_count // self.lanes)
+
+    def _issue(self):
+        main = torch.cuda.current_stream(self.device)
+        self.status.zero_()
+        for s in self.streams:
+            s.wait_stream(main)
+        for k, (p, s, ws) in enumerate(zip(self.plan, self.streams, self.ws)):
+            with torch.cuda.stream(s):
+                word = ws[:4].view(torch.int32)
+                for i in p:
+                    vol_into(self.inputs[i], self.outputs[i], ws, self.spot, self.outline, s.cuda_stream)
+                    torch.maximum(self.status[k:k + 1], word, out=self.status[k:k + 1])
+        for s in self.streams:
+            main.wait_stream(s)
+
+    def capture(self):
+        lib = _lib.load()
+        lib.cle_set_cooperative_ctas(self._coop if self.lanes > 1 else 0)
+        try:
+            self._issue()                       # uncaptured warm-up (sets kernel attributes)
+            torch.cuda.synchronize(self.device)
+            self.check()
+            if self.use_graph:
+                g = torch.cuda.CUDAGraph()
+                cap = torch.cuda.Stream(device=self.device)
+                cap.wait_stream(torch.cuda.current_stream(self.device))
+                with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
+                    self._issue()
+                self.graph = g
+        finally:
+            lib.cle_set_cooperative_ctas(0)
+        return self
+
+    def run(self):
+        """One batch on the current stream (graph replay when captured)."""
+        lib = _lib.load()
+        lib.cle_set_cooperative_ctas(self._coop if self.lanes > 1 else 0)
+        try:
+            if self.graph is None and self.use_graph:
+                self.capture()
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._issue()
+        finally:
+            lib.cle_set_cooperative_ctas(0)
+        return self.outputs
+
+    def check(self):
+        """Raises if any tile's device loop reported a limit (synchronises)."""
+        st = int(self.status.max().item())
+        if st:
+            raise _lib.ERRORS.get(st, RuntimeError)(f"voronoi_otsu_labeling (batch): device status {st}")

@@ -37,6 +37,7 @@ const char *cle_version(void) { return "cle_b200 1.0 (sm_100a)"; }
 const char *cle_last_error_message(void) { return last_error(); }
 unsigned long long cle_kernel_launches(void) { return launches_issued(); }
 int cle_profile_enable(int flags) { return profile_enable(flags); }
+void cle_set_cooperative_ctas(int max_ctas) { set_cooperative_ctas(max_ctas); }
 int cle_profile_stage_ms(float *out, int max) { return stage_ms(out, max); }
 int cle_profile_trace(void *host, size_t bytes) { return profile_trace_read(host, bytes); }
 
@@ -311,6 +312,10 @@ int cle_voronoi_otsu_labeling(const cle_tensor *src, const cle_tensor *dst, doub
     return voronoi_otsu_labeling(a, d, spot_sigma, outline_sigma, ar, S(stream));
 }
 
+const uint32_t *cle_workspace_label_count(const void *ws) {
+    return ws ? workspace_label_count_ptr(const_cast<void *>(ws)) : nullptr;
+}
+
 int cle_workspace_status(const void *ws, size_t ws_bytes, void *stream) {
     if (!ws || ws_bytes < sizeof(int)) { set_error("workspace_status: no workspace"); return CLE_ERR_WORKSPACE; }
     int v = 0;
@@ -350,6 +355,20 @@ int cle_statistics_of_labelled_pixels(const cle_tensor *inten, const cle_tensor 
     CLE_TRY(set_device_of(a, inten));
     Arena ar(ws, ws_bytes);
     return statistics(a, b, L, d_table, ar, S(stream));
+}
+
+int cle_statistics_of_labelled_pixels_device_count(const cle_tensor *inten, const cle_tensor *labels,
+                                                   const uint32_t *d_num_labels, int64_t capacity,
+                                                   float *d_table, void *ws, size_t ws_bytes,
+                                                   void *stream) {
+    Img a, b;
+    CLE_TRY(to_img(inten, a, "intensity_image"));
+    CLE_TRY(to_img(labels, b, "label_image"));
+    if (!d_num_labels || !d_table || capacity < 1) { set_error("statistics: null count/table or capacity < 1"); return CLE_ERR_ARG; }
+    CLE_TRY(ws_check(ws, ws_bytes, stats_workspace_bytes(b, capacity), "statistics_of_labelled_pixels"));
+    CLE_TRY(set_device_of(a, inten));
+    Arena ar(ws, ws_bytes);
+    return statistics(a, b, capacity, d_table, ar, S(stream), d_num_labels);
 }
 
 }  // extern "C"

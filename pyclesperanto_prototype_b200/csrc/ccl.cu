@@ -173,6 +173,12 @@ __global__ void ccl_label_list(uint32_t *__restrict__ lab, const uint32_t *__res
     }
 }
 
+__global__ void count_ranks_kernel(const uint32_t *__restrict__ bitmap,
+                                   const uint32_t *__restrict__ prefix, uint32_t words,
+                                   uint32_t *__restrict__ out) {
+    *out = prefix[words - 1] + __popc(bitmap[words - 1]);
+}
+
 // ---- rank machinery -------------------------------------------------------
 __global__ void chunk_count_kernel(const uint32_t *__restrict__ bitmap, uint32_t words,
                                    uint32_t *__restrict__ chunk) {
@@ -361,7 +367,8 @@ int ccl_dense(const Img &bin, uint32_t *lab, Arena &ws, cudaStream_t st) {
 }
 
 int ccl_list(const Geo &g, int64_t n, uint32_t *lab, const uint32_t *list,
-             const uint32_t *d_count, int64_t cap, Arena &ws, cudaStream_t st) {
+             const uint32_t *d_count, int64_t cap, Arena &ws, cudaStream_t st,
+             uint32_t *d_nlabels) {
     Rank r = take_rank(ws, fkey_bits_for(n));
     if (!ws.ok()) { set_error("seed labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
     const int b = launch_blocks(cap, kT);
@@ -373,6 +380,10 @@ int ccl_list(const Geo &g, int64_t n, uint32_t *lab, const uint32_t *list,
     CLE_TRY(rank_build(r, st));
     ccl_label_list<<<b, kT, 0, st>>>(lab, list, d_count, r.bitmap, r.prefix);
     CLE_LAUNCH_CHECK("ccl list label");
+    if (d_nlabels) {
+        count_ranks_kernel<<<1, 1, 0, st>>>(r.bitmap, r.prefix, r.words, d_nlabels);
+        CLE_LAUNCH_CHECK("label count");
+    }
     return CLE_OK;
 }
 

@@ -225,6 +225,14 @@ int num_sms(int device) {
     return cache[device];
 }
 
+static std::atomic<int> g_coop_ctas{0};
+void set_cooperative_ctas(int n) { g_coop_ctas.store(n > 0 ? n : 0); }
+int cooperative_ctas(int device) {
+    const int sms = num_sms(device);
+    const int cap = g_coop_ctas.load();
+    return (cap > 0 && cap < sms) ? cap : sms;
+}
+
 int launch_blocks(int64_t items, int threads, int max_blocks_per_sm) {
     int dev = 0;
     cudaGetDevice(&dev);

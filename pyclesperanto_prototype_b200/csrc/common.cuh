@@ -229,6 +229,11 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, int *err, uint64_t lim
 
 // Launch helpers
 int num_sms(int device);
+// Upper bound on the CTAs of one cooperative launch (0 = one per SM).  Set
+// when several pipelines run concurrently (batched / served forms) so their
+// cooperative grids fit on the GPU together.
+void set_cooperative_ctas(int n);
+int cooperative_ctas(int device);
 int launch_blocks(int64_t items, int threads, int max_blocks_per_sm = 8);
 
 }  // namespace cle

@@ -50,7 +50,8 @@ int ccl_dense(const Img &binary, uint32_t *labels, Arena &ws, cudaStream_t st);
 // already hold (own x-major key + 1); on return those entries hold labels.
 // d_count: device count of list entries; cap: list capacity.
 int ccl_list(const Geo &g, int64_t n, uint32_t *labels, const uint32_t *list,
-             const uint32_t *d_count, int64_t cap, Arena &ws, cudaStream_t st);
+             const uint32_t *d_count, int64_t cap, Arena &ws, cudaStream_t st,
+             uint32_t *d_nlabels = nullptr);
 int ccl_to_dst(const uint32_t *lab, const Img &dst, cudaStream_t st);
 size_t relabel_workspace_bytes(uint32_t max_label);
 int relabel_sequential(const Img &src, const Img &dst, uint32_t max_label, Arena &ws,
@@ -72,7 +73,7 @@ int masked_voronoi_dense(const Img &binary, const Img &mask, const Img &dst, int
 // stats.cu
 size_t stats_workspace_bytes(const Img &labels, int64_t L);
 int statistics(const Img &inten, const Img &labels, int64_t L, float *d_table, Arena &ws,
-               cudaStream_t st);
+               cudaStream_t st, const uint32_t *d_L = nullptr);
 
 // pipeline.cu
 size_t vol_workspace_bytes(const Img &im);
@@ -90,5 +91,6 @@ int threshold_otsu_noalloc(const Img &src, const Img &dst, cudaStream_t st);
 
 // Status word at a fixed offset of every composite workspace (first 256 B).
 int *workspace_status_ptr(void *ws);
+uint32_t *workspace_label_count_ptr(void *ws);
 
 }  // namespace cle

@@ -21,6 +21,8 @@ namespace {
 struct Scalars {
     int status;
     uint32_t seed_count;
+    uint32_t nlabels;        // labels of the last call (= its maximum label)
+    uint32_t pad0;
     float minmax[2];
     float thr32;
     float pad;
@@ -182,7 +184,7 @@ int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena
         case CLE_U32: CLE_TRY(launch_mask_seeds<uint32_t>(bin, mask, g, l, lab, st)); break;
         default: set_error("masked_voronoi_labeling: unsupported binary dtype %d", bin.dtype); return CLE_ERR_DTYPE;
     }
-    CLE_TRY(ccl_list(g, bin.n(), lab, l.seeds, &l.sc->seed_count, bin.n(), ws, st));
+    CLE_TRY(ccl_list(g, bin.n(), lab, l.seeds, &l.sc->seed_count, bin.n(), ws, st, &l.sc->nlabels));
     ws.off = tail_off;
     CLE_TRY(voronoi_frontier(bin, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st));
     if (dst.dtype == CLE_F32) {
@@ -193,6 +195,7 @@ int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena
 }
 
 int *workspace_status_ptr(void *ws) { return &reinterpret_cast<Scalars *>(ws)->status; }
+uint32_t *workspace_label_count_ptr(void *ws) { return &reinterpret_cast<Scalars *>(ws)->nlabels; }
 
 size_t vol_workspace_bytes(const Img &im) {
     Arena a(nullptr, 0);
@@ -261,7 +264,7 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     stage_mark(5, st);
 
     // 8: label the seeds
-    CLE_TRY(ccl_list(g, n, lab, l.seeds, &l.sc->seed_count, n, ws, st));
+    CLE_TRY(ccl_list(g, n, lab, l.seeds, &l.sc->seed_count, n, ws, st, &l.sc->nlabels));
     ws.off = tail_off;
     stage_mark(6, st);
 

@@ -150,7 +150,8 @@ __device__ __forceinline__ Seg make_seg(uint32_t l) {
 template <typename TL, typename TI>
 __global__ void __launch_bounds__(kST)
 stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t L, Acc1 a, FastDiv fc, FastDiv fh) {
+            int64_t W, int64_t Lcap, Acc1 a, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
+    const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
     const int lane = threadIdx.x & 31;
     const uint32_t chunks = (uint32_t)((W + 31) / 32);
     const uint32_t tasks = (uint32_t)(D * H) * chunks;
@@ -267,7 +268,8 @@ __global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T) {
 template <typename TL, typename TI>
 __global__ void __launch_bounds__(kST)
 stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t L, Acc2 b, FastDiv fc, FastDiv fh) {
+            int64_t W, int64_t Lcap, Acc2 b, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
+    const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
     const int lane = threadIdx.x & 31;
     const uint32_t chunks = (uint32_t)((W + 31) / 32);
     const uint32_t tasks = (uint32_t)(D * H) * chunks;
@@ -350,18 +352,18 @@ __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T) {
 
 template <typename TL, typename TI>
 int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a,
-                const Acc2 &b, cudaStream_t st) {
+                const Acc2 &b, cudaStream_t st, const uint32_t *d_L) {
     const int64_t tasks = lab.D * lab.H * ((lab.W + 31) / 32);
     const int blocks = launch_blocks(tasks * 32, kST, 8);
     const FastDiv fc((uint32_t)((lab.W + 31) / 32)), fh((uint32_t)lab.H);
     stage_mark(8, st);
     stats_pass1<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, a, fc, fh);
+                                                lab.H, lab.W, L, a, fc, fh, d_L);
     stage_mark(9, st);
     stats_final1<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, T);
     stage_mark(10, st);
     stats_pass2<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, b, fc, fh);
+                                                lab.H, lab.W, L, b, fc, fh, d_L);
     stage_mark(11, st);
     stats_final2<<<launch_blocks(L, 256), 256, 0, st>>>(b, L, T);
     stage_mark(12, st);
@@ -371,12 +373,12 @@ int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc
 
 template <typename TL>
 int stats_i(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a, const Acc2 &b,
-            cudaStream_t st) {
+            cudaStream_t st, const uint32_t *d_L) {
     switch (inten.dtype) {
-        case CLE_F32: return stats_typed<TL, float>(inten, lab, L, T, a, b, st);
-        case CLE_U16: return stats_typed<TL, uint16_t>(inten, lab, L, T, a, b, st);
-        case CLE_U8: return stats_typed<TL, uint8_t>(inten, lab, L, T, a, b, st);
-        case CLE_U32: return stats_typed<TL, uint32_t>(inten, lab, L, T, a, b, st);
+        case CLE_F32: return stats_typed<TL, float>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_U16: return stats_typed<TL, uint16_t>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_U8: return stats_typed<TL, uint8_t>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_U32: return stats_typed<TL, uint32_t>(inten, lab, L, T, a, b, st, d_L);
         default: set_error("statistics: unsupported intensity dtype %d", inten.dtype); return CLE_ERR_DTYPE;
     }
 }
@@ -390,7 +392,8 @@ size_t stats_workspace_bytes(const Img &, int64_t L) {
     return a.off;
 }
 
-int statistics(const Img &inten, const Img &lab, int64_t L, float *T, Arena &ws, cudaStream_t st) {
+int statistics(const Img &inten, const Img &lab, int64_t L, float *T, Arena &ws, cudaStream_t st,
+               const uint32_t *d_L) {
     CLE_TRY(same_shape(inten, lab, "intensity_image", "label_image"));
     if (L < 0 || L > 0x7FFFFFFF) { set_error("statistics: bad label count %lld", (long long)L); return CLE_ERR_ARG; }
     if (L == 0) return CLE_OK;
@@ -400,10 +403,10 @@ int statistics(const Img &inten, const Img &lab, int64_t L, float *T, Arena &ws,
     stats_init<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L);
     CLE_LAUNCH_CHECK("statistics init");
     switch (lab.dtype) {
-        case CLE_U32: return stats_i<uint32_t>(inten, lab, L, T, a, b, st);
-        case CLE_F32: return stats_i<float>(inten, lab, L, T, a, b, st);
-        case CLE_U16: return stats_i<uint16_t>(inten, lab, L, T, a, b, st);
-        case CLE_U8: return stats_i<uint8_t>(inten, lab, L, T, a, b, st);
+        case CLE_U32: return stats_i<uint32_t>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_F32: return stats_i<float>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_U16: return stats_i<uint16_t>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_U8: return stats_i<uint8_t>(inten, lab, L, T, a, b, st, d_L);
         default: set_error("statistics: unsupported label dtype %d", lab.dtype); return CLE_ERR_DTYPE;
     }
 }

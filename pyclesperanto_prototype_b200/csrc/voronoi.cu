@@ -125,7 +125,7 @@ int coop_grid(const void *func, int threads, size_t smem, int64_t work, int max_
         per_sm < 1)
         per_sm = 1;
     if (per_sm > max_per_sm) per_sm = max_per_sm;
-    int64_t cap = (int64_t)per_sm * num_sms(dev);
+    int64_t cap = (int64_t)per_sm * cooperative_ctas(dev);
     int64_t want = (work + threads * 4 - 1) / (threads * 4);
     if (want < 1) want = 1;
     return (int)(want < cap ? want : cap);

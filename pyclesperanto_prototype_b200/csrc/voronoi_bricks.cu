@@ -314,7 +314,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, kBBufBytes));
     if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
-    const int grid = (int)std::min<int64_t>(want, num_sms(dev));
+    const int grid = (int)std::min<int64_t>(want, cooperative_ctas(dev));
     unsigned long long *trace =
         (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv,

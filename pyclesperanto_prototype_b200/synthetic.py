@@ -125,22 +125,16 @@ def lightsheet_volume(shape=(512, 1024, 1024), n_objects=30000, seed=2, device="
     return out.clamp_(0, 65535).to(torch.int32).to(torch.uint16)
 
 
-def _gauss_kernel1d(s, device):
-    import torch
-
-    r = int(math.ceil(3 * s))
-    t = torch.arange(-r, r + 1, device=device, dtype=torch.float32)
-    k = torch.exp(-t * t / (2 * s * s))
-    return k  # peak-normalised: an impulse of weight A has peak A
-
-
 def blob_tile(shape, density, seed, device="cuda"):
     """float32 torch tile: background N(10,3) clipped at 0, isotropic Gaussian
     blobs (sigma U(4,10), peak U(120,250)) at `density` blobs per voxel,
-    Poisson noise.  Blobs are rendered per sigma class (1 px wide) by separable
-    convolution of peak-weighted impulses."""
+    Poisson noise.  Blobs are rendered per sigma class (1 px wide) by blurring
+    impulses of weight peak / w0^d with the library's Gaussian (w0 = centre
+    weight), so each blob has its drawn peak."""
     import torch
-    import torch.nn.functional as F
+    from . import _ops
+    from ._tier0 import B200Array
+    from . import _lib
 
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
@@ -156,20 +150,13 @@ def blob_tile(shape, density, seed, device="cuda"):
         sel = cls == c
         if not bool(sel.any()):
             continue
+        s_c = 4.5 + c
+        n = int(8 * s_c) | 1
+        r = n // 2
+        w0 = 1.0 / float(np.exp(-(np.arange(-r, r + 1) ** 2) / (2 * s_c * s_c)).sum())
         imp = torch.zeros(nvox, device=device)
-        imp.index_put_((idx[sel],), amp[sel], accumulate=True)
-        imp = imp.view(shape)
-        k = _gauss_kernel1d(4.5 + c, device)
-        r = (k.numel() - 1) // 2
-        x = imp.unsqueeze(0).unsqueeze(0)
-        for ax in range(len(shape)):
-            ks = [1] * len(shape)
-            ks[ax] = k.numel()
-            pad = [0] * (2 * len(shape))
-            pad[2 * (len(shape) - 1 - ax)] = r
-            pad[2 * (len(shape) - 1 - ax) + 1] = r
-            xp = F.pad(x, pad)
-            w = k.view(1, 1, *ks)
-            x = F.conv2d(xp, w) if len(shape) == 2 else F.conv3d(xp, w)
-        img += x[0, 0]
+        imp.index_put_((idx[sel],), amp[sel] / (w0 ** len(shape)), accumulate=True)
+        out = torch.empty(shape, dtype=torch.float32, device=device)
+        _ops.gaussian_blur(B200Array(imp.view(shape)), B200Array(out), s_c, s_c, s_c)
+        img += out
     return torch.poisson(img, generator=g).to(torch.float32)
