@@ -17,8 +17,8 @@ benchmark workloads (there is no public dataset for them):
   blob_tile        a 2D or 3D tile of isotropic Gaussian blobs at a given
                    density per voxel, per-tile seed (batched / served forms).
 
-Every generator takes a ``scale`` so tests can build small instances with
-the same recipe.
+Every generator takes its shape and object counts as arguments, so tests
+build small instances with the same recipe.
 """
 from __future__ import annotations
 
@@ -134,7 +134,6 @@ def blob_tile(shape, density, seed, device="cuda"):
     import torch
     from . import _ops
     from ._tier0 import B200Array
-    from . import _lib
 
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
