@@ -99,6 +99,7 @@ class VolBatch:
         self.status = torch.zeros(len(self.plan), dtype=torch.int32, device=self.device)
         self.graph = None
         self.use_graph = use_graph
+        self.launches_per_run = 0     # library kernels one run launches
         self._coop = max(1, torch.cuda.get_device_properties(self.device).multi_processor_count // self.lanes)
 
     def _issue(self):
@@ -126,8 +127,10 @@ class VolBatch:
                 g = torch.cuda.CUDAGraph()
                 cap = torch.cuda.Stream(device=self.device)
                 cap.wait_stream(torch.cuda.current_stream(self.device))
+                n0 = lib.cle_kernel_launches()
                 with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
                     self._issue()
+                self.launches_per_run = int(lib.cle_kernel_launches() - n0)
                 self.graph = g
         finally:
             lib.cle_set_cooperative_ctas(0)
@@ -143,7 +146,9 @@ class VolBatch:
             if self.graph is not None:
                 self.graph.replay()
             else:
+                n0 = lib.cle_kernel_launches()
                 self._issue()
+                self.launches_per_run = int(lib.cle_kernel_launches() - n0)
         finally:
             lib.cle_set_cooperative_ctas(0)
         return self.outputs

@@ -178,10 +178,12 @@ class SegmentationServer:
         return requests
 
 
-def per_call_loop(requests, spot_sigma: float, outline_sigma: float, realtime: bool = True):
+def per_call_loop(requests, spot_sigma: float, outline_sigma: float, realtime: bool = True,
+                  keep_labels: bool = False):
     """The plain per-call path on the same trace: one request at a time through
     the public API (voronoi_otsu_labeling, then statistics_of_labelled_pixels),
-    each started at max(arrival, previous completion)."""
+    each started at max(arrival, previous completion).  With keep_labels each
+    request keeps its device label image (memory grows with the trace)."""
     from . import _ops
     from ._tier0 import push_native
     t0 = time.perf_counter()
@@ -197,5 +199,6 @@ def per_call_loop(requests, spot_sigma: float, outline_sigma: float, realtime: b
         req.done = time.perf_counter() - t0
         req.num_labels = len(stats["label"])
         req.table = np.stack([stats[k] for k in STAT_KEYS]) if req.num_labels else np.zeros((35, 0), np.float32)
-        req.labels = lab.tensor
+        if keep_labels:
+            req.labels = lab.tensor
     return requests
