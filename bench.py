@@ -76,6 +76,19 @@ ALGO_BYTES = {"blur_spot": 2 + 4, "detect_maxima": 4 + 1, "blur_outline": 2 + 4,
               "voronoi_growth": 1 + 1 + 4, "stats_pass1": 4 + 2, "stats_pass2": 4 + 2}
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one ncu --set full capture per kernel on the nuclei workload; the captures
+# are summarised in profiles/<kernel>_nuclei_128x512x512.md.
+MEASURED_TRAFFIC = {
+    "nuclei": {"voronoi_growth": (547.733e6 + 164.538e6, "voronoi_bricks_kernel_nuclei_128x512x512.md"),
+               "blur_spot": (68.036e6 + 80.706e6, "blur_fused_kernel_nuclei_128x512x512.md"),
+               "blur_outline": (67.404e6 + 81.943e6, "blur_fused_kernel_nuclei_128x512x512.md"),
+               "detect_maxima": (135.090e6 + 19.932e6, "maxima_kernel_nuclei_128x512x512.md"),
+               "stats_pass1": (165.253e6 + 3.873e6, "stats_pass1_nuclei_128x512x512.md"),
+               "stats_pass2": (165.247e6 + 3.618e6, "stats_pass2_nuclei_128x512x512.md")},
+}
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -184,12 +197,15 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def cpu_baseline_sample(vol, spot, outline, reps=2):
-    """Oracle on the host cores (all threads); returns (Mvox/s, cores, sample)."""
+def cpu_baseline_sample(vol, spot, outline, reps=2, max_voxels=48 * 1024 * 1024):
+    """Oracle on the host cores (all threads); returns (Mvox/s, cores, voxels,
+    seconds).  Volumes above max_voxels are sampled as their first z planes."""
     import oracle
     oracle.build()
     cores = oracle.num_threads()
-    f = vol.astype(np.float32) if not hasattr(vol, "cpu") else vol.cpu().numpy().astype(np.float32)
+    if vol.ndim == 3 and vol.size > max_voxels:
+        vol = vol[:max(1, max_voxels // (vol.shape[1] * vol.shape[2]))]
+    f = vol.astype(np.float32)
     ts = []
     for _ in range(reps):
         t0 = time.perf_counter()
@@ -197,7 +213,7 @@ def cpu_baseline_sample(vol, spot, outline, reps=2):
         oracle.statistics_of_labelled_pixels(f, lab)
         ts.append(time.perf_counter() - t0)
     t = min(ts)
-    return f.size / t / 1e6, cores, t
+    return f.size / t / 1e6, cores, f.shape, t
 
 
 def run_b200(args):
@@ -211,8 +227,9 @@ def run_b200(args):
     w = WORKLOADS[args.workload]
     host = make_input(args.workload, device=dev)
     if isinstance(host, torch.Tensor):
+        # generated on the device; a host copy feeds the end-to-end leg
         src = cle.B200Array(host.contiguous())
-        host_np = None
+        host_np = host.cpu().numpy()
     else:
         host_np = host
         src = cle.push_native(host_np)
@@ -300,16 +317,27 @@ def run_b200(args):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None, "algorithmic_bytes_per_voxel": ALGO_BYTES[dom]}
+    tr = MEASURED_TRAFFIC.get(args.workload, {}).get(dom)
+    if tr:
+        roofline["traffic"] = tr[0]
+        roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/" + tr[1]
     stages = {STAGES[i]: round(float(mean_stage[i]), 4) for i in range(12) if STAGES[i]}
     stage_roofline = {name: round(ALGO_BYTES[name] * nvox / (stages[name] / 1e3) / 1e9 / peak, 4)
                       for name in ALGO_BYTES if stages.get(name)}
+    # the whole pipeline against the same peak: every stage's algorithmic
+    # bytes over the step time
+    pipe_bytes = sum(ALGO_BYTES.values()) * nvox
+    pipeline_roofline = {"bytes_per_voxel": sum(ALGO_BYTES.values()),
+                         "achieved": round(pipe_bytes / (ms_per_step / 1e3) / 1e9, 1),
+                         "frac": round(pipe_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4)}
     lat = np.array(times)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and host_np is not None:
-        v, cores, t = cpu_baseline_sample(host_np, w["spot"], w["outline"])
+        v, cores, shp, t = cpu_baseline_sample(host_np, w["spot"], w["outline"])
+        what = "full workload" if int(np.prod(shp)) == nvox else "first %d z planes of the workload" % shp[0]
         cpu = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"full workload ({nvox} voxels) once per repetition, best of 2, {t:.2f} s"}
+               "sample": f"{what} ({'x'.join(map(str, shp))} voxels) per repetition, best of 2, {t:.2f} s"}
     if rank == 0:
         out = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -321,7 +349,8 @@ def run_b200(args):
                "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                               "p99": round(float(np.percentile(lat, 99)), 4)},
                "stages_ms": stages, "stage_roofline_frac": stage_roofline, "voronoi_trace": vor_trace if args.trace else None, "e2e": e2e, "gpu_launches": int(launches),
-               "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+               "roofline": roofline, "pipeline_roofline": pipeline_roofline, "cpu_baseline": cpu,
+               "clocks": clk}
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
