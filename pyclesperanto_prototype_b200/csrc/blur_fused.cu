@@ -7,8 +7,9 @@
 //   * a CTA owns a kTX x kTY output tile in (x, y) and marches along z over a
 //     chunk of planes (plus R halo planes at each end, clamped);
 //   * per input plane it stages the clamped (kTY+2R) x (kTX+2R) tile in
-//     shared memory -- the next plane's values are loaded into registers
-//     while the current one is computed;
+//     shared memory -- the next plane's raw values are loaded into registers
+//     while the current one is computed and converted to float32 only when
+//     stored, so no instruction waits on them early;
 //   * x pass: each thread produces 4 consecutive x outputs from 128-bit
 //     shared loads, for all kTY+2R rows (the y halo);
 //   * y pass: each thread produces kRY consecutive rows of one column from a
@@ -73,7 +74,9 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
     int gx[G::COL_LOADS];
 #pragma unroll
     for (int c = 0; c < G::COL_LOADS; ++c) gx[c] = clampi(x0 - R + lane + 32 * c, 0, W - 1);
-    float pre[G::LOADS];
+    // raw source values; converted when stored, so the loads of the next
+    // plane stay in flight while the current plane is computed
+    Tin pre[G::LOADS];
     auto load_plane = [&](int v) {
         const int zi = Z ? clampi(zbase + v, 0, D - 1) : 0;
         const Tin *p = src + (int64_t)zi * plane;
@@ -84,7 +87,7 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
 #pragma unroll
             for (int c = 0; c < G::COL_LOADS; ++c) {
                 const bool ok = r < G::ROWS && lane + 32 * c < G::COLS;
-                pre[rr * G::COL_LOADS + c] = ok ? to_f32(__ldg(row + gx[c])) : 0.0f;
+                pre[rr * G::COL_LOADS + c] = ok ? __ldg(row + gx[c]) : Tin(0);
             }
         }
     };
@@ -94,7 +97,7 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
             const int r = warp + rr * kWarps;
 #pragma unroll
             for (int c = 0; c < G::COL_LOADS; ++c)
-                if (r < G::ROWS && lane + 32 * c < G::COLS) In[r * G::STRIDE + lane + 32 * c] = pre[rr * G::COL_LOADS + c];
+                if (r < G::ROWS && lane + 32 * c < G::COLS) In[r * G::STRIDE + lane + 32 * c] = to_f32(pre[rr * G::COL_LOADS + c]);
         }
     };
 
