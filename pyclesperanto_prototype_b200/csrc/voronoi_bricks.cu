@@ -32,9 +32,8 @@ namespace {
 
 constexpr int kBT = 1024;                       // threads per CTA (one CTA per SM)
 constexpr int kWPB = kBT / 32;                  // warps per CTA
-constexpr int kBBuf = 8192;                     // CTA append buffer (entries)
-constexpr int kBFlushAt = kBBuf - 27 * kWPB;    // a round queues <= 27 bricks per warp
-constexpr size_t kBBufBytes = sizeof(uint32_t) * kBBuf;
+constexpr int kSlice = 256;                     // per-warp append slice (entries)
+constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
 constexpr uint32_t kPend = 0x80000000u;         // Mv: face stencil missed, box will hit
 constexpr uint32_t kTraceSteps = 256;
@@ -58,31 +57,44 @@ struct BGeo {
     int is3d;
 };
 
-struct BAppender {
-    uint32_t *buf;
-    uint32_t *cnt;
+// Per-warp append slice in shared memory, flushed to a global list by the
+// warp alone, so no CTA barrier sits inside the brick loops.
+struct WarpAppender {
     int *err;
-    // Rounds are sized so the buffer cannot fill; the check turns a broken
-    // bound into an error status instead of an out-of-range write.
-    __device__ __forceinline__ void push(uint32_t v) {
-        const uint32_t pos = atomicAdd(cnt, 1u);
-        if (pos < (uint32_t)kBBuf) buf[pos] = v;
-        else atomicExch(err, (int)CLE_ERR_ITER_LIMIT);
+    uint32_t cnt;       // warp-uniform fill
+    // this warp's kSlice entries of the dynamic shared buffer
+    __device__ __forceinline__ uint32_t *buf() const {
+        extern __shared__ uint32_t s_buf[];
+        return s_buf + (threadIdx.x >> 5) * kSlice;
+    }
+    // Warp-wide: lanes with `take` append v.  A call appends at most 27
+    // entries and maybe_flush empties the slice above kSlice - 27, so it
+    // cannot overflow; the check turns a broken bound into an error status.
+    __device__ __forceinline__ void push(bool take, uint32_t v) {
+        const unsigned bal = __ballot_sync(0xffffffffu, take);
+        if (!bal) return;
+        if (take) {
+            const uint32_t pos = cnt + (uint32_t)__popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+            if (pos < (uint32_t)kSlice) buf()[pos] = v;
+            else atomicExch(err, (int)CLE_ERR_ITER_LIMIT);
+        }
+        cnt += (uint32_t)__popc(bal);
+        __syncwarp();
     }
     __device__ __forceinline__ void flush(uint32_t *dst, uint32_t *dst_size) {
-        __shared__ uint32_t base;
-        __syncthreads();
-        const uint32_t n = min(*cnt, (uint32_t)kBBuf);
-        if (threadIdx.x == 0) base = n ? atomicAdd(dst_size, n) : 0u;
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) dst[base + i] = buf[i];
-        __syncthreads();
-        if (threadIdx.x == 0) *cnt = 0;
-        __syncthreads();
+        const uint32_t k = min(cnt, (uint32_t)kSlice);
+        if (!k) return;
+        const int lane = threadIdx.x & 31;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(dst_size, k);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const uint32_t *b = buf();
+        for (uint32_t i = lane; i < k; i += 32) dst[base + i] = b[i];
+        __syncwarp();
+        cnt = 0;
     }
     __device__ __forceinline__ void maybe_flush(uint32_t *dst, uint32_t *dst_size) {
-        __syncthreads();
-        if (*cnt >= (uint32_t)kBFlushAt) flush(dst, dst_size);
+        if (cnt > (uint32_t)(kSlice - 27)) flush(dst, dst_size);
     }
 };
 
@@ -99,17 +111,22 @@ __device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
 }
 
 // Queues bricks (z+dz, y+dy, xb+dxb) for the step tagged `tag`; lane k of the
-// warp handles offset k of the 3x3x3 neighbourhood when want(k).
+// warp handles offset k of the 3x3x3 neighbourhood when want.  Warp-wide.
 __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint32_t y, uint32_t xb,
                                                  bool want, uint32_t tag, uint32_t *bstep,
-                                                 BAppender &ap) {
+                                                 WarpAppender &ap) {
     const int lane = threadIdx.x & 31;
-    if (!want || lane >= 27) return;
-    const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
-    const int zz = (int)z + dz, yy = (int)y + dy, xx = (int)xb + dxb;
-    if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)G.g.D || yy >= (int)G.g.H || xx >= (int)G.WB) return;
-    const uint32_t nb = ((uint32_t)zz * G.g.H + (uint32_t)yy) * G.WB + (uint32_t)xx;
-    if (atomicMax(bstep + nb, tag) < tag) ap.push(nb);
+    bool take = false;
+    uint32_t nb = 0;
+    if (want && lane < 27) {
+        const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+        const int zz = (int)z + dz, yy = (int)y + dy, xx = (int)xb + dxb;
+        if (zz >= 0 && yy >= 0 && xx >= 0 && zz < (int)G.g.D && yy < (int)G.g.H && xx < (int)G.WB) {
+            nb = ((uint32_t)zz * G.g.H + (uint32_t)yy) * G.WB + (uint32_t)xx;
+            take = atomicMax(bstep + nb, tag) < tag;
+        }
+    }
+    ap.push(take, nb);
 }
 
 template <bool IS3D>
@@ -118,14 +135,10 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *bstep, BState *S, int *d_status,
                       uint32_t max_steps, unsigned long long *trace) {
-    extern __shared__ uint32_t s_buf[];
-    __shared__ uint32_t s_cnt;
     __shared__ uint32_t s_red[kWPB];
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    BAppender ap{s_buf, &s_cnt, &S->err};
     const Geo &g = G.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpAppender ap{&S->err, 0u};
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
     constexpr int ZR = IS3D ? 1 : 0;
 
