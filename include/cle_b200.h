@@ -160,6 +160,11 @@ int cle_greater_constant(const cle_tensor *src, const cle_tensor *dst, float con
 int cle_binary_and(const cle_tensor *a, const cle_tensor *b, const cle_tensor *dst, void *stream);
 int cle_mask(const cle_tensor *src, const cle_tensor *mask, const cle_tensor *dst, void *stream);
 
+/* erode_box replaces _tier1/_erode_box.py:6-47 (erode_box_{2,3}d_x.cl): 1 where the
+ * voxel and all of its 3x3(x3) box neighbours are nonzero, reads clamped to the
+ * edge; source u8/u16/u32/i32/f32, destination u8/u16/u32/f32. */
+int cle_erode_box(const cle_tensor *src, const cle_tensor *dst, void *stream);
+
 /* ---- detect_maxima_box ---------------------------------------------------
  * replaces _tier1/_detect_maxima_box.py:5-48 with kernels
  * _tier1/detect_maxima_3d_x.cl:1-49, _tier1/detect_maxima_2d_x.cl:1-35.

@@ -83,6 +83,11 @@ def lib():
         L.orc_masked_voronoi.argtypes = [P, P, P, P, I64, I64, I64, I]
         L.orc_masked_voronoi.restype = I64
         L.orc_voronoi_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, D, D, P, P, P]
+        L.orc_erode_box.argtypes = [P, P, I64, I64, I64, I]
+        L.orc_gauss_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, D]
+        L.orc_gauss_otsu_labeling.restype = I64
+        L.orc_eroded_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, I, D]
+        L.orc_eroded_otsu_labeling.restype = I64
         L.orc_voronoi_otsu_labeling.restype = I64
         L.orc_statistics.argtypes = [P, P, I64, I64, I64, I64, P]
         L.orc_stats_ncols.restype = I
@@ -232,6 +237,31 @@ def voronoi_otsu_labeling(img, spot_sigma=2.0, outline_sigma=2.0, debug=False):
                                             float(outline_sigma), _p(spots), _p(seg), _p(thr))
     if debug:
         return out, dict(seeds=spots, segmentation=seg, threshold=float(thr[0]), steps=steps)
+    return out
+
+
+def erode_box(img) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint8)
+    D, H, W = _dhw(a.shape)
+    lib().orc_erode_box(_p(a), _p(out), D, H, W, a.ndim)
+    return out
+
+
+def gauss_otsu_labeling(img, outline_sigma=2.0) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint32)
+    D, H, W = _dhw(a.shape)
+    lib().orc_gauss_otsu_labeling(_p(a), _p(out), D, H, W, a.ndim, float(outline_sigma))
+    return out
+
+
+def eroded_otsu_labeling(img, number_of_erosions=5, outline_sigma=2.0) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty(a.shape, np.uint32)
+    D, H, W = _dhw(a.shape)
+    lib().orc_eroded_otsu_labeling(_p(a), _p(out), D, H, W, a.ndim, max(0, int(number_of_erosions)),
+                                   float(outline_sigma))
     return out
 
 

@@ -457,6 +457,82 @@ int64_t orc_masked_voronoi(const uint8_t *seeds, const float *mask, float *out_f
 }
 
 /* ------------------------------------------------------------------ */
+/* erode_box: _tier1/_erode_box.py:6-47 (erode_box_{2,3}d_x.cl, absent  */
+/* from the checkout).  out = 1 iff v(p) != 0 and v(q) != 0 for every q */
+/* of the 3x3(x3) box around p.  Reads clamp to the edge, and a clamped */
+/* read lands on a voxel of the same box, so out-of-range neighbours    */
+/* are skipped.  Pinned by tests/test_erode_box.py (2D 5x5).           */
+/* ------------------------------------------------------------------ */
+static void erode_u8(const uint8_t *src, uint8_t *dst, int64_t D, int64_t H, int64_t W,
+                     int ndim) {
+    const int zr = (ndim == 3) ? 1 : 0;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int64_t z = 0; z < D; ++z)
+        for (int64_t y = 0; y < H; ++y)
+            for (int64_t x = 0; x < W; ++x) {
+                uint8_t o = src[IDX(z, y, x)] != 0;
+                for (int dz = -zr; dz <= zr && o; ++dz)
+                    for (int dy = -1; dy <= 1 && o; ++dy)
+                        for (int dx = -1; dx <= 1 && o; ++dx) {
+                            const int64_t qz = z + dz, qy = y + dy, qx = x + dx;
+                            if (qz < 0 || qz >= D || qy < 0 || qy >= H || qx < 0 || qx >= W)
+                                continue;
+                            if (src[IDX(qz, qy, qx)] == 0) o = 0;
+                        }
+                dst[IDX(z, y, x)] = o;
+            }
+}
+
+void orc_erode_box(const float *src, uint8_t *dst, int64_t D, int64_t H, int64_t W, int ndim) {
+    const int64_t n = D * H * W;
+    uint8_t *nz = (uint8_t *)malloc(n);
+    for (int64_t i = 0; i < n; ++i) nz[i] = src[i] != 0.0f;
+    erode_u8(nz, dst, D, H, W, ndim);
+    free(nz);
+}
+
+/* gauss_otsu_labeling: _tier9/_gauss_otsu_labeling.py:36-45 -- blur with */
+/* outline_sigma on every axis, threshold_otsu, connected components    */
+/* (box).  Returns the number of labels.                                */
+int64_t orc_gauss_otsu_labeling(const float *src, uint32_t *labels, int64_t D, int64_t H,
+                                int64_t W, int ndim, double outline_sigma) {
+    const int64_t n = D * H * W;
+    float *tmp = (float *)malloc(sizeof(float) * n);
+    uint8_t *seg = (uint8_t *)malloc(n);
+    orc_gaussian_blur(src, tmp, D, H, W, ndim, outline_sigma, outline_sigma, outline_sigma);
+    orc_threshold_otsu(tmp, seg, D, H, W);
+    const int64_t nl = orc_ccl_box(seg, labels, D, H, W);
+    free(tmp);
+    free(seg);
+    return nl;
+}
+
+/* eroded_otsu_labeling: _tier9/_eroded_otsu_labeling.py:46-62 -- blur, */
+/* threshold_otsu, number_of_erosions box erosions of the binary image  */
+/* (int() of the argument, none when it is <= 0), then                  */
+/* masked_voronoi_labeling(eroded, binary).  Returns the Voronoi steps.  */
+int64_t orc_eroded_otsu_labeling(const float *src, uint32_t *labels, int64_t D, int64_t H,
+                                 int64_t W, int ndim, int number_of_erosions,
+                                 double outline_sigma) {
+    const int64_t n = D * H * W;
+    float *tmp = (float *)malloc(sizeof(float) * n);
+    uint8_t *binary = (uint8_t *)malloc(n);
+    uint8_t *e0 = (uint8_t *)malloc(n);
+    uint8_t *e1 = (uint8_t *)malloc(n);
+    orc_gaussian_blur(src, tmp, D, H, W, ndim, outline_sigma, outline_sigma, outline_sigma);
+    orc_threshold_otsu(tmp, binary, D, H, W);
+    memcpy(e0, binary, n);
+    for (int i = 0; i < number_of_erosions; ++i) {
+        erode_u8(e0, e1, D, H, W, ndim);
+        uint8_t *t = e0; e0 = e1; e1 = t;
+    }
+    for (int64_t i = 0; i < n; ++i) tmp[i] = (float)binary[i];
+    const int64_t steps = orc_masked_voronoi(e0, tmp, NULL, labels, D, H, W, ndim);
+    free(tmp); free(binary); free(e0); free(e1);
+    return steps;
+}
+
+/* ------------------------------------------------------------------ */
 /* A1-A12 voronoi_otsu_labeling: _tier9/_voronoi_otsu_labeling.py:57-71*/
 /* Optional debug outputs (may be NULL): spots (u8), seg (u8),         */
 /* threshold (double).                                                 */

@@ -14,6 +14,7 @@ from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, cr
                      create_labels_like, create_like, create_none, create_zyx, is_image, nparray,
                      plugin_function, pull, pull_zyx, push, push_native, push_zyx)
 from ._ops import (binary_and, connected_components_labeling_box, detect_maxima_box,
+                   erode_box, eroded_otsu_labeling, gauss_otsu_labeling,
                    gaussian_blur, greater_constant, histogram, mask, masked_voronoi_labeling,
                    masked_voronoi_labeling_binary,
                    maximum_of_all_pixels, minimum_of_all_pixels, radius_to_kernel_size,

@@ -75,6 +75,7 @@ _SIGS = {
     "cle_threshold_otsu_noalloc_scratch_bytes": (_SZ, []),
     "cle_greater_constant": (ctypes.c_int, [_T, _T, ctypes.c_float, _P]),
     "cle_binary_and": (ctypes.c_int, [_T, _T, _T, _P]),
+    "cle_erode_box": (ctypes.c_int, [_T, _T, _P]),
     "cle_mask": (ctypes.c_int, [_T, _T, _T, _P]),
     "cle_detect_maxima_box_workspace_bytes": (_SZ, [_T, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "cle_detect_maxima_box": (ctypes.c_int, [_T, _T, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _SZ, _P]),

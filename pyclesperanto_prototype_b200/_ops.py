@@ -252,6 +252,48 @@ def masked_voronoi_labeling_binary(binary_source, mask_image, labeling_destinati
     return labeling_destination
 
 
+@plugin_function(categories=['binary processing'], output_creator=create_binary_like)
+def erode_box(source: Image, destination: Image = None) -> Image:
+    """Binary erosion over the Moore neighbourhood (_tier1/_erode_box.py:6-47):
+    1 where the pixel and all of its 8 (2D) or 26 (3D) neighbours are nonzero,
+    else 0; reads clamp to the image edge."""
+    _call("cle_erode_box", _lib.ref(_T(source)), _lib.ref(_T(destination)), _lib.stream_ptr())
+    return destination
+
+
+@plugin_function(categories=['label', 'in assistant'], output_creator=create_labels_like,
+                 native_inputs=("source",))
+def gauss_otsu_labeling(source: Image, label_image_destination: Image = None,
+                        outline_sigma: float = 2) -> Image:
+    """Gaussian blur, Otsu threshold, connected components (box) of the binary
+    image (_tier9/_gauss_otsu_labeling.py:6-45); every step a device kernel,
+    no host round trip."""
+    temp = create(source)                       # float32, like the reference's create(source)
+    gaussian_blur(source, temp, outline_sigma, outline_sigma, outline_sigma)
+    segmentation = threshold_otsu(temp)
+    return connected_components_labeling_box(segmentation, label_image_destination)
+
+
+@plugin_function(categories=['label', 'in assistant'], output_creator=create_labels_like,
+                 native_inputs=("image",))
+def eroded_otsu_labeling(image: Image, labels_destination: Image = None, number_of_erosions: int = 5,
+                         outline_sigma: float = 2) -> Image:
+    """Gaussian blur, Otsu threshold, int(number_of_erosions) box erosions, then
+    the eroded objects' labels grown back inside the binary image by masked
+    Voronoi labelling (_tier9/_eroded_otsu_labeling.py:4-62).  The eroded
+    image lies inside the 0/1 binary image, so the growth runs on the
+    active-front kernel."""
+    blurred = create(image)
+    gaussian_blur(image, blurred, outline_sigma, outline_sigma, outline_sigma)
+    binary = threshold_otsu(blurred)
+    eroded = B200Array(binary.tensor.clone())
+    eroded1 = create_binary_like(binary)
+    for _ in range(int(number_of_erosions)):
+        erode_box(eroded, eroded1)
+        eroded, eroded1 = eroded1, eroded
+    return masked_voronoi_labeling_binary(eroded, binary, labels_destination)
+
+
 class Workspaces:
     """Per-shape cache of voronoi_otsu_labeling workspaces (device memory is
     reused across calls on one stream; calls on different streams must not

@@ -171,6 +171,14 @@ int cle_mask(const cle_tensor *src, const cle_tensor *msk, const cle_tensor *dst
     return mask_op(a, m, d, S(stream));
 }
 
+int cle_erode_box(const cle_tensor *src, const cle_tensor *dst, void *stream) {
+    Img a, d;
+    CLE_TRY(to_img(src, a, "source"));
+    CLE_TRY(to_img(dst, d, "destination"));
+    CLE_TRY(set_device_of(a, src));
+    return erode_box(a, d, S(stream));
+}
+
 // ---- detect_maxima_box -------------------------------------------------------
 size_t cle_detect_maxima_box_workspace_bytes(const cle_tensor *src, int rx, int ry, int rz) {
     Img im;

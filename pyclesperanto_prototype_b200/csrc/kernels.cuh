@@ -36,6 +36,9 @@ int otsu(const float *d_hist, const float *d_minmax, double *d_thr, float *d_thr
 int greater_constant(const Img &src, const Img &dst, float c, const float *d_c, cudaStream_t st);
 int binary_and(const Img &a, const Img &b, const Img &dst, cudaStream_t st);
 int mask_op(const Img &src, const Img &mask, const Img &dst, cudaStream_t st);
+
+// morph.cu
+int erode_box(const Img &src, const Img &dst, cudaStream_t st);
 int label_max(const Img &labels, uint32_t *d_max, Arena &ws, cudaStream_t st);
 size_t label_max_workspace_bytes(const Img &im);
 

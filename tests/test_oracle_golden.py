@@ -186,3 +186,42 @@ def test_blobs_statistics_table(oracle, blobs):
             assert np.isclose(np.float32(s[col].mean()), d["mean"], rtol=1e-5), col
             assert np.isclose(s[col].min(), d["min"], rtol=1e-5), col
             assert np.isclose(s[col].max(), d["max"], rtol=1e-5), col
+
+
+# ---- gauss_otsu_labeling / eroded_otsu_labeling / erode_box --------------
+def test_erode_box_golden(oracle):
+    # tests/test_erode_box.py:5-29
+    t = np.array([[0, 0, 0, 0, 0], [0, 1, 1, 1, 0], [0, 1, 1, 1, 0], [0, 1, 1, 1, 0], [0, 0, 0, 0, 0]])
+    ref = np.zeros((5, 5), np.uint8)
+    ref[2, 2] = 1
+    assert np.array_equal(oracle.erode_box(t), ref)
+
+
+def test_erode_box_clamps_at_the_edge(oracle):
+    # a full image stays full: out-of-range neighbours read the edge voxel
+    assert oracle.erode_box(np.ones((4, 5, 6))).all()
+    assert oracle.erode_box(np.ones((3, 7))).all()
+
+
+def test_gauss_otsu_labeling_golden(oracle):
+    # tests/test_gauss_otsu_labeling.py:4-41
+    src = np.array([[0, 0, 1, 1, 0, 0], [0, 1, 8, 9, 1, 0], [0, 1, 1, 0, 0, 0], [0, 0, 0, 0, 0, 0],
+                    [0, 0, 0, 1, 1, 0], [0, 0, 1, 8, 7, 1], [0, 0, 1, 1, 1, 0]])
+    ref = np.array([[0, 0, 1, 1, 0, 0], [0, 1, 1, 1, 1, 0], [0, 1, 1, 1, 0, 0], [0, 0, 0, 0, 0, 0],
+                    [0, 0, 0, 2, 2, 0], [0, 0, 2, 2, 2, 2], [0, 0, 2, 2, 2, 0]])
+    assert np.array_equal(oracle.gauss_otsu_labeling(src, 1), ref)
+
+
+def test_eroded_otsu_labeling_golden(oracle):
+    # tests/test_eroded_otsu_labeling.py:4-41 (number_of_erosions given as 1.0)
+    src = np.array([[0, 0, 5, 5, 0, 0], [0, 5, 8, 9, 1, 0], [0, 5, 7, 6, 1, 1], [0, 0, 0, 5, 5, 1],
+                    [0, 0, 0, 5, 5, 1], [0, 0, 5, 5, 5, 1], [0, 0, 5, 5, 5, 0]])
+    ref = np.array([[0, 0, 1, 1, 0, 0], [0, 1, 1, 1, 1, 0], [0, 1, 1, 1, 1, 0], [0, 0, 1, 1, 1, 0],
+                    [0, 0, 0, 2, 2, 0], [0, 0, 2, 2, 2, 0], [0, 0, 2, 2, 2, 0]])
+    assert np.array_equal(oracle.eroded_otsu_labeling(src, 1.0, 1), ref)
+
+
+@pytest.mark.parametrize("key,sigma", [("gauss_otsu_1", 1), ("gauss_otsu_5", 5)])
+def test_blobs_gauss_otsu_labeling(oracle, blobs, key, sigma):
+    # demo/segmentation/labeling.ipynb cells 13-14 through the composed oracle
+    assert _corners(oracle.gauss_otsu_labeling(blobs, sigma)) == _known()[key]["corners"]

@@ -1,0 +1,115 @@
+"""erode_box, gauss_otsu_labeling and eroded_otsu_labeling on the device
+against the oracle: binary images and label images bit for bit, on the
+reference's own fixtures, seeded random images of ragged 2D/3D shapes and
+blob images."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cle():
+    import pyclesperanto_prototype_b200 as m
+    from pyclesperanto_prototype_b200 import _build
+    _build.build()
+    return m
+
+
+SHAPES = [(1, 1), (1, 9), (9, 1), (5, 7), (33, 65), (130, 257),
+          (1, 1, 1), (1, 6, 5), (4, 1, 9), (3, 40, 33), (17, 100, 70), (40, 64, 31)]
+
+
+# ---------------------------------------------------------------- erode ---
+def test_erode_box_reference_test(cle):
+    # tests/test_erode_box.py:5-29 of the reference
+    t = cle.push(np.asarray([[0, 0, 0, 0, 0], [0, 1, 1, 1, 0], [0, 1, 1, 1, 0], [0, 1, 1, 1, 0],
+                             [0, 0, 0, 0, 0]]))
+    r = cle.create(t)
+    cle.erode_box(t, r)
+    ref = np.zeros((5, 5))
+    ref[2, 2] = 1
+    assert np.array_equal(cle.pull(r), ref)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("density", [0.6, 0.9, 1.0])
+def test_erode_box_matches_oracle(cle, oracle, shape, density):
+    a = (np.random.default_rng(3).random(shape) < density).astype(np.uint8)
+    got = cle.pull(cle.erode_box(cle.push_native(a)))
+    assert got.dtype == np.uint8
+    assert np.array_equal(got, oracle.erode_box(a))
+
+
+@pytest.mark.parametrize("src_dtype", [np.uint8, np.uint16, np.uint32, np.int32, np.float32])
+@pytest.mark.parametrize("dst_dtype", [np.uint8, np.uint16, np.uint32, np.float32])
+def test_erode_box_dtypes(cle, oracle, src_dtype, dst_dtype):
+    rng = np.random.default_rng(4)
+    a = np.where(rng.random((6, 35, 41)) < 0.85, rng.integers(1, 100, (6, 35, 41)), 0).astype(src_dtype)
+    if src_dtype == np.float32:
+        a[0, 0, :5] = [0.5, -1.0, np.nan, -0.0, 2.0]     # nonzero test on floats (NaN != 0)
+    dst = cle.create(a.shape, dst_dtype)
+    cle.erode_box(cle.push_native(a), dst)
+    got = cle.pull(dst)
+    assert got.dtype == dst_dtype
+    assert np.array_equal(got.astype(np.uint8), oracle.erode_box(a))
+
+
+# ------------------------------------------------------- gauss_otsu -------
+def test_gauss_otsu_labeling_reference_test(cle):
+    # tests/test_gauss_otsu_labeling.py:4-41 of the reference
+    src = np.asarray([[0, 0, 1, 1, 0, 0], [0, 1, 8, 9, 1, 0], [0, 1, 1, 0, 0, 0], [0, 0, 0, 0, 0, 0],
+                      [0, 0, 0, 1, 1, 0], [0, 0, 1, 8, 7, 1], [0, 0, 1, 1, 1, 0]])
+    ref = np.asarray([[0, 0, 1, 1, 0, 0], [0, 1, 1, 1, 1, 0], [0, 1, 1, 1, 0, 0], [0, 0, 0, 0, 0, 0],
+                      [0, 0, 0, 2, 2, 0], [0, 0, 2, 2, 2, 2], [0, 0, 2, 2, 2, 0]])
+    out = cle.gauss_otsu_labeling(cle.push(src), outline_sigma=1)
+    assert out.dtype == np.uint32
+    assert np.array_equal(cle.pull(out), ref)
+
+
+def _blob_image(shape, seed):
+    rng = np.random.default_rng(seed)
+    img = rng.normal(10, 3, shape).clip(0)
+    grids = np.meshgrid(*[np.arange(s) for s in shape], indexing="ij")
+    for _ in range(max(3, int(np.prod(shape) / 1500))):
+        c = [rng.uniform(0, s) for s in shape]
+        r2 = sum((g - ci) ** 2 for g, ci in zip(grids, c))
+        img += rng.uniform(100, 250) * np.exp(-r2 / (2 * rng.uniform(2, 5) ** 2))
+    return rng.poisson(img).astype(np.float32)
+
+
+@pytest.mark.parametrize("shape,sigma", [((64, 80), 1.0), ((200, 150), 2.0), ((256, 256), 5.0),
+                                         ((20, 60, 70), 1.0), ((33, 80, 65), 2.0)])
+def test_gauss_otsu_labeling_matches_oracle(cle, oracle, shape, sigma):
+    img = _blob_image(shape, 11)
+    got = cle.pull(cle.gauss_otsu_labeling(img, outline_sigma=sigma))
+    ref = oracle.gauss_otsu_labeling(img, sigma)
+    assert ref.max() > 0
+    assert np.array_equal(got, ref)
+
+
+def test_gauss_otsu_labeling_uint16_input(cle, oracle):
+    # a uint16 volume is blurred in place of its float32 copy: same labels
+    img = _blob_image((24, 70, 66), 12).clip(0, 65535).astype(np.uint16)
+    got = cle.pull(cle.gauss_otsu_labeling(img, outline_sigma=2))
+    assert np.array_equal(got, oracle.gauss_otsu_labeling(img.astype(np.float32), 2))
+
+
+# ----------------------------------------------------- eroded_otsu --------
+def test_eroded_otsu_labeling_reference_test(cle):
+    # tests/test_eroded_otsu_labeling.py:4-41 of the reference
+    src = np.asarray([[0, 0, 5, 5, 0, 0], [0, 5, 8, 9, 1, 0], [0, 5, 7, 6, 1, 1], [0, 0, 0, 5, 5, 1],
+                      [0, 0, 0, 5, 5, 1], [0, 0, 5, 5, 5, 1], [0, 0, 5, 5, 5, 0]])
+    ref = np.asarray([[0, 0, 1, 1, 0, 0], [0, 1, 1, 1, 1, 0], [0, 1, 1, 1, 1, 0], [0, 0, 1, 1, 1, 0],
+                      [0, 0, 0, 2, 2, 0], [0, 0, 2, 2, 2, 0], [0, 0, 2, 2, 2, 0]])
+    out = cle.eroded_otsu_labeling(cle.push(src), number_of_erosions=1.0, outline_sigma=1)
+    assert np.array_equal(cle.pull(out), ref)
+
+
+@pytest.mark.parametrize("shape,erosions,sigma", [((64, 80), 0, 1.0), ((200, 150), 2, 1.0),
+                                                  ((256, 256), 5, 2.0), ((20, 60, 70), 1, 1.0),
+                                                  ((33, 80, 65), 3, 2.0), ((30, 50, 40), 40, 1.0)])
+def test_eroded_otsu_labeling_matches_oracle(cle, oracle, shape, erosions, sigma):
+    img = _blob_image(shape, 13)
+    got = cle.pull(cle.eroded_otsu_labeling(img, number_of_erosions=erosions, outline_sigma=sigma))
+    assert np.array_equal(got, oracle.eroded_otsu_labeling(img, erosions, sigma))
