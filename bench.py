@@ -53,6 +53,10 @@ WORKLOADS = {
     "lightsheet": dict(desc="light-sheet volume uint16 512x1024x1024 (30000 ellipsoids, sinusoidal background, "
                             "Poisson, seed 2): voronoi_otsu_labeling(spot_sigma=2, outline_sigma=2) + "
                             "statistics_of_labelled_pixels", shape=(512, 1024, 1024), spot=2.0, outline=2.0),
+    "lightsheet_dense": dict(desc="light-sheet volume uint16 512x1024x1024 (as above): gauss_otsu_labeling("
+                                  "outline_sigma=2) (blur, Otsu, connected components of the dense mask) + "
+                                  "statistics_of_labelled_pixels", shape=(512, 1024, 1024), spot=None,
+                             outline=2.0, op="gauss_otsu"),
     "batch": dict(desc="512 tiles, voxel counts log-uniform between 2D 64x64 and 3D 96x512x512 (2D and 3D "
                        "mixed), Gaussian-blob tiles with U(0.5,5)e-4 blobs/voxel and per-tile seeds (4+i); "
                        "voronoi_otsu_labeling(spot_sigma=3.5, outline_sigma=1) on float32 tiles, uint32 labels",
@@ -89,6 +93,22 @@ MEASURED_TRAFFIC = {
 }
 
 
+# Algorithmic bytes per voxel of a whole gauss_otsu_labeling + statistics step
+# (u16 source): blur 2+4, min/max 4, histogram 4, threshold 4+1, CCL of the
+# dense mask 1+4, two statistics passes 2 x (4+2).
+DENSE_BYTES_PER_VOXEL = 6 + 4 + 4 + 5 + 5 + 12
+
+
+def cpu_step(f, w):
+    """One step of the workload on the oracle (f: float32 host volume)."""
+    import oracle
+    if w.get("op") == "gauss_otsu":
+        lab = oracle.gauss_otsu_labeling(f, w["outline"])
+    else:
+        lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
+    oracle.statistics_of_labelled_pixels(f, lab)
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -105,7 +125,9 @@ def make_input(name, device=None):
         return synthetic.cached("c2_nuclei_128x512x512_s1", synthetic.nuclei_volume)
     if name == "blobs2d":
         return synthetic.blobs_2d((256, 256), 60, seed=0)
-    vol = synthetic.lightsheet_volume(w["shape"], 30000, seed=2, device=device)
+    import torch
+    dev = device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu")
+    vol = synthetic.lightsheet_volume(w["shape"], 30000, seed=2, device=dev)
     return vol
 
 
@@ -197,7 +219,7 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def cpu_baseline_sample(vol, spot, outline, reps=2, max_voxels=48 * 1024 * 1024):
+def cpu_baseline_sample(vol, w, reps=2, max_voxels=48 * 1024 * 1024):
     """Oracle on the host cores (all threads); returns (Mvox/s, cores, voxels,
     seconds).  Volumes above max_voxels are sampled as their first z planes."""
     import oracle
@@ -209,8 +231,7 @@ def cpu_baseline_sample(vol, spot, outline, reps=2, max_voxels=48 * 1024 * 1024)
     ts = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        lab = oracle.voronoi_otsu_labeling(f, spot, outline)
-        oracle.statistics_of_labelled_pixels(f, lab)
+        cpu_step(f, w)
         ts.append(time.perf_counter() - t0)
     t = min(ts)
     return f.size / t / 1e6, cores, f.shape, t
@@ -238,13 +259,19 @@ def run_b200(args):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     labels = cle.create_labels_like(src)
 
+    dense = w.get("op") == "gauss_otsu"
+
     def step():
-        cle._ops._vol(src, labels, w["spot"], w["outline"], check=False)
+        if dense:
+            cle.gauss_otsu_labeling(src, labels, outline_sigma=w["outline"])
+        else:
+            cle._ops._vol(src, labels, w["spot"], w["outline"], check=False)
         L = cle._ops._label_max(labels)
         return cle.statistics_table(src, labels, L), L
 
     # correctness of the loop status once (not timed)
-    cle._ops._vol(src, labels, w["spot"], w["outline"], check=True)
+    if not dense:
+        cle._ops._vol(src, labels, w["spot"], w["outline"], check=True)
     # clocks are sampled from the start of the warm-up (under load) through
     # the timed region; short runs add untimed steps until 3 samples exist
     clocks = ClockSampler(local)
@@ -294,7 +321,10 @@ def run_b200(args):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             img = cle.push_native(pinned_in)
-            lab = cle.voronoi_otsu_labeling(img, spot_sigma=w["spot"], outline_sigma=w["outline"])
+            if dense:
+                lab = cle.gauss_otsu_labeling(img, outline_sigma=w["outline"])
+            else:
+                lab = cle.voronoi_otsu_labeling(img, spot_sigma=w["spot"], outline_sigma=w["outline"])
             stats = cle.statistics_of_labelled_pixels(img, lab)
             pinned_lab.copy_(lab.tensor, non_blocking=True)
             torch.cuda.synchronize()
@@ -311,12 +341,17 @@ def run_b200(args):
     sm = np.array([s + [0.0] * (12 - len(s)) for s in stage_ms])[:, :12]
     mean_stage = sm.mean(axis=0)
     cands = [(mean_stage[i], STAGES[i]) for i in range(12) if STAGES[i] in ALGO_BYTES]
-    t_dom, dom = max(cands)
     peak, peak_kind = load_peaks()
-    achieved = ALGO_BYTES[dom] * nvox / (t_dom / 1e3) / 1e9
+    if dense:
+        # no stage events on this composition: the whole step against the peak
+        dom, t_dom, bpv = "gauss_otsu_labeling + statistics (whole step)", ms_per_step, DENSE_BYTES_PER_VOXEL
+    else:
+        t_dom, dom = max(cands)
+        bpv = ALGO_BYTES[dom]
+    achieved = bpv * nvox / (t_dom / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes_per_voxel": ALGO_BYTES[dom]}
+                "traffic": None, "algorithmic_bytes_per_voxel": bpv}
     tr = MEASURED_TRAFFIC.get(args.workload, {}).get(dom)
     if tr:
         roofline["traffic"] = tr[0]
@@ -326,15 +361,16 @@ def run_b200(args):
                       for name in ALGO_BYTES if stages.get(name)}
     # the whole pipeline against the same peak: every stage's algorithmic
     # bytes over the step time
-    pipe_bytes = sum(ALGO_BYTES.values()) * nvox
-    pipeline_roofline = {"bytes_per_voxel": sum(ALGO_BYTES.values()),
+    bpv_pipe = DENSE_BYTES_PER_VOXEL if dense else sum(ALGO_BYTES.values())
+    pipe_bytes = bpv_pipe * nvox
+    pipeline_roofline = {"bytes_per_voxel": bpv_pipe,
                          "achieved": round(pipe_bytes / (ms_per_step / 1e3) / 1e9, 1),
                          "frac": round(pipe_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4)}
     lat = np.array(times)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and host_np is not None:
-        v, cores, shp, t = cpu_baseline_sample(host_np, w["spot"], w["outline"])
+        v, cores, shp, t = cpu_baseline_sample(host_np, w)
         what = "full workload" if int(np.prod(shp)) == nvox else "first %d z planes of the workload" % shp[0]
         cpu = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{what} ({'x'.join(map(str, shp))} voxels) per repetition, best of 2, {t:.2f} s"}
@@ -496,31 +532,26 @@ def run_reference(args):
     import oracle
     oracle.build()
     w = WORKLOADS[args.workload]
-    if args.workload == "lightsheet":
-        print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement needs hours per step "
-                          "on this workload; timed on the nuclei workload instead"}))
-        return
     host = make_input(args.workload)
+    if hasattr(host, "cpu"):
+        host = host.cpu().numpy()
     f = host.astype(np.float32)
     cores = oracle.num_threads()
     # one untimed full step sizes the per-step sample so the run stays short
     t0 = time.perf_counter()
-    lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
-    oracle.statistics_of_labelled_pixels(f, lab)
-    t_full = time.perf_counter() - t0
+    cpu_step(f if f.ndim == 2 or f.shape[0] <= 128 else f[:32], w)
+    t_full = (time.perf_counter() - t0) * (1 if f.ndim == 2 or f.shape[0] <= 128 else f.shape[0] / 32)
     budget = 150.0
     if f.ndim == 3 and t_full * (args.steps + args.warmup) > budget:
         planes = max(8, int(f.shape[0] * budget / (t_full * (args.steps + args.warmup))))
         f = np.ascontiguousarray(f[:planes])
     sample = f"{f.shape} slab of the workload per step" if f.shape != host.shape else "full workload per step"
     for _ in range(args.warmup):
-        lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
-        oracle.statistics_of_labelled_pixels(f, lab)
+        cpu_step(f, w)
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        lab = oracle.voronoi_otsu_labeling(f, w["spot"], w["outline"])
-        oracle.statistics_of_labelled_pixels(f, lab)
+        cpu_step(f, w)
         ts.append(time.perf_counter() - t0)
     total = sum(ts)
     v = f.size * args.steps / total / 1e6

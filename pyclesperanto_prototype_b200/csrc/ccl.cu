@@ -63,24 +63,84 @@ __device__ __forceinline__ void union_back(uint32_t *lab, const Geo &g, uint32_t
             }
 }
 
+// ---- dense labelling on row runs ------------------------------------------
+// A warp covers one row segment: 32 consecutive x of one (z, y) row.  In a
+// row, x-major keys grow with x, so the first voxel of a run holds the run's
+// smallest key: init links every foreground voxel straight to the start of
+// its run inside the segment.  The union step then joins whole runs: a run
+// [a, b] of the segment is united once with every run of each backward row
+// ((y-1, z) and (y-1..y+1, z-1)) that overlaps it (through the first voxel of
+// the overlap), with a run of that row that touches it only diagonally at
+// a-1 or b+1, and with the run that continues it from the previous segment.
+// That is every 26-neighbour contact (each adjacent pair has one backward
+// side), with a few unions per run instead of 13 per voxel.
+constexpr int kRowWarps = 8;   // warps (row segments in flight) per CTA
+
+struct Rows {
+    uint32_t WS;     // segments per row
+    FastDiv fWS;
+    uint32_t nseg;   // D * H * WS
+};
+
 template <typename T>
-__global__ void ccl_init_kernel(const T *__restrict__ bin, uint32_t *__restrict__ lab, Geo g,
-                                int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t x, y, z;
-        m2xyz(g, (uint32_t)i, x, y, z);
-        lab[i] = (bin[i] != (T)0) ? xyz2k(g, x, y, z) + 1u : 0u;
+__global__ void __launch_bounds__(kRowWarps * 32)
+ccl_init_rows(const T *__restrict__ bin, uint32_t *__restrict__ lab, Geo g, Rows R) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s = blockIdx.x * kRowWarps + (threadIdx.x >> 5); s < R.nseg; s += gridDim.x * kRowWarps) {
+        const uint32_t r = R.fWS.div(s), xs = s - r * R.WS;       // r = z * H + y
+        const uint32_t z = g.fH.div(r), y = r - z * g.H;
+        const uint32_t x = xs * 32u + (uint32_t)lane;
+        const bool in = x < g.W;
+        const bool fg = in && bin[r * g.W + x] != (T)0;
+        const unsigned F = __ballot_sync(0xffffffffu, fg);
+        const unsigned starts = F & ~(F << 1);                    // fg lanes after a bg lane (or lane 0)
+        if (in) {
+            uint32_t v = 0u;
+            if (fg) {
+                const uint32_t a = 31u - __clz(starts & (0xffffffffu >> (31 - lane)));   // run start lane
+                v = xyz2k(g, xs * 32u + a, y, z) + 1u;
+            }
+            lab[r * g.W + x] = v;
+        }
     }
 }
 
-__global__ void ccl_union_dense(uint32_t *lab, Geo g, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (!ld_cg(lab + i)) continue;
-        uint32_t x, y, z;
-        m2xyz(g, (uint32_t)i, x, y, z);
-        union_back(lab, g, x, y, z);
+__global__ void __launch_bounds__(kRowWarps * 32)
+ccl_union_rows(uint32_t *lab, Geo g, Rows R) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t xstep = g.H * g.D;                             // key distance of x +- 1
+    for (uint32_t s = blockIdx.x * kRowWarps + (threadIdx.x >> 5); s < R.nseg; s += gridDim.x * kRowWarps) {
+        const uint32_t r = R.fWS.div(s), xs = s - r * R.WS;
+        const uint32_t z = g.fH.div(r), y = r - z * g.H;
+        const uint32_t x = xs * 32u + (uint32_t)lane;
+        const bool in = x < g.W;
+        // foreground-ness never changes while parents are relinked
+        const bool fg = in && ld_cg(lab + r * g.W + x) != 0u;
+        const unsigned F = __ballot_sync(0xffffffffu, fg);
+        if (!F) continue;
+        const bool is_start = (F & ~(F << 1)) >> lane & 1u;
+        const bool is_end = (F & ~(F >> 1)) >> lane & 1u;
+        const uint32_t kp = xyz2k(g, x, y, z);
+        // the run continued from the previous segment
+        if (lane == 0 && fg && xs > 0 && ld_cg(lab + r * g.W + x - 1u) != 0u) unite(lab, g, kp, kp - xstep);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int qy = (int)y + (k == 0 ? -1 : k - 2), qz = (int)z - (k == 0 ? 0 : 1);
+            if (qy < 0 || qy >= (int)g.H || qz < 0) continue;    // warp-uniform
+            const uint32_t *row = lab + ((uint32_t)qz * g.H + (uint32_t)qy) * g.W;
+            const bool q = in && ld_cg(row + x) != 0u;
+            bool qe = false;                                     // lane 0: row[x-1], lane 31: row[x+1]
+            if (lane == 0 && xs > 0) qe = ld_cg(row + x - 1u) != 0u;
+            if (lane == 31 && x + 1u < g.W) qe = ld_cg(row + x + 1u) != 0u;
+            const unsigned Q = __ballot_sync(0xffffffffu, q);
+            const bool qL = (lane == 0) ? qe : ((Q >> (lane - 1)) & 1u);
+            const bool qR = (lane == 31) ? qe : ((Q >> (lane + 1)) & 1u);
+            if (!fg) continue;
+            const uint32_t kq = xyz2k(g, x, (uint32_t)qy, (uint32_t)qz);
+            if (q && (is_start || !qL)) unite(lab, g, kp, kq);            // first voxel of an overlap
+            if (is_start && qL && !q) unite(lab, g, kp, kq - xstep);     // diagonal contact at a-1
+            if (is_end && qR && !q) unite(lab, g, kp, kq + xstep);       // diagonal contact at b+1
+        }
     }
 }
 
@@ -265,9 +325,9 @@ int rank_build(const Rank &r, cudaStream_t st) {
 }
 
 template <typename T>
-int launch_ccl_init(const Img &bin, uint32_t *lab, const Geo &g, cudaStream_t st) {
-    const int64_t n = bin.n();
-    ccl_init_kernel<T><<<launch_blocks(n, kT), kT, 0, st>>>((const T *)bin.data, lab, g, n);
+int launch_ccl_init(const Img &bin, uint32_t *lab, const Geo &g, const Rows &R, int blocks,
+                    cudaStream_t st) {
+    ccl_init_rows<T><<<blocks, kRowWarps * 32, 0, st>>>((const T *)bin.data, lab, g, R);
     CLE_LAUNCH_CHECK("ccl init");
     return CLE_OK;
 }
@@ -347,15 +407,20 @@ int ccl_dense(const Img &bin, uint32_t *lab, Arena &ws, cudaStream_t st) {
     Rank r = take_rank(ws, fkey_bits_for(n));
     if (!ws.ok()) { set_error("connected_components_labeling_box: workspace too small"); return CLE_ERR_WORKSPACE; }
     const Geo g = make_geo(bin);
+    Rows R;
+    R.WS = (uint32_t)((bin.W + 31) / 32);
+    R.fWS = FastDiv(R.WS);
+    R.nseg = (uint32_t)(bin.D * bin.H) * R.WS;
+    const int rb = launch_blocks((int64_t)R.nseg * 32, kRowWarps * 32);
     switch (bin.dtype) {
-        case CLE_U8: CLE_TRY(launch_ccl_init<uint8_t>(bin, lab, g, st)); break;
-        case CLE_U32: CLE_TRY(launch_ccl_init<uint32_t>(bin, lab, g, st)); break;
-        case CLE_F32: CLE_TRY(launch_ccl_init<float>(bin, lab, g, st)); break;
-        case CLE_U16: CLE_TRY(launch_ccl_init<uint16_t>(bin, lab, g, st)); break;
+        case CLE_U8: CLE_TRY(launch_ccl_init<uint8_t>(bin, lab, g, R, rb, st)); break;
+        case CLE_U32: CLE_TRY(launch_ccl_init<uint32_t>(bin, lab, g, R, rb, st)); break;
+        case CLE_F32: CLE_TRY(launch_ccl_init<float>(bin, lab, g, R, rb, st)); break;
+        case CLE_U16: CLE_TRY(launch_ccl_init<uint16_t>(bin, lab, g, R, rb, st)); break;
         default: set_error("connected_components_labeling_box: unsupported dtype %d", bin.dtype); return CLE_ERR_DTYPE;
     }
     const int b = launch_blocks(n, kT);
-    ccl_union_dense<<<b, kT, 0, st>>>(lab, g, n);
+    ccl_union_rows<<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
     ccl_flatten_dense<<<b, kT, 0, st>>>(lab, g, n);
     CLE_CUDA(cudaMemsetAsync(r.bitmap, 0, sizeof(uint32_t) * r.words, st));
     ccl_mark_dense<<<b, kT, 0, st>>>(lab, g, n, r.bitmap);

@@ -28,6 +28,7 @@ static constexpr int kMaxStages = 16;
 static thread_local cudaEvent_t g_ev[kMaxStages];
 static thread_local bool g_prof = false;
 static thread_local int g_marks = 0;
+static thread_local unsigned g_recorded = 0;   // bit i: event i recorded since the last mark 0
 
 static thread_local void *g_trace = nullptr;
 static thread_local size_t g_trace_bytes = 0;
@@ -79,10 +80,15 @@ int profile_enable(int flags) {
 void stage_mark(int i, cudaStream_t st) {
     if (!g_prof || i < 0 || i >= kMaxStages) return;
     cudaEventRecord(g_ev[i], st);
-    if (i == 0) g_marks = 1;
-    else if (i + 1 > g_marks) g_marks = i + 1;
+    if (i == 0) { g_marks = 1; g_recorded = 1u; }
+    else {
+        if (i + 1 > g_marks) g_marks = i + 1;
+        g_recorded |= 1u << i;
+    }
 }
 
+// Interval i-1 -> i in ms for every mark pair recorded (0 where either mark
+// was not recorded, e.g. a call that runs only some of the stages).
 int stage_ms(float *out, int max) {
     if (!g_prof || g_marks < 2) return 0;
     cudaError_t e = cudaEventSynchronize(g_ev[g_marks - 1]);
@@ -90,7 +96,11 @@ int stage_ms(float *out, int max) {
     int n = 0;
     for (int i = 1; i < g_marks && n < max; ++i, ++n) {
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, g_ev[i - 1], g_ev[i]);
+        const unsigned pair = (1u << (i - 1)) | (1u << i);
+        if ((g_recorded & pair) == pair && cudaEventElapsedTime(&ms, g_ev[i - 1], g_ev[i]) != cudaSuccess) {
+            (void)cudaGetLastError();   // leave no error behind for the next launch check
+            ms = 0.f;
+        }
         out[n] = ms;
     }
     return n;
