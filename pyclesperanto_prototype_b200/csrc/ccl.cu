@@ -32,10 +32,29 @@ __device__ __forceinline__ uint32_t find_root(const uint32_t *lab, const Geo &g,
     return k;
 }
 
+// find_root with path halving, for the union phase: a visited non-root
+// entry is lowered to its grandparent with atomicMin.  Entries only ever move
+// to an ancestor in the same tree and roots are never touched, so concurrent
+// unions (which link roots only) are unaffected.
+__device__ __forceinline__ uint32_t find_root_halve(uint32_t *lab, const Geo &g, uint32_t k) {
+    uint32_t mk = k2m(g, k);
+    uint32_t p = ld_cg(lab + mk) - 1u;
+    while (p != k) {
+        const uint32_t mp = k2m(g, p);
+        const uint32_t gp = ld_cg(lab + mp) - 1u;
+        if (gp == p) return p;
+        atomicMin(lab + mk, gp + 1u);
+        k = gp;
+        mk = k2m(g, k);
+        p = ld_cg(lab + mk) - 1u;
+    }
+    return k;
+}
+
 __device__ __forceinline__ void unite(uint32_t *lab, const Geo &g, uint32_t a, uint32_t b) {
     for (;;) {
-        a = find_root(lab, g, a);
-        b = find_root(lab, g, b);
+        a = find_root_halve(lab, g, a);
+        b = find_root_halve(lab, g, b);
         if (a == b) return;
         if (a < b) { uint32_t t = a; a = b; b = t; }
         // link root a (larger key) under b
@@ -118,9 +137,13 @@ ccl_union_rows(uint32_t *lab, Geo g, Rows R) {
         const bool fg = in && ld_cg(lab + r * g.W + x) != 0u;
         const unsigned F = __ballot_sync(0xffffffffu, fg);
         if (!F) continue;
-        const bool is_start = (F & ~(F << 1)) >> lane & 1u;
+        const unsigned starts = F & ~(F << 1);
+        const bool is_start = starts >> lane & 1u;
         const bool is_end = (F & ~(F >> 1)) >> lane & 1u;
         const uint32_t kp = xyz2k(g, x, y, z);
+        // unions start from the run's first voxel (every run voxel points at it)
+        const uint32_t a = fg ? 31u - __clz(starts & (0xffffffffu >> (31 - lane))) : (uint32_t)lane;
+        const uint32_t ka = kp - ((uint32_t)lane - a) * xstep;
         // the run continued from the previous segment
         if (lane == 0 && fg && xs > 0 && ld_cg(lab + r * g.W + x - 1u) != 0u) unite(lab, g, kp, kp - xstep);
 #pragma unroll
@@ -137,20 +160,33 @@ ccl_union_rows(uint32_t *lab, Geo g, Rows R) {
             const bool qR = (lane == 31) ? qe : ((Q >> (lane + 1)) & 1u);
             if (!fg) continue;
             const uint32_t kq = xyz2k(g, x, (uint32_t)qy, (uint32_t)qz);
-            if (q && (is_start || !qL)) unite(lab, g, kp, kq);            // first voxel of an overlap
-            if (is_start && qL && !q) unite(lab, g, kp, kq - xstep);     // diagonal contact at a-1
-            if (is_end && qR && !q) unite(lab, g, kp, kq + xstep);       // diagonal contact at b+1
+            if (q && (is_start || !qL)) unite(lab, g, ka, kq);            // first voxel of an overlap
+            if (is_start && qL && !q) unite(lab, g, ka, kq - xstep);     // diagonal contact at a-1
+            if (is_end && qR && !q) unite(lab, g, ka, kq + xstep);       // diagonal contact at b+1
         }
     }
 }
 
-__global__ void ccl_flatten_dense(uint32_t *lab, Geo g, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t v = ld_cg(lab + i);
-        if (!v) continue;
-        uint32_t r = find_root(lab, g, v - 1u);
-        if (r != v - 1u) st_cg(lab + i, r + 1u);
+// Flatten on row runs: the run-start lane of each run (whose voxels all
+// point at it after init) walks to the root; its run gets the root by shuffle.
+// The forest no longer changes here except that entries move to their roots.
+__global__ void __launch_bounds__(kRowWarps * 32)
+ccl_flatten_rows(uint32_t *lab, Geo g, Rows R) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t s = blockIdx.x * kRowWarps + (threadIdx.x >> 5); s < R.nseg; s += gridDim.x * kRowWarps) {
+        const uint32_t r = R.fWS.div(s), xs = s - r * R.WS;
+        const uint32_t z = g.fH.div(r), y = r - z * g.H;
+        const uint32_t x = xs * 32u + (uint32_t)lane;
+        const bool in = x < g.W;
+        const uint32_t v = in ? ld_cg(lab + r * g.W + x) : 0u;
+        const unsigned F = __ballot_sync(0xffffffffu, v != 0u);
+        if (!F) continue;
+        const unsigned starts = F & ~(F << 1);
+        uint32_t root = 0u;
+        if ((starts >> lane) & 1u) root = find_root(lab, g, xyz2k(g, x, y, z)) + 1u;
+        const int a = (v != 0u) ? 31 - __clz(starts & (0xffffffffu >> (31 - lane))) : lane;
+        root = __shfl_sync(0xffffffffu, root, a);
+        if (v != 0u && root != v) st_cg(lab + r * g.W + x, root);
     }
 }
 
@@ -421,7 +457,7 @@ int ccl_dense(const Img &bin, uint32_t *lab, Arena &ws, cudaStream_t st) {
     }
     const int b = launch_blocks(n, kT);
     ccl_union_rows<<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
-    ccl_flatten_dense<<<b, kT, 0, st>>>(lab, g, n);
+    ccl_flatten_rows<<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
     CLE_CUDA(cudaMemsetAsync(r.bitmap, 0, sizeof(uint32_t) * r.words, st));
     ccl_mark_dense<<<b, kT, 0, st>>>(lab, g, n, r.bitmap);
     CLE_LAUNCH_CHECK_N("ccl dense", 3);
