@@ -57,6 +57,9 @@ WORKLOADS = {
                                   "outline_sigma=2) (blur, Otsu, connected components of the dense mask) + "
                                   "statistics_of_labelled_pixels", shape=(512, 1024, 1024), spot=None,
                              outline=2.0, op="gauss_otsu"),
+    "published": dict(desc="the reference's own published benchmark cases (benchmarks/*.ipynb): "
+                           "seeded inputs of the notebooks' shapes and distributions", shape=None,
+                      spot=None, outline=None),
     "batch": dict(desc="512 tiles, voxel counts log-uniform between 2D 64x64 and 3D 96x512x512 (2D and 3D "
                        "mixed), Gaussian-blob tiles with U(0.5,5)e-4 blobs/voxel and per-tile seeds (4+i); "
                        "voronoi_otsu_labeling(spot_sigma=3.5, outline_sigma=1) on float32 tiles, uint32 labels",
@@ -525,6 +528,105 @@ def run_served(args):
     print(json.dumps(out), flush=True)
 
 
+def _tissue_2d(width, height, dx, dy, seed):
+    """Label image of a jittered-grid Voronoi tessellation (the shape of
+    artificial_tissue_2d: one cell per dx x dy grid cell)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    gy, gx = np.mgrid[dy / 2:height:dy, dx / 2:width:dx]
+    pts = np.stack([gy.ravel(), gx.ravel()], 1) + rng.uniform(-0.3, 0.3, (gy.size, 2)) * [dy, dx]
+    yy, xx = np.mgrid[0:height, 0:width]
+    _, idx = cKDTree(pts).query(np.stack([yy.ravel(), xx.ravel()], 1))
+    return (idx.reshape(height, width) + 1).astype(np.float32)
+
+
+def _spheres(n, size, radius, seed):
+    rng = np.random.default_rng(seed)
+    img = np.zeros((size, size, size), np.uint8)
+    r = int(radius)
+    zz, yy, xx = np.mgrid[-r:r + 1, -r:r + 1, -r:r + 1]
+    ball = zz * zz + yy * yy + xx * xx <= radius * radius
+    for c in (rng.random((n, 3)) * size).astype(int):
+        lo, hi = np.maximum(c - r, 0), np.minimum(c + r + 1, size)
+        b = ball[lo[0] - c[0] + r:hi[0] - c[0] + r, lo[1] - c[1] + r:hi[1] - c[1] + r,
+                 lo[2] - c[2] + r:hi[2] - c[2] + r]
+        img[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] |= b
+    return img.astype(np.float32)
+
+
+def run_published(args):
+    """Times the cases the reference's notebooks publish
+    on seeded inputs of the same shape and distribution, inputs resident on the
+    device: CUDA-event time per call and wall time with a synchronize."""
+    import torch
+    import pyclesperanto_prototype_b200 as cle
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(7)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    tissue = _tissue_2d(2048, 1024, 128, 96, 8)
+    cases = [
+        ("voronoi_otsu_labeling 2048x2048 uniform random, spot_sigma=outline_sigma=1",
+         lambda: cle.push(rng.random((2048, 2048))), lambda a, o: cle.voronoi_otsu_labeling(a, o, 1, 1),
+         cle.create_labels_like, 530.0, "Apple M1 Max CPU, OpenCL (benchmarks/apple_m1_voronoi_otsu_labeling.ipynb)"),
+        ("gaussian_blur sigma=2, 64x1024x1024 uniform random",
+         lambda: cle.push(rng.random((64, 1024, 1024))), lambda a, o: cle.gaussian_blur(a, o, 2, 2, 2),
+         cle.create_like, 49.8, "RTX 2070 (benchmarks/benchmarking_some_operations.ipynb)"),
+        ("gaussian_blur sigma=10, 64x1024x1024 uniform random",
+         lambda: cle.push(rng.random((64, 1024, 1024))), lambda a, o: cle.gaussian_blur(a, o, 10, 10, 10),
+         cle.create_like, 134.1, "RTX 2070 (benchmarks/benchmarking_some_operations.ipynb)"),
+        ("gaussian_blur sigma=10, 100x512x512 uniform random",
+         lambda: cle.push(rng.random((100, 512, 512))), lambda a, o: cle.gaussian_blur(a, o, 10, 10, 10),
+         cle.create_like, 214.0, "RTX 3050 Ti Laptop (benchmarks/gaussian_blur.ipynb)"),
+        ("histogram 256 bins with min/max, 100x1024x1024 normal",
+         lambda: cle.push(rng.normal(size=(100, 1024, 1024))), lambda a, o: cle.histogram(a, num_bins=256),
+         None, 140.0, "RTX 3050 Ti Laptop (benchmarks/histograms.ipynb)"),
+        ("threshold_otsu 100x512x512 uniform random",
+         lambda: cle.push(rng.random((100, 512, 512))), lambda a, o: cle.threshold_otsu(a, o),
+         cle.create_binary_like, 38.0, "RTX 2070 (benchmarks/threshold_otsu.ipynb, best of 38-50 ms)"),
+        ("connected_components_labeling_box 400^3, 200 balls of radius 10",
+         lambda: cle.push(_spheres(200, 400, 10, 9)), lambda a, o: cle.connected_components_labeling_box(a, o),
+         cle.create_labels_like, 98.0, "RTX 2080 Ti (benchmarks/connected_component_labeling.ipynb, best of 98-156 ms)"),
+        ("statistics_of_labelled_pixels 2048x1024 tissue labels (intensity None)",
+         lambda: cle.push(tissue), lambda a, o: cle.statistics_of_labelled_pixels(None, a),
+         None, 39.0, "RTX 2070 (benchmarks/statistics_of_labeled_pixels.ipynb)"),
+        ("statistics_of_labelled_pixels 128x1024x1024 (the tissue stacked, intensity None)",
+         lambda: cle.push(np.broadcast_to(tissue[:, :1024], (128, 1024, 1024)).copy()),
+         lambda a, o: cle.statistics_of_labelled_pixels(None, a),
+         None, 765.0, "RTX 2070 (benchmarks/statistics_of_labeled_pixels.ipynb)"),
+    ]
+    out_cases = []
+    for name, make, call, creator, pub_ms, pub_hw in cases:
+        a = make()
+        o = creator(a) if creator else None
+        for _ in range(args.warmup):
+            call(a, o)
+        torch.cuda.synchronize()
+        dev, wall = [], []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            call(a, o)
+            e1.record(stream)
+            e1.synchronize()
+            wall.append((time.perf_counter() - t0) * 1e3)
+            dev.append(e0.elapsed_time(e1))
+        d, w = float(np.median(dev)), float(np.median(wall))
+        out_cases.append({"case": name, "ms_device": round(d, 3), "ms_wall": round(w, 3),
+                          "published_ms": pub_ms, "published_hardware": pub_hw,
+                          "wall_speedup_vs_published": round(pub_ms / w, 1)})
+        del a, o
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "ms per call on the reference's published benchmark cases", "impl": "b200",
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+                      "config": {"workload": WORKLOADS["published"]["desc"],
+                                 "timing": "median over steps; L2 flushed between calls; inputs resident"},
+                      "cases": out_cases}), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -532,6 +634,11 @@ def run_reference(args):
     import oracle
     oracle.build()
     w = WORKLOADS[args.workload]
+    if args.workload in ("batch", "served", "published"):
+        print(json.dumps({"impl": "reference", "workload": args.workload,
+                          "note": "the CPU arm times the single-volume workloads (nuclei, lightsheet, "
+                                  "lightsheet_dense, blobs2d); run it with one of those"}), flush=True)
+        return
     host = make_input(args.workload)
     if hasattr(host, "cpu"):
         host = host.cpu().numpy()
@@ -589,6 +696,8 @@ def main():
         run_batch(args)
     elif args.workload == "served":
         run_served(args)
+    elif args.workload == "published":
+        run_published(args)
     else:
         run_b200(args)
 
