@@ -500,7 +500,8 @@ def run_served(args):
     def make():
         return [Request(i, pool[c][j], arrival=a) for i, (a, c, j) in enumerate(trace)]
     warm = [Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)]
-    server = SegmentationServer(budget_bytes=60e9, slots=args.lanes, spot_sigma=w["spot"],
+    server = SegmentationServer(budget_bytes=60e9, slots=args.lanes, compute_streams=args.compute_streams,
+                                spot_sigma=w["spot"],
                                 outline_sigma=w["outline"])
     server.run(warm, realtime=False)
     per_call_loop([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)], w["spot"],
@@ -520,7 +521,8 @@ def run_served(args):
     out = {"metric": METRIC, "value": s["mvoxels_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(trace),
            "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "b200",
-           "form": "served (continuous batching, %d slots, 60 GB budget)" % args.lanes,
+           "form": "served (continuous batching: %d requests in flight, uploads and downloads on copy "
+                   "streams overlapping %d compute stream(s), 60 GB budget)" % (args.lanes, args.compute_streams),
            "config": {"workload": w["desc"], "rate_per_s": args.rate, "duration_s": args.duration,
                       "volumes": "%d pre-generated per size class, reused" % pool_per_class},
            "served": s, "per_call_loop": p, "label_counts_equal": bool(same),
@@ -687,6 +689,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=8, help="batch/served: concurrent lanes (slots)")
     ap.add_argument("--duration", type=float, default=60.0, help="served workload: trace length in s")
     ap.add_argument("--rate", type=float, default=200.0, help="served workload: arrivals per s")
+    ap.add_argument("--compute-streams", type=int, default=1, help="served workload: compute streams")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -1,16 +1,26 @@
 """Served form: continuous batching of segmentation requests on one GPU.
 
-A request is a volume in (pinned) host memory.  The server keeps K slots --
-one CUDA stream each -- and admits a waiting request as soon as a slot is
-free and its device memory fits in the HBM budget: the input copy, the
-pipeline (voronoi_otsu_labeling, then statistics_of_labelled_pixels reading
-the label count the pipeline left on the device, with no host round trip)
-and the copy of the statistics table run on the slot's stream, overlapping
-with the requests on the other slots.  Device buffers (input, labels,
-workspaces, tables) are kept per shape and reused, so after warm-up no
-request allocates.  Completion is detected by polling CUDA events; latency =
-completion - arrival.  Each request's result is the same as the per-call
-path's (tests/test_batch_serve_gpu.py).
+A request is a volume in (pinned) host memory.  The server admits a waiting
+request as soon as one of its `slots` (requests in flight) is free and the
+request's device memory fits in the HBM budget, and enqueues all of its work
+at once, on three kinds of streams:
+
+  * the copy-in stream uploads the volume (requests in admission order);
+  * a compute stream waits for that upload and runs the pipeline
+    (voronoi_otsu_labeling, then statistics_of_labelled_pixels reading the
+    label count the pipeline left on the device -- no host round trip) and
+    copies the loop status and label count (8 bytes) to the host;
+  * once those 8 bytes are on the host, the copy-out stream brings back the
+    statistics of exactly that many labels.
+
+So uploads and downloads overlap the computation of other requests, while
+the computations themselves run one after another on the whole GPU (one
+compute stream, the default) or two at a time (compute_streams=2, each
+cooperative launch then capped at half the SMs).  Device buffers (input,
+labels, workspaces, tables) are kept per shape and reused, so after warm-up
+no request allocates.  Completion is detected by polling CUDA events;
+latency = completion - arrival.  Each request's result is the same as the
+per-call path's (tests/test_batch_serve_gpu.py).
 """
 from __future__ import annotations
 
@@ -64,7 +74,9 @@ class _Buffers:
         d = _lib.tensor_desc(self.labels)
         self.stats_ws = torch.empty(int(lib.cle_statistics_workspace_bytes(_lib.ref(d), self.capacity)),
                                     dtype=torch.uint8, device=device)
-        self.host_table = torch.empty((len(STAT_KEYS), self.capacity), dtype=torch.float32).pin_memory()
+        # pinned host copy of the statistics, grown when a request has more labels
+        self.host_table = torch.empty(len(STAT_KEYS) * min(self.capacity, 1 << 16),
+                                      dtype=torch.float32).pin_memory()
         self.host_count = torch.empty(2, dtype=torch.int32).pin_memory()
         self.bytes = sum(t.numel() * t.element_size() for t in
                          (self.src, self.labels, self.ws, self.table, self.stats_ws))
@@ -80,7 +92,8 @@ def request_bytes(shape, dtype) -> int:
 
 class SegmentationServer:
     def __init__(self, budget_bytes: float = 60e9, slots: int = 4, spot_sigma: float = 2.0,
-                 outline_sigma: float = 2.0, device=None, keep_labels: bool = False):
+                 outline_sigma: float = 2.0, device=None, keep_labels: bool = False,
+                 compute_streams: int = 1):
         _lib.load()
         self.keep_labels = keep_labels
         self.device = torch.device(device or "cuda", torch.cuda.current_device()) \
@@ -88,10 +101,13 @@ class SegmentationServer:
         self.budget = float(budget_bytes)
         self.slots = int(slots)
         self.spot, self.outline = float(spot_sigma), float(outline_sigma)
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.slots)]
+        self.copy_in = torch.cuda.Stream(device=self.device)
+        self.copy_out = torch.cuda.Stream(device=self.device)
+        self.computes = [torch.cuda.Stream(device=self.device) for _ in range(max(1, int(compute_streams)))]
+        self._next = 0
         self.pool = collections.defaultdict(list)    # (shape, dtype) -> [_Buffers] free
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        self.coop = max(1, sms // self.slots)
+        self.coop = max(1, sms // len(self.computes))
 
     # -- buffers ----------------------------------------------------------
     def _take(self, shape, dtype):
@@ -105,19 +121,23 @@ class SegmentationServer:
 
     # -- one request on one slot -------------------------------------------
     def _start(self, req: Request, k: int, t_ref: float):
-        s = self.streams[k]
         b = self._take(req.volume.shape, req.volume.dtype)
         lib = _lib.load()
-        with torch.cuda.stream(s):
+        with torch.cuda.stream(self.copy_in):
             b.src.copy_(req.volume, non_blocking=True)
+            uploaded = torch.cuda.Event()
+            uploaded.record(self.copy_in)
+        s = self.computes[self._next]
+        self._next = (self._next + 1) % len(self.computes)
+        s.wait_event(uploaded)
+        with torch.cuda.stream(s):
             vol_into(b.src, b.labels, b.ws, self.spot, self.outline, s.cuda_stream)
             count = lib.cle_workspace_label_count(b.ws.data_ptr())
             i, l = _lib.tensor_desc(b.src), _lib.tensor_desc(b.labels)
             _lib.check(lib.cle_statistics_of_labelled_pixels_device_count(
                 _lib.ref(i), _lib.ref(l), count, b.capacity, b.table.data_ptr(), b.stats_ws.data_ptr(),
                 b.stats_ws.numel(), s.cuda_stream), "statistics_of_labelled_pixels")
-            b.host_table.copy_(b.table, non_blocking=True)
-            # label count and loop status back to the host with the table
+            # loop status and label count back to the host first (8 bytes)
             status_count = torch.stack([b.ws[0:4].view(torch.int32)[0], b.ws[8:12].view(torch.int32)[0]])
             b.host_count.copy_(status_count, non_blocking=True)
             ev = torch.cuda.Event()
@@ -125,16 +145,32 @@ class SegmentationServer:
         req.admitted = time.perf_counter() - t_ref
         return b, ev
 
-    def _finish(self, req: Request, b: _Buffers):
+    def _copy_table(self, req: Request, b: _Buffers, done_compute):
+        """Second half of a request: checks status and count, then copies the
+        statistics of the request's labels only; returns the event to poll."""
         status, count = int(b.host_count[0]), int(b.host_count[1])
         if status:
             raise _lib.ERRORS.get(status, RuntimeError)(f"request {req.rid}: device status {status}")
         if count > b.capacity:
             raise RuntimeError(f"request {req.rid}: {count} labels exceed the table capacity {b.capacity}")
         req.num_labels = count
-        req.table = b.host_table[:, :count].numpy().copy()
-        if self.keep_labels:
-            req.labels = b.labels.clone()  # the pooled buffer is reused by later requests
+        s = self.copy_out
+        s.wait_event(done_compute)
+        if len(STAT_KEYS) * count > b.host_table.numel():
+            b.host_table = torch.empty(len(STAT_KEYS) * count * 2, dtype=torch.float32).pin_memory()
+        with torch.cuda.stream(s):
+            if count:
+                b.host_table[:len(STAT_KEYS) * count].copy_(b.table[:, :count].contiguous().view(-1),
+                                                             non_blocking=True)
+            if self.keep_labels:
+                req.labels = b.labels.clone()  # the pooled buffer is reused by later requests
+            ev = torch.cuda.Event()
+            ev.record(s)
+        return ev
+
+    def _finish(self, req: Request, b: _Buffers):
+        n = req.num_labels
+        req.table = b.host_table[:len(STAT_KEYS) * n].view(len(STAT_KEYS), n).numpy().copy()
 
     # -- trace replay --------------------------------------------------------
     def run(self, requests, realtime: bool = True):
@@ -142,22 +178,26 @@ class SegmentationServer:
         not admitted before its arrival time.  Returns the requests with their
         admitted / done times (seconds since the start)."""
         lib = _lib.load()
-        lib.cle_set_cooperative_ctas(self.coop if self.slots > 1 else 0)
+        lib.cle_set_cooperative_ctas(self.coop if len(self.computes) > 1 else 0)
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
-        running = {}       # slot -> (req, buffers, event, bytes)
+        running = {}       # slot -> [req, buffers, event, bytes, stage]
         in_use = 0.0
         t0 = time.perf_counter()
         try:
             while pending or running:
                 now = time.perf_counter() - t0
                 for k in list(running):
-                    req, b, ev, nbytes = running[k]
-                    if ev.query():
-                        req.done = time.perf_counter() - t0
-                        self._finish(req, b)
-                        self._give(req.volume.shape, req.volume.dtype, b)
-                        in_use -= nbytes
-                        del running[k]
+                    req, b, ev, nbytes, stage = running[k]
+                    if not ev.query():
+                        continue
+                    if stage == 0:                 # status and count arrived: copy the table
+                        running[k] = [req, b, self._copy_table(req, b, ev), nbytes, 1]
+                        continue
+                    req.done = time.perf_counter() - t0
+                    self._finish(req, b)
+                    self._give(req.volume.shape, req.volume.dtype, b)
+                    in_use -= nbytes
+                    del running[k]
                 free = [k for k in range(self.slots) if k not in running]
                 while pending and free and (not realtime or pending[0].arrival <= now):
                     req = pending[0]
@@ -167,7 +207,7 @@ class SegmentationServer:
                     pending.popleft()
                     k = free.pop(0)
                     b, ev = self._start(req, k, t0)
-                    running[k] = (req, b, ev, nbytes)
+                    running[k] = [req, b, ev, nbytes, 0]
                     in_use += nbytes
                 if running and not free:
                     time.sleep(20e-6)
