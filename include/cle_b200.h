@@ -183,6 +183,15 @@ int cle_connected_components_labeling_box(const cle_tensor *binary, const cle_te
                                           void *workspace, size_t workspace_bytes,
                                           void *stream);
 
+/* ---- connected_components_labeling_diamond -----------------------------
+ * replaces _tier5/_connected_components_labeling_diamond.py:6-40: the same as
+ * the box form with face connectivity (4 neighbours in 2D, 6 in 3D).  Same
+ * workspace size as the box form. */
+size_t cle_connected_components_labeling_diamond_workspace_bytes(const cle_tensor *binary);
+int cle_connected_components_labeling_diamond(const cle_tensor *binary, const cle_tensor *dst,
+                                              void *workspace, size_t workspace_bytes,
+                                              void *stream);
+
 /* ---- relabel_sequential --------------------------------------------------
  * replaces _tier3/_relabel_sequential.py:12-58.  src: u32 or f32 labels;
  * dst: u32 or f32.  max_label is the maximum of src (the reference also
@@ -210,6 +219,21 @@ size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *bina
 int cle_masked_voronoi_labeling_binary(const cle_tensor *binary, const cle_tensor *mask,
                                        const cle_tensor *dst, void *workspace,
                                        size_t workspace_bytes, void *stream);
+
+/* ---- extend_labeling_via_voronoi / voronoi_labeling -------------------
+ * extend_labeling_via_voronoi replaces _tier4/_extend_labeling_via_voronoi.py:13-60:
+ * labels (u8/u16/u32/i32/f32, converted to uint32 like the reference's copy)
+ * grow into every zero voxel, box and diamond steps alternating, until a
+ * step changes nothing.  voronoi_labeling replaces _tier5/_voronoi_labeling.py:8-40
+ * (connected_components_labeling_box, then that growth).  dst: u32 or f32.
+ * The status word of the workspace (cle_workspace_status) reports the loop
+ * outcome. */
+size_t cle_extend_labeling_via_voronoi_workspace_bytes(const cle_tensor *src);
+int cle_extend_labeling_via_voronoi(const cle_tensor *src, const cle_tensor *dst, void *workspace,
+                                    size_t workspace_bytes, void *stream);
+size_t cle_voronoi_labeling_workspace_bytes(const cle_tensor *binary);
+int cle_voronoi_labeling(const cle_tensor *binary, const cle_tensor *dst, void *workspace,
+                         size_t workspace_bytes, void *stream);
 
 /* ---- voronoi_otsu_labeling ---------------------------------------------
  * replaces _tier9/_voronoi_otsu_labeling.py:11-73.  src: u8/u16/f32 (u8 and

@@ -83,6 +83,12 @@ def lib():
         L.orc_masked_voronoi.argtypes = [P, P, P, P, I64, I64, I64, I]
         L.orc_masked_voronoi.restype = I64
         L.orc_voronoi_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, D, D, P, P, P]
+        L.orc_ccl_diamond.argtypes = [P, P, I64, I64, I64]
+        L.orc_ccl_diamond.restype = I64
+        L.orc_extend_labeling_via_voronoi.argtypes = [P, P, I64, I64, I64, I]
+        L.orc_extend_labeling_via_voronoi.restype = I64
+        L.orc_voronoi_labeling.argtypes = [P, P, I64, I64, I64, I]
+        L.orc_voronoi_labeling.restype = I64
         L.orc_erode_box.argtypes = [P, P, I64, I64, I64, I]
         L.orc_gauss_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, D]
         L.orc_gauss_otsu_labeling.restype = I64
@@ -237,6 +243,40 @@ def voronoi_otsu_labeling(img, spot_sigma=2.0, outline_sigma=2.0, debug=False):
                                             float(outline_sigma), _p(spots), _p(seg), _p(thr))
     if debug:
         return out, dict(seeds=spots, segmentation=seg, threshold=float(thr[0]), steps=steps)
+    return out
+
+
+def connected_components_labeling_diamond(binary) -> np.ndarray:
+    fg = _u8(binary)
+    out = np.empty(fg.shape, np.uint32)
+    D, H, W = _dhw(fg.shape)
+    lib().orc_ccl_diamond(_p(fg), _p(out), D, H, W)
+    return out
+
+
+def _labels_u32(a) -> np.ndarray:
+    """uint32 labels as the reference's copy into a uint32 image makes them
+    (float values: saturating conversion, fractions dropped)."""
+    a = np.asarray(a)
+    if a.dtype.kind == "f":
+        a = np.where(np.isnan(a), 0, np.clip(a, 0, 4294967295.0))
+        return np.ascontiguousarray(a.astype(np.uint64).astype(np.uint32))
+    return np.ascontiguousarray(np.clip(a.astype(np.int64), 0, 4294967295).astype(np.uint32))
+
+
+def extend_labeling_via_voronoi(labels) -> np.ndarray:
+    a = _labels_u32(labels)
+    out = np.empty(a.shape, np.uint32)
+    D, H, W = _dhw(a.shape)
+    lib().orc_extend_labeling_via_voronoi(_p(a), _p(out), D, H, W, a.ndim)
+    return out
+
+
+def voronoi_labeling(binary) -> np.ndarray:
+    fg = _u8(binary)
+    out = np.empty(fg.shape, np.uint32)
+    D, H, W = _dhw(fg.shape)
+    lib().orc_voronoi_labeling(_p(fg), _p(out), D, H, W, fg.ndim)
     return out
 
 

@@ -305,7 +305,22 @@ static int cmp_u32(const void *a, const void *b) {
 
 /* fg: nonzero = foreground.  labels: output uint32.  Returns the number of
  * labels. */
+static int64_t ccl_conn(const uint8_t *fg, uint32_t *labels, int64_t D, int64_t H, int64_t W,
+                        int diamond);
+
 int64_t orc_ccl_box(const uint8_t *fg, uint32_t *labels, int64_t D, int64_t H, int64_t W) {
+    return ccl_conn(fg, labels, D, H, W, 0);
+}
+
+/* connected_components_labeling_diamond: _tier5/_connected_components_labeling_diamond.py:
+ * 39 -- the box labelling with nonzero_minimum_diamond as the propagation
+ * filter, i.e. face connectivity; keys and relabel as for the box form. */
+int64_t orc_ccl_diamond(const uint8_t *fg, uint32_t *labels, int64_t D, int64_t H, int64_t W) {
+    return ccl_conn(fg, labels, D, H, W, 1);
+}
+
+static int64_t ccl_conn(const uint8_t *fg, uint32_t *labels, int64_t D, int64_t H, int64_t W,
+                        int diamond) {
     const int64_t n = D * H * W;
     int64_t *par = (int64_t *)malloc(sizeof(int64_t) * n);
     for (int64_t i = 0; i < n; ++i) par[i] = fg[i] ? i : -1;
@@ -319,6 +334,7 @@ int64_t orc_ccl_box(const uint8_t *fg, uint32_t *labels, int64_t D, int64_t H, i
                     for (int dy = -1; dy <= 1; ++dy)
                         for (int dx = -1; dx <= 1; ++dx) {
                             if (dz == 0 && (dy > 0 || (dy == 0 && dx >= 0))) continue;
+                            if (diamond && (abs(dx) + abs(dy) + abs(dz)) > 1) continue;
                             int64_t qz = z + dz, qy = y + dy, qx = x + dx;
                             if (qz < 0 || qy < 0 || qy >= H || qx < 0 || qx >= W) continue;
                             int64_t q = IDX(qz, qy, qx);
@@ -529,6 +545,66 @@ int64_t orc_eroded_otsu_labeling(const float *src, uint32_t *labels, int64_t D, 
     for (int64_t i = 0; i < n; ++i) tmp[i] = (float)binary[i];
     const int64_t steps = orc_masked_voronoi(e0, tmp, NULL, labels, D, H, W, ndim);
     free(tmp); free(binary); free(e0); free(e1);
+    return steps;
+}
+
+/* ------------------------------------------------------------------ */
+/* extend_labeling_via_voronoi: _tier4/_extend_labeling_via_voronoi.py:*/
+/* 30-56.  uint32 state (flip/flop are uint32 label images): every 0   */
+/* voxel takes the maximum over the box (even steps) or the face       */
+/* neighbours (odd steps) including itself; stop after the first step  */
+/* that changes nothing.  Returns the number of steps.                 */
+/* ------------------------------------------------------------------ */
+int64_t orc_extend_labeling_via_voronoi(const uint32_t *src, uint32_t *out, int64_t D,
+                                        int64_t H, int64_t W, int ndim) {
+    const int64_t n = D * H * W;
+    uint32_t *a = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    uint32_t *b = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    memcpy(a, src, sizeof(uint32_t) * n);
+    const int zr = (ndim == 3) ? 1 : 0;
+    int64_t step = 0;
+    for (;;) {
+        const int box = (step % 2) == 0;
+        int64_t changed = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(+ : changed)
+        for (int64_t z = 0; z < D; ++z)
+            for (int64_t y = 0; y < H; ++y)
+                for (int64_t x = 0; x < W; ++x) {
+                    const int64_t p = IDX(z, y, x);
+                    const uint32_t v = a[p];
+                    if (v != 0) { b[p] = v; continue; }
+                    uint32_t m = 0;
+                    for (int dz = -zr; dz <= zr; ++dz)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dx = -1; dx <= 1; ++dx) {
+                                if (!box && (abs(dx) + abs(dy) + abs(dz)) > 1) continue;
+                                const int64_t qz = z + dz, qy = y + dy, qx = x + dx;
+                                if (qz < 0 || qz >= D || qy < 0 || qy >= H || qx < 0 || qx >= W)
+                                    continue;
+                                const uint32_t q = a[IDX(qz, qy, qx)];
+                                if (q > m) m = q;
+                            }
+                    b[p] = m;
+                    if (m != 0) changed++;
+                }
+        uint32_t *t = a; a = b; b = t;
+        step++;
+        if (changed == 0) break;
+    }
+    memcpy(out, a, sizeof(uint32_t) * n);
+    free(a); free(b);
+    return step;
+}
+
+/* voronoi_labeling: _tier5/_voronoi_labeling.py:36-40 -- connected       */
+/* components (box), then extend_labeling_via_voronoi.                    */
+int64_t orc_voronoi_labeling(const uint8_t *fg, uint32_t *out, int64_t D, int64_t H, int64_t W,
+                             int ndim) {
+    const int64_t n = D * H * W;
+    uint32_t *cc = (uint32_t *)malloc(sizeof(uint32_t) * n);
+    orc_ccl_box(fg, cc, D, H, W);
+    const int64_t steps = orc_extend_labeling_via_voronoi(cc, out, D, H, W, ndim);
+    free(cc);
     return steps;
 }
 

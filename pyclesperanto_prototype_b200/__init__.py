@@ -13,8 +13,10 @@ the library or a CUDA device the ops raise; there is no CPU fallback.
 from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, create_binary_like,
                      create_labels_like, create_like, create_none, create_zyx, is_image, nparray,
                      plugin_function, pull, pull_zyx, push, push_native, push_zyx)
-from ._ops import (binary_and, connected_components_labeling_box, detect_maxima_box,
-                   erode_box, eroded_otsu_labeling, gauss_otsu_labeling,
+from ._ops import (binary_and, connected_components_labeling_box,
+                   connected_components_labeling_diamond, detect_maxima_box,
+                   erode_box, eroded_otsu_labeling, extend_labeling_via_voronoi, gauss_otsu_labeling,
+                   voronoi_labeling,
                    gaussian_blur, greater_constant, histogram, mask, masked_voronoi_labeling,
                    masked_voronoi_labeling_binary,
                    maximum_of_all_pixels, minimum_of_all_pixels, radius_to_kernel_size,

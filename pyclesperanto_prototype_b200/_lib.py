@@ -85,6 +85,12 @@ _SIGS = {
     "cle_relabel_sequential": (ctypes.c_int, [_T, _T, ctypes.c_uint32, _P, _SZ, _P]),
     "cle_masked_voronoi_labeling_workspace_bytes": (_SZ, [_T]),
     "cle_masked_voronoi_labeling": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
+    "cle_connected_components_labeling_diamond_workspace_bytes": (_SZ, [_T]),
+    "cle_connected_components_labeling_diamond": (ctypes.c_int, [_T, _T, _P, _SZ, _P]),
+    "cle_extend_labeling_via_voronoi_workspace_bytes": (_SZ, [_T]),
+    "cle_extend_labeling_via_voronoi": (ctypes.c_int, [_T, _T, _P, _SZ, _P]),
+    "cle_voronoi_labeling_workspace_bytes": (_SZ, [_T]),
+    "cle_voronoi_labeling": (ctypes.c_int, [_T, _T, _P, _SZ, _P]),
     "cle_masked_voronoi_labeling_binary_workspace_bytes": (_SZ, [_T]),
     "cle_masked_voronoi_labeling_binary": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
     "cle_voronoi_otsu_labeling_workspace_bytes": (_SZ, [_T]),

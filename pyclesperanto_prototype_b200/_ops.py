@@ -252,6 +252,41 @@ def masked_voronoi_labeling_binary(binary_source, mask_image, labeling_destinati
     return labeling_destination
 
 
+@plugin_function(categories=['label', 'in assistant'], output_creator=create_labels_like)
+def connected_components_labeling_diamond(binary_input: Image, labeling_destination: Image = None) -> Image:
+    """Connected components with face connectivity (4 neighbours in 2D, 6 in 3D),
+    labels as in connected_components_labeling_box
+    (_tier5/_connected_components_labeling_diamond.py:6-40)."""
+    b, d = _T(binary_input), _T(labeling_destination)
+    ws = _ws("cle_connected_components_labeling_diamond_workspace_bytes", _lib.ref(b))
+    _call("cle_connected_components_labeling_diamond", _lib.ref(b), _lib.ref(d), _ptr(ws), ws.numel(),
+          _lib.stream_ptr())
+    return labeling_destination
+
+
+def _grow_call(name, src: B200Array, dst: B200Array):
+    s, d = _T(src), _T(dst)
+    ws = _ws(name + "_workspace_bytes", _lib.ref(s))
+    stream = _lib.stream_ptr()
+    _call(name, _lib.ref(s), _lib.ref(d), _ptr(ws), ws.numel(), stream)
+    _lib.check(_lib.load().cle_workspace_status(ws.data_ptr(), ws.numel(), stream), name[4:])
+    return dst
+
+
+@plugin_function(categories=['label processing', 'in assistant'], output_creator=create_labels_like)
+def extend_labeling_via_voronoi(labeling_source: Image, labeling_destination: Image = None) -> Image:
+    """Grows every label into the zero voxels around it, box and diamond steps
+    alternating, until the labels touch (_tier4/_extend_labeling_via_voronoi.py:13-60)."""
+    return _grow_call("cle_extend_labeling_via_voronoi", labeling_source, labeling_destination)
+
+
+@plugin_function(categories=['label', 'in assistant', 'bia-bob-suggestion'], output_creator=create_labels_like)
+def voronoi_labeling(binary_source: Image, labeling_destination: Image = None) -> Image:
+    """Connected components (box) of the binary image, then their Voronoi
+    extension over the whole image (_tier5/_voronoi_labeling.py:8-40)."""
+    return _grow_call("cle_voronoi_labeling", binary_source, labeling_destination)
+
+
 @plugin_function(categories=['binary processing'], output_creator=create_binary_like)
 def erode_box(source: Image, destination: Image = None) -> Image:
     """Binary erosion over the Moore neighbourhood (_tier1/_erode_box.py:6-47):

@@ -283,6 +283,63 @@ int cle_masked_voronoi_labeling(const cle_tensor *bin, const cle_tensor *msk, co
     return masked_voronoi_dense(a, m, d, status, ar, S(stream));
 }
 
+size_t cle_connected_components_labeling_diamond_workspace_bytes(const cle_tensor *bin) {
+    Img im;
+    if (to_img(bin, im, "binary_input")) return 0;
+    return ccl_workspace_bytes(im);
+}
+
+int cle_connected_components_labeling_diamond(const cle_tensor *bin, const cle_tensor *dst, void *ws,
+                                              size_t ws_bytes, void *stream) {
+    Img a, d;
+    CLE_TRY(to_img(bin, a, "binary_input"));
+    CLE_TRY(to_img(dst, d, "labeling_destination"));
+    CLE_TRY(same_shape(a, d, "binary_input", "labeling_destination"));
+    if (d.dtype != CLE_U32 && d.dtype != CLE_F32) { set_error("connected_components_labeling_diamond: destination must be uint32 or float32"); return CLE_ERR_DTYPE; }
+    CLE_TRY(ws_check(ws, ws_bytes, ccl_workspace_bytes(a), "connected_components_labeling_diamond"));
+    CLE_TRY(set_device_of(a, bin));
+    Arena ar(ws, ws_bytes);
+    uint32_t *lab = ar.take<uint32_t>(a.n());
+    if (d.dtype == CLE_U32) lab = (uint32_t *)d.data;
+    CLE_TRY(ccl_dense(a, lab, ar, S(stream), true));
+    if (d.dtype == CLE_F32) return ccl_to_dst(lab, d, S(stream));
+    return CLE_OK;
+}
+
+size_t cle_extend_labeling_via_voronoi_workspace_bytes(const cle_tensor *src) {
+    Img im;
+    if (to_img(src, im, "labeling_source")) return 0;
+    return extend_voronoi_workspace_bytes(im);
+}
+
+int cle_extend_labeling_via_voronoi(const cle_tensor *src, const cle_tensor *dst, void *ws, size_t ws_bytes,
+                                    void *stream) {
+    Img a, d;
+    CLE_TRY(to_img(src, a, "labeling_source"));
+    CLE_TRY(to_img(dst, d, "labeling_destination"));
+    CLE_TRY(ws_check(ws, ws_bytes, extend_voronoi_workspace_bytes(a), "extend_labeling_via_voronoi"));
+    CLE_TRY(set_device_of(a, src));
+    Arena ar(ws, ws_bytes);
+    return extend_labeling_via_voronoi(a, d, ar, S(stream));
+}
+
+size_t cle_voronoi_labeling_workspace_bytes(const cle_tensor *bin) {
+    Img im;
+    if (to_img(bin, im, "binary_source")) return 0;
+    return extend_voronoi_workspace_bytes(im);
+}
+
+int cle_voronoi_labeling(const cle_tensor *bin, const cle_tensor *dst, void *ws, size_t ws_bytes,
+                         void *stream) {
+    Img a, d;
+    CLE_TRY(to_img(bin, a, "binary_source"));
+    CLE_TRY(to_img(dst, d, "labeling_destination"));
+    CLE_TRY(ws_check(ws, ws_bytes, extend_voronoi_workspace_bytes(a), "voronoi_labeling"));
+    CLE_TRY(set_device_of(a, bin));
+    Arena ar(ws, ws_bytes);
+    return voronoi_labeling(a, d, ar, S(stream));
+}
+
 size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *bin) {
     Img im;
     if (to_img(bin, im, "binary_source")) return 0;

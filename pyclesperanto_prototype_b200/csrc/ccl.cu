@@ -124,6 +124,9 @@ ccl_init_rows(const T *__restrict__ bin, uint32_t *__restrict__ lab, Geo g, Rows
     }
 }
 
+// DIAMOND: face connectivity (connected_components_labeling_diamond): only
+// the backward rows (y-1, z) and (y, z-1) at the same x, no diagonal contacts.
+template <bool DIAMOND>
 __global__ void __launch_bounds__(kRowWarps * 32)
 ccl_union_rows(uint32_t *lab, Geo g, Rows R) {
     const int lane = threadIdx.x & 31;
@@ -148,6 +151,7 @@ ccl_union_rows(uint32_t *lab, Geo g, Rows R) {
         if (lane == 0 && fg && xs > 0 && ld_cg(lab + r * g.W + x - 1u) != 0u) unite(lab, g, kp, kp - xstep);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
+            if (DIAMOND && (k == 1 || k == 3)) continue;        // (y-1, z-1), (y+1, z-1): no face contact
             const int qy = (int)y + (k == 0 ? -1 : k - 2), qz = (int)z - (k == 0 ? 0 : 1);
             if (qy < 0 || qy >= (int)g.H || qz < 0) continue;    // warp-uniform
             const uint32_t *row = lab + ((uint32_t)qz * g.H + (uint32_t)qy) * g.W;
@@ -161,6 +165,7 @@ ccl_union_rows(uint32_t *lab, Geo g, Rows R) {
             if (!fg) continue;
             const uint32_t kq = xyz2k(g, x, (uint32_t)qy, (uint32_t)qz);
             if (q && (is_start || !qL)) unite(lab, g, ka, kq);            // first voxel of an overlap
+            if (DIAMOND) continue;
             if (is_start && qL && !q) unite(lab, g, ka, kq - xstep);     // diagonal contact at a-1
             if (is_end && qR && !q) unite(lab, g, ka, kq + xstep);       // diagonal contact at b+1
         }
@@ -438,7 +443,7 @@ size_t ccl_workspace_bytes(const Img &im) {
     return a.off;
 }
 
-int ccl_dense(const Img &bin, uint32_t *lab, Arena &ws, cudaStream_t st) {
+int ccl_dense(const Img &bin, uint32_t *lab, Arena &ws, cudaStream_t st, bool diamond) {
     const int64_t n = bin.n();
     Rank r = take_rank(ws, fkey_bits_for(n));
     if (!ws.ok()) { set_error("connected_components_labeling_box: workspace too small"); return CLE_ERR_WORKSPACE; }
@@ -456,7 +461,8 @@ int ccl_dense(const Img &bin, uint32_t *lab, Arena &ws, cudaStream_t st) {
         default: set_error("connected_components_labeling_box: unsupported dtype %d", bin.dtype); return CLE_ERR_DTYPE;
     }
     const int b = launch_blocks(n, kT);
-    ccl_union_rows<<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
+    if (diamond) ccl_union_rows<true><<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
+    else ccl_union_rows<false><<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
     ccl_flatten_rows<<<rb, kRowWarps * 32, 0, st>>>(lab, g, R);
     CLE_CUDA(cudaMemsetAsync(r.bitmap, 0, sizeof(uint32_t) * r.words, st));
     ccl_mark_dense<<<b, kT, 0, st>>>(lab, g, n, r.bitmap);

@@ -48,7 +48,8 @@ int detect_maxima(const Img &src, const Img &dst, cudaStream_t st);
 // ccl.cu
 size_t ccl_workspace_bytes(const Img &im);
 // Dense CCL of (binary != 0) into u32 labels (x-major float32 key ranks).
-int ccl_dense(const Img &binary, uint32_t *labels, Arena &ws, cudaStream_t st);
+// diamond: face connectivity (4 in 2D, 6 in 3D) instead of the 3^d box
+int ccl_dense(const Img &binary, uint32_t *labels, Arena &ws, cudaStream_t st, bool diamond = false);
 // CCL restricted to a device list of voxel indices whose entries in `labels`
 // already hold (own x-major key + 1); on return those entries hold labels.
 // d_count: device count of list entries; cap: list capacity.
@@ -87,6 +88,10 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma,
 // composite's case), on the active-brick growth.
 size_t masked_voronoi_binary_workspace_bytes(const Img &im);
 int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st);
+// extend_labeling_via_voronoi / voronoi_labeling (status word at workspace offset 0)
+size_t extend_voronoi_workspace_bytes(const Img &im);
+int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaStream_t st);
+int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st);
 
 // noalloc.cu: threshold_otsu with a built-in scratch array
 size_t threshold_otsu_noalloc_capacity();

@@ -194,6 +194,155 @@ int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena
     return CLE_OK;
 }
 
+// ---- extend_labeling_via_voronoi / voronoi_labeling -------------------------
+// _tier4/_extend_labeling_via_voronoi.py:13-60: the labels (uint32, any values)
+// grow into every zero voxel with the onlyzero_overwrite_maximum box/diamond
+// Jacobi steps until a step changes nothing -- the brick growth kernel with a
+// mask that covers the whole image.  voronoi_labeling (_tier5/_voronoi_labeling.py:
+// 8-40) is connected_components_labeling_box followed by that growth.
+namespace {
+
+template <typename T>
+__global__ void to_labels_kernel(const T *__restrict__ src, uint32_t *__restrict__ lab, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const T v = src[i];
+        uint32_t o;
+        if constexpr (std::is_floating_point<T>::value)   // clij_convert_uint_sat
+            o = !(v > (T)0) ? 0u : (v >= (T)4294967295.0 ? 0xFFFFFFFFu : (uint32_t)v);
+        else if constexpr (std::is_signed<T>::value)
+            o = v < (T)0 ? 0u : (uint32_t)v;
+        else
+            o = (uint32_t)v;
+        lab[i] = o;
+    }
+}
+
+constexpr int kSeedWarps = 8;
+
+// One seed voxel per 32-voxel row brick that holds a label: its 3x3x3 brick
+// neighbourhood covers every voxel next to a label.  One global atomic per CTA.
+__global__ void __launch_bounds__(kSeedWarps * 32)
+brick_seeds_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t WB, FastDiv fWB, uint32_t nb,
+                   uint32_t *__restrict__ seeds, uint32_t *__restrict__ d_count) {
+    __shared__ uint32_t s_n, s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t base = blockIdx.x * kSeedWarps; base < nb; base += gridDim.x * kSeedWarps) {
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        const uint32_t b = base + warp;
+        uint32_t pos = 0, m = 0;
+        bool has = false;
+        if (b < nb) {
+            const uint32_t r = fWB.div(b), xb = b - r * WB, x = xb * 32u + (uint32_t)lane;
+            const unsigned bal = __ballot_sync(0xffffffffu, x < W && lab[r * W + x] != 0u);
+            has = bal != 0u;
+            if (has && lane == 0) {
+                m = r * W + xb * 32u + (uint32_t)(__ffs(bal) - 1);
+                pos = atomicAdd(&s_n, 1u);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_base = s_n ? atomicAdd(d_count, s_n) : 0u;
+        __syncthreads();
+        if (has && lane == 0) seeds[s_base + pos] = m;
+    }
+}
+
+struct ExtLayout {
+    Scalars *sc;
+    uint8_t *seg;
+    uint32_t *seeds;
+    uint32_t *lab;    // used when the destination is float32
+};
+
+ExtLayout take_ext_layout(Arena &a, const Img &im) {
+    ExtLayout l;
+    l.sc = a.take<Scalars>(1);
+    l.seg = a.take<uint8_t>(im.n());
+    l.seeds = a.take<uint32_t>((im.n() + 31) / 32 + (size_t)(im.D * im.H));
+    l.lab = a.take<uint32_t>(im.n());
+    return l;
+}
+
+// Grows `lab` in place over the whole image; status in l.sc.
+int grow_everywhere(const Img &im, uint32_t *lab, ExtLayout &l, Arena &tail, cudaStream_t st) {
+    CLE_CUDA(cudaMemsetAsync(l.seg, 1, (size_t)im.n(), st));
+    const uint32_t WB = (uint32_t)((im.W + 31) / 32);
+    const uint32_t nb = (uint32_t)(im.D * im.H) * WB;
+    brick_seeds_kernel<<<launch_blocks((int64_t)nb * 32, kSeedWarps * 32), kSeedWarps * 32, 0, st>>>(
+        lab, (uint32_t)im.W, WB, FastDiv(WB), nb, l.seeds, &l.sc->seed_count);
+    CLE_LAUNCH_CHECK("brick seeds");
+    return voronoi_frontier(im, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, tail, st);
+}
+
+}  // namespace
+
+size_t extend_voronoi_workspace_bytes(const Img &im) {
+    Arena a(nullptr, 0);
+    take_ext_layout(a, im);
+    const size_t tail = std::max(ccl_workspace_bytes(im), voronoi_frontier_workspace_bytes(im));
+    return a.off + tail;
+}
+
+int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaStream_t st) {
+    CLE_TRY(same_shape(src, dst, "labeling_source", "labeling_destination"));
+    if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
+        set_error("extend_labeling_via_voronoi: destination must be uint32 or float32");
+        return CLE_ERR_DTYPE;
+    }
+    ExtLayout l = take_ext_layout(ws, src);
+    if (!ws.measuring && ws.cap < extend_voronoi_workspace_bytes(src)) {
+        set_error("extend_labeling_via_voronoi: workspace too small");
+        return CLE_ERR_WORKSPACE;
+    }
+    CLE_CUDA(cudaMemsetAsync(l.sc, 0, sizeof(Scalars), st));
+    uint32_t *lab = dst.dtype == CLE_U32 ? (uint32_t *)dst.data : l.lab;
+    const int64_t n = src.n();
+    const int b = launch_blocks(n, 256);
+    switch (src.dtype) {
+        case CLE_U8: to_labels_kernel<uint8_t><<<b, 256, 0, st>>>((const uint8_t *)src.data, lab, n); break;
+        case CLE_U16: to_labels_kernel<uint16_t><<<b, 256, 0, st>>>((const uint16_t *)src.data, lab, n); break;
+        case CLE_U32:
+            if (src.data != (void *)lab) to_labels_kernel<uint32_t><<<b, 256, 0, st>>>((const uint32_t *)src.data, lab, n);
+            break;
+        case CLE_I32: to_labels_kernel<int32_t><<<b, 256, 0, st>>>((const int32_t *)src.data, lab, n); break;
+        case CLE_F32: to_labels_kernel<float><<<b, 256, 0, st>>>((const float *)src.data, lab, n); break;
+        default: set_error("extend_labeling_via_voronoi: unsupported source dtype %d", src.dtype); return CLE_ERR_DTYPE;
+    }
+    CLE_LAUNCH_CHECK("labels");
+    CLE_TRY(grow_everywhere(src, lab, l, ws, st));
+    if (dst.dtype == CLE_F32) {
+        u32_to_f32<<<launch_blocks(n, 256), 256, 0, st>>>(lab, (float *)dst.data, n);
+        CLE_LAUNCH_CHECK("labels to f32");
+    }
+    return CLE_OK;
+}
+
+int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st) {
+    CLE_TRY(same_shape(bin, dst, "binary_source", "labeling_destination"));
+    if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
+        set_error("voronoi_labeling: destination must be uint32 or float32");
+        return CLE_ERR_DTYPE;
+    }
+    ExtLayout l = take_ext_layout(ws, bin);
+    const size_t tail_off = ws.off;
+    if (!ws.measuring && ws.cap < extend_voronoi_workspace_bytes(bin)) {
+        set_error("voronoi_labeling: workspace too small");
+        return CLE_ERR_WORKSPACE;
+    }
+    CLE_CUDA(cudaMemsetAsync(l.sc, 0, sizeof(Scalars), st));
+    uint32_t *lab = dst.dtype == CLE_U32 ? (uint32_t *)dst.data : l.lab;
+    CLE_TRY(ccl_dense(bin, lab, ws, st));
+    ws.off = tail_off;
+    CLE_TRY(grow_everywhere(bin, lab, l, ws, st));
+    if (dst.dtype == CLE_F32) {
+        u32_to_f32<<<launch_blocks(dst.n(), 256), 256, 0, st>>>(lab, (float *)dst.data, dst.n());
+        CLE_LAUNCH_CHECK("labels to f32");
+    }
+    return CLE_OK;
+}
+
 int *workspace_status_ptr(void *ws) { return &reinterpret_cast<Scalars *>(ws)->status; }
 uint32_t *workspace_label_count_ptr(void *ws) { return &reinterpret_cast<Scalars *>(ws)->nlabels; }
 

@@ -1,5 +1,7 @@
-// voronoi_bricks.cu -- the masked Voronoi growth of voronoi_otsu_labeling
-// (_tier5/_masked_voronoi_labeling.py:44-76, with a 0/1 mask and seeds inside it).
+// voronoi_bricks.cu -- the Voronoi growth of voronoi_otsu_labeling, masked_voronoi_labeling
+// with a 0/1 mask, extend_labeling_via_voronoi and voronoi_labeling
+// (_tier5/_masked_voronoi_labeling.py:44-76 with a 0/1 mask and seeds inside it,
+// _tier4/_extend_labeling_via_voronoi.py:30-56 with the whole image as mask).
 //
 // The reference's Jacobi steps (box stencil on even steps, face stencil on odd
 // steps, a voxel rewritten only while 0 with the maximum over the stencil
@@ -35,7 +37,6 @@ constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kSlice = 256;                     // per-warp append slice (entries)
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
-constexpr uint32_t kPend = 0x80000000u;         // Mv: face stencil missed, box will hit
 constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 constexpr uint64_t kKernelLimitNs = 20000000000ull;
@@ -133,7 +134,7 @@ template <bool IS3D>
 __global__ void __launch_bounds__(kBT, 1)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
-                      uint32_t *B1, uint32_t *Mv, uint32_t *bstep, BState *S, int *d_status,
+                      uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
                       uint32_t max_steps, unsigned long long *trace) {
     __shared__ uint32_t s_red[kWPB];
     const Geo &g = G.g;
@@ -200,7 +201,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const int kc = ZR * 3 + 1;          // centre row
             const bool cand = inmask && rows[kc] == 0u;
             uint32_t out = 0;
-            bool remain = false;
+            bool remain = false, pend = false;
             if (__any_sync(0xffffffffu, cand)) {
                 uint32_t bm = 0, dm = 0;
 #pragma unroll
@@ -215,14 +216,18 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                     if (dz == 0 && dy == 0) dm = max(dm, max(l, rr));
                     else if (dz == 0 || dy == 0) dm = max(dm, c);
                 }
+                bool pl = false;
                 if (cand) {
                     const uint32_t m = box ? bm : dm;
-                    out = m ? m : ((bm != 0u) ? kPend : 0u);
+                    out = m;
+                    pl = m == 0u && bm != 0u;     // face stencil missed, the box stencil will hit
                     changed += (m != 0u);
                     remain = (m == 0u);
                 }
+                pend = __any_sync(0xffffffffu, pl);
             }
             Mv[(size_t)idx * 32 + lane] = out;
+            if (lane == 0) Pf[idx] = pend ? 1u : 0u;
             // no unlabelled mask voxel left after this step: never queue it again
             if (!__any_sync(0xffffffffu, remain) && lane == 0) atomicExch(bstep + b, 0xFFFFFFFFu);
         }
@@ -249,13 +254,12 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const uint32_t idx = base + warp;
             if (idx < nB) {
                 const uint32_t b = __ldcg(F + idx);
-                const uint32_t mv = Mv[(size_t)idx * 32 + lane];
+                const uint32_t m = Mv[(size_t)idx * 32 + lane];
+                const bool pend = __ldcg(Pf + idx) != 0u;
                 const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
                 const uint32_t z = g.fH.div(r), y = r - z * g.H;
-                const uint32_t m = (mv & kPend) ? 0u : mv;
                 if (m) st_cg(lab + r * g.W + xb * 32u + (uint32_t)lane, m);
                 const unsigned ch = __ballot_sync(0xffffffffu, m != 0u);
-                const bool pend = __any_sync(0xffffffffu, mv == kPend);
                 bool want = false;
                 if (lane < 27) {
                     const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
@@ -294,6 +298,7 @@ size_t voronoi_frontier_workspace_bytes(const Img &im) {
     a.take<uint32_t>(nb);        // list 1
     a.take<uint32_t>(nb);        // per-brick step tags
     a.take<uint32_t>(nb * 32);   // per-voxel phase-A results
+    a.take<uint32_t>(nb);        // per-entry pending flags
     return a.off;
 }
 
@@ -305,6 +310,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     uint32_t *B1 = ws.take<uint32_t>(nb);
     uint32_t *bstep = ws.take<uint32_t>(nb);
     uint32_t *Mv = ws.take<uint32_t>(nb * 32);
+    uint32_t *Pf = ws.take<uint32_t>(nb);
     if (!ws.ok()) { set_error("masked_voronoi_labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(BState), st));
     CLE_CUDA(cudaMemsetAsync(bstep, 0, sizeof(uint32_t) * nb, st));
@@ -330,7 +336,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     const int grid = (int)std::min<int64_t>(want, cooperative_ctas(dev));
     unsigned long long *trace =
         (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long), st);
-    void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv,
+    void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv, &Pf,
                     &bstep, &S, &d_status, &max_steps, &trace};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
     count_launches(1);

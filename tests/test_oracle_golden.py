@@ -225,3 +225,28 @@ def test_eroded_otsu_labeling_golden(oracle):
 def test_blobs_gauss_otsu_labeling(oracle, blobs, key, sigma):
     # demo/segmentation/labeling.ipynb cells 13-14 through the composed oracle
     assert _corners(oracle.gauss_otsu_labeling(blobs, sigma)) == _known()[key]["corners"]
+
+
+# ---- diamond CCL, extend_labeling_via_voronoi, voronoi_labeling ----------
+def test_ccl_diamond_golden(oracle):
+    # tests/test_connected_components_labeling_diamond.py:4-27
+    src = np.array([[[0, 1, 0, 1], [0, 1, 0, 0], [1, 0, 0, 1]]])
+    ref = np.array([[[0, 2, 0, 3], [0, 2, 0, 0], [1, 0, 0, 4]]])
+    assert np.array_equal(oracle.connected_components_labeling_diamond(src), ref)
+
+
+def test_extend_labeling_via_voronoi_golden(oracle):
+    # tests/test_extend_labeling_via_voronoi.py:4-37
+    src = np.array([[[0, 0, 0, 0, 3, 3], [0, 4, 0, 0, 3, 3], [0, 0, 0, 0, 0, 0], [0, 0, 0, 0, 0, 0],
+                     [0, 2, 0, 0, 1, 0], [0, 0, 0, 0, 0, 0]]])
+    ref = np.array([[[4, 4, 4, 3, 3, 3], [4, 4, 4, 3, 3, 3], [4, 4, 4, 3, 3, 3], [2, 2, 2, 1, 1, 1],
+                     [2, 2, 2, 1, 1, 1], [2, 2, 2, 1, 1, 1]]])
+    assert np.array_equal(oracle.extend_labeling_via_voronoi(src), ref)
+
+
+def test_voronoi_labeling_golden(oracle):
+    # tests/test_voronoi_labeling.py:4-37
+    src = np.zeros((1, 6, 6))
+    src[0, 1, 1] = src[0, 1, 4] = src[0, 4, 1] = src[0, 4, 4] = 1
+    ref = np.array([[[1, 1, 1, 3, 3, 3]] * 3 + [[2, 2, 2, 4, 4, 4]] * 3])
+    assert np.array_equal(oracle.voronoi_labeling(src), ref)

@@ -1,7 +1,8 @@
-"""erode_box, gauss_otsu_labeling and eroded_otsu_labeling on the device
-against the oracle: binary images and label images bit for bit, on the
-reference's own fixtures, seeded random images of ragged 2D/3D shapes and
-blob images."""
+"""erode_box, gauss_otsu_labeling, eroded_otsu_labeling,
+connected_components_labeling_diamond, extend_labeling_via_voronoi and
+voronoi_labeling on the device against the oracle: binary images and label
+images bit for bit, on the reference's own fixtures, seeded random images of
+ragged 2D/3D shapes and blob images."""
 import numpy as np
 import pytest
 
@@ -113,3 +114,59 @@ def test_eroded_otsu_labeling_matches_oracle(cle, oracle, shape, erosions, sigma
     img = _blob_image(shape, 13)
     got = cle.pull(cle.eroded_otsu_labeling(img, number_of_erosions=erosions, outline_sigma=sigma))
     assert np.array_equal(got, oracle.eroded_otsu_labeling(img, erosions, sigma))
+
+
+# ------------------------------- diamond CCL and Voronoi labelling -------
+def test_ccl_diamond_reference_test(cle):
+    # tests/test_connected_components_labeling_diamond.py:4-27 of the reference
+    src = cle.push(np.asarray([[[0, 1, 0, 1], [0, 1, 0, 0], [1, 0, 0, 1]]]))
+    out = cle.connected_components_labeling_diamond(src)
+    assert np.array_equal(cle.pull(out), [[[0, 2, 0, 3], [0, 2, 0, 0], [1, 0, 0, 4]]])
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("density", [0.3, 0.55, 0.8])
+def test_ccl_diamond_matches_oracle(cle, oracle, shape, density):
+    a = (np.random.default_rng(5).random(shape) < density).astype(np.uint8)
+    got = cle.pull(cle.connected_components_labeling_diamond(cle.push_native(a)))
+    assert np.array_equal(got, oracle.connected_components_labeling_diamond(a))
+
+
+def test_extend_labeling_via_voronoi_reference_test(cle):
+    # tests/test_extend_labeling_via_voronoi.py:4-37 of the reference
+    src = cle.push(np.asarray([[[0, 0, 0, 0, 3, 3], [0, 4, 0, 0, 3, 3], [0, 0, 0, 0, 0, 0],
+                                [0, 0, 0, 0, 0, 0], [0, 2, 0, 0, 1, 0], [0, 0, 0, 0, 0, 0]]]))
+    ref = [[[4, 4, 4, 3, 3, 3], [4, 4, 4, 3, 3, 3], [4, 4, 4, 3, 3, 3], [2, 2, 2, 1, 1, 1],
+            [2, 2, 2, 1, 1, 1], [2, 2, 2, 1, 1, 1]]]
+    assert np.array_equal(cle.pull(cle.extend_labeling_via_voronoi(src)), ref)
+
+
+def test_voronoi_labeling_reference_test(cle):
+    # tests/test_voronoi_labeling.py:4-37 of the reference
+    src = np.zeros((1, 6, 6))
+    src[0, 1, 1] = src[0, 1, 4] = src[0, 4, 1] = src[0, 4, 4] = 1
+    ref = [[[1, 1, 1, 3, 3, 3]] * 3 + [[2, 2, 2, 4, 4, 4]] * 3]
+    assert np.array_equal(cle.pull(cle.voronoi_labeling(cle.push(src))), ref)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("density", [0.0005, 0.01, 0.2])
+def test_voronoi_labeling_matches_oracle(cle, oracle, shape, density):
+    a = (np.random.default_rng(6).random(shape) < density).astype(np.uint8)
+    got = cle.pull(cle.voronoi_labeling(cle.push_native(a)))
+    assert np.array_equal(got, oracle.voronoi_labeling(a))
+
+
+@pytest.mark.parametrize("shape", [(70, 90), (20, 64, 50), (9, 130, 40)])
+def test_extend_labeling_via_voronoi_any_label_values(cle, oracle, shape):
+    # arbitrary uint32 label values, including ones at and above 2^31, held as
+    # a uint32 device image (push would round them to float32 like the reference)
+    import torch
+    rng = np.random.default_rng(7)
+    lab = np.zeros(shape, np.uint32)
+    idx = rng.choice(lab.size, 25, replace=False)
+    lab.flat[idx] = rng.integers(1, 2 ** 32 - 1, 25, dtype=np.uint64).astype(np.uint32)
+    lab.flat[idx[:3]] = [2 ** 31, 2 ** 31 + 5, 2 ** 32 - 1]
+    src = cle.B200Array(torch.from_numpy(lab).cuda())
+    got = cle.pull(cle.extend_labeling_via_voronoi(src, cle.create_labels_like(src)))
+    assert np.array_equal(got, oracle.extend_labeling_via_voronoi(lab))
