@@ -165,6 +165,21 @@ int cle_mask(const cle_tensor *src, const cle_tensor *mask, const cle_tensor *ds
  * edge; source u8/u16/u32/i32/f32, destination u8/u16/u32/f32. */
 int cle_erode_box(const cle_tensor *src, const cle_tensor *dst, void *stream);
 
+/* ---- minimum_box / maximum_box / top_hat_box ----------------------------
+ * minimum_box replaces _tier1/_minimum_box.py:6-55, maximum_box
+ * _tier1/_maximum_box.py, top_hat_box _tier2/_top_hat_box.py:6-43 (source minus
+ * maximum_box(minimum_box(source)), in float32).  Separable passes over clamped
+ * windows of int(2 * radius + 1) voxels; radius <= 0 leaves an axis alone;
+ * radii above 700 are rejected.  src: u8/u16/f32; dst: f32.  One workspace
+ * size (cle_box_filter_workspace_bytes) serves all three. */
+size_t cle_box_filter_workspace_bytes(const cle_tensor *src);
+int cle_minimum_box(const cle_tensor *src, const cle_tensor *dst, double radius_x, double radius_y,
+                    double radius_z, void *workspace, size_t workspace_bytes, void *stream);
+int cle_maximum_box(const cle_tensor *src, const cle_tensor *dst, double radius_x, double radius_y,
+                    double radius_z, void *workspace, size_t workspace_bytes, void *stream);
+int cle_top_hat_box(const cle_tensor *src, const cle_tensor *dst, double radius_x, double radius_y,
+                    double radius_z, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- detect_maxima_box ---------------------------------------------------
  * replaces _tier1/_detect_maxima_box.py:5-48 with kernels
  * _tier1/detect_maxima_3d_x.cl:1-49, _tier1/detect_maxima_2d_x.cl:1-35.

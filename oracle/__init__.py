@@ -90,6 +90,8 @@ def lib():
         L.orc_voronoi_labeling.argtypes = [P, P, I64, I64, I64, I]
         L.orc_voronoi_labeling.restype = I64
         L.orc_erode_box.argtypes = [P, P, I64, I64, I64, I]
+        L.orc_minmax_box.argtypes = [P, P, I64, I64, I64, I, D, D, D, I]
+        L.orc_top_hat_box.argtypes = [P, P, I64, I64, I64, I, D, D, D]
         L.orc_gauss_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, D]
         L.orc_gauss_otsu_labeling.restype = I64
         L.orc_eroded_otsu_labeling.argtypes = [P, P, I64, I64, I64, I, I, D]
@@ -277,6 +279,28 @@ def voronoi_labeling(binary) -> np.ndarray:
     out = np.empty(fg.shape, np.uint32)
     D, H, W = _dhw(fg.shape)
     lib().orc_voronoi_labeling(_p(fg), _p(out), D, H, W, fg.ndim)
+    return out
+
+
+def minimum_box(img, radius_x=0.0, radius_y=0.0, radius_z=0.0, _max=0) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty_like(a)
+    D, H, W = _dhw(a.shape)
+    lib().orc_minmax_box(_p(a), _p(out), D, H, W, a.ndim, float(radius_x), float(radius_y),
+                         float(radius_z), int(_max))
+    return out
+
+
+def maximum_box(img, radius_x=0.0, radius_y=0.0, radius_z=0.0) -> np.ndarray:
+    return minimum_box(img, radius_x, radius_y, radius_z, _max=1)
+
+
+def top_hat_box(img, radius_x=1.0, radius_y=1.0, radius_z=1.0) -> np.ndarray:
+    a = _f32(img)
+    out = np.empty_like(a)
+    D, H, W = _dhw(a.shape)
+    lib().orc_top_hat_box(_p(a), _p(out), D, H, W, a.ndim, float(radius_x), float(radius_y),
+                          float(radius_z))
     return out
 
 

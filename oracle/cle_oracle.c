@@ -507,6 +507,60 @@ void orc_erode_box(const float *src, uint8_t *dst, int64_t D, int64_t H, int64_t
     free(nz);
 }
 
+/* minimum_box / maximum_box: _tier1/_minimum_box.py:6-55 with             */
+/* _tier1/_execute_separable_kernel.py:7-76 -- passes x, y, z (3D); each     */
+/* the min (max) over i = -c..c, c = (N-1)/2, N = int(2*radius + 1), reads   */
+/* clamped to the edge; radius <= 0 copies.  top_hat_box: _tier2/            */
+/* _top_hat_box.py:37-43, source - maximum_box(minimum_box(source)).          */
+static void minmax_line_pass(const float *src, float *dst, int64_t D, int64_t H, int64_t W,
+                             int axis, int c, int is_max) {
+    const int64_t n = D * H * W;
+    if (c <= 0) { memcpy(dst, src, sizeof(float) * n); return; }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int64_t z = 0; z < D; ++z)
+        for (int64_t y = 0; y < H; ++y)
+            for (int64_t x = 0; x < W; ++x) {
+                float m = src[IDX(z, y, x)];
+                for (int i = -c; i <= c; ++i) {
+                    int64_t qz = z, qy = y, qx = x;
+                    if (axis == 0) qx = clampi(x + i, 0, W - 1);
+                    else if (axis == 1) qy = clampi(y + i, 0, H - 1);
+                    else qz = clampi(z + i, 0, D - 1);
+                    const float v = src[IDX(qz, qy, qx)];
+                    m = is_max ? (v > m ? v : m) : (v < m ? v : m);
+                }
+                dst[IDX(z, y, x)] = m;
+            }
+}
+
+static int box_radius(double r) {
+    if (!(r > 0)) return 0;
+    const int64_t n = (int64_t)(r * 2 + 1);
+    return (int)((n - 1) / 2);
+}
+
+void orc_minmax_box(const float *src, float *dst, int64_t D, int64_t H, int64_t W, int ndim,
+                    double rx, double ry, double rz, int is_max) {
+    const int64_t n = D * H * W;
+    float *t = (float *)malloc(sizeof(float) * n);
+    float *u = (float *)malloc(sizeof(float) * n);
+    minmax_line_pass(src, t, D, H, W, 0, box_radius(rx), is_max);
+    minmax_line_pass(t, ndim == 3 ? u : dst, D, H, W, 1, box_radius(ry), is_max);
+    if (ndim == 3) minmax_line_pass(u, dst, D, H, W, 2, box_radius(rz), is_max);
+    free(t); free(u);
+}
+
+void orc_top_hat_box(const float *src, float *dst, int64_t D, int64_t H, int64_t W, int ndim,
+                     double rx, double ry, double rz) {
+    const int64_t n = D * H * W;
+    float *mn = (float *)malloc(sizeof(float) * n);
+    float *op = (float *)malloc(sizeof(float) * n);
+    orc_minmax_box(src, mn, D, H, W, ndim, rx, ry, rz, 0);
+    orc_minmax_box(mn, op, D, H, W, ndim, rx, ry, rz, 1);
+    for (int64_t i = 0; i < n; ++i) dst[i] = src[i] - op[i];
+    free(mn); free(op);
+}
+
 /* gauss_otsu_labeling: _tier9/_gauss_otsu_labeling.py:36-45 -- blur with */
 /* outline_sigma on every axis, threshold_otsu, connected components    */
 /* (box).  Returns the number of labels.                                */

@@ -18,6 +18,7 @@ from ._ops import (binary_and, connected_components_labeling_box,
                    erode_box, eroded_otsu_labeling, extend_labeling_via_voronoi, gauss_otsu_labeling,
                    voronoi_labeling,
                    gaussian_blur, greater_constant, histogram, mask, masked_voronoi_labeling,
+                   maximum_box, minimum_box, top_hat_box,
                    masked_voronoi_labeling_binary,
                    maximum_of_all_pixels, minimum_of_all_pixels, radius_to_kernel_size,
                    relabel_sequential, scikit_image_threshold_otsu, sigma_to_kernel_size,

@@ -76,6 +76,10 @@ _SIGS = {
     "cle_greater_constant": (ctypes.c_int, [_T, _T, ctypes.c_float, _P]),
     "cle_binary_and": (ctypes.c_int, [_T, _T, _T, _P]),
     "cle_erode_box": (ctypes.c_int, [_T, _T, _P]),
+    "cle_box_filter_workspace_bytes": (_SZ, [_T]),
+    "cle_minimum_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
+    "cle_maximum_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
+    "cle_top_hat_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
     "cle_mask": (ctypes.c_int, [_T, _T, _T, _P]),
     "cle_detect_maxima_box_workspace_bytes": (_SZ, [_T, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "cle_detect_maxima_box": (ctypes.c_int, [_T, _T, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _SZ, _P]),

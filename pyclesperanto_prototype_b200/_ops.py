@@ -56,7 +56,8 @@ def sigma_to_kernel_size(sigma):
 
 
 def radius_to_kernel_size(radius):
-    return int(radius) * 2 + 1
+    """_tier0/_radius_to_kernel_size.py:1-2."""
+    return int(radius * 2 + 1)
 
 
 # ---------------------------------------------------------------------------
@@ -285,6 +286,39 @@ def voronoi_labeling(binary_source: Image, labeling_destination: Image = None) -
     """Connected components (box) of the binary image, then their Voronoi
     extension over the whole image (_tier5/_voronoi_labeling.py:8-40)."""
     return _grow_call("cle_voronoi_labeling", binary_source, labeling_destination)
+
+
+def _box_call(name, source, destination, rx, ry, rz):
+    s, d = _T(source), _T(destination)
+    ws = _ws("cle_box_filter_workspace_bytes", _lib.ref(s))
+    _call(name, _lib.ref(s), _lib.ref(d), float(rx), float(ry), float(rz), _ptr(ws), ws.numel(),
+          _lib.stream_ptr())
+    return destination
+
+
+@plugin_function(categories=['filter', 'in assistant'], native_inputs=("source",))
+def minimum_box(source: Image, destination: Image = None, radius_x: float = 0, radius_y: float = 0,
+                radius_z: float = 0) -> Image:
+    """Local minimum over a box of int(2*radius+1) voxels per axis, separable
+    (_tier1/_minimum_box.py:6-55)."""
+    return _box_call("cle_minimum_box", source, destination, radius_x, radius_y, radius_z)
+
+
+@plugin_function(categories=['filter', 'in assistant'], native_inputs=("source",))
+def maximum_box(source: Image, destination: Image = None, radius_x: float = 0, radius_y: float = 0,
+                radius_z: float = 0) -> Image:
+    """Local maximum over a box of int(2*radius+1) voxels per axis, separable
+    (_tier1/_maximum_box.py)."""
+    return _box_call("cle_maximum_box", source, destination, radius_x, radius_y, radius_z)
+
+
+@plugin_function(categories=['filter', 'background removal', 'in assistant'], priority=1,
+                 native_inputs=("source",))
+def top_hat_box(source: Image, destination: Image = None, radius_x: float = 1, radius_y: float = 1,
+                radius_z: float = 1) -> Image:
+    """Background subtraction: source minus its opening (maximum_box of
+    minimum_box), float32 (_tier2/_top_hat_box.py:6-43)."""
+    return _box_call("cle_top_hat_box", source, destination, radius_x, radius_y, radius_z)
 
 
 @plugin_function(categories=['binary processing'], output_creator=create_binary_like)

@@ -179,6 +179,40 @@ int cle_erode_box(const cle_tensor *src, const cle_tensor *dst, void *stream) {
     return erode_box(a, d, S(stream));
 }
 
+size_t cle_box_filter_workspace_bytes(const cle_tensor *src) {
+    Img im;
+    if (to_img(src, im, "source")) return 0;
+    return box_filter_workspace_bytes(im);
+}
+
+static int box_entry(const cle_tensor *src, const cle_tensor *dst, double rx, double ry, double rz, int kind,
+                     void *ws, size_t ws_bytes, void *stream) {
+    static const char *names[3] = {"minimum_box", "maximum_box", "top_hat_box"};
+    Img a, d;
+    CLE_TRY(to_img(src, a, "source"));
+    CLE_TRY(to_img(dst, d, "destination"));
+    CLE_TRY(ws_check(ws, ws_bytes, box_filter_workspace_bytes(a), names[kind]));
+    CLE_TRY(set_device_of(a, src));
+    Arena ar(ws, ws_bytes);
+    if (kind == 2) return top_hat_box(a, d, rx, ry, rz, ar, S(stream));
+    return box_filter(a, d, rx, ry, rz, kind == 1, ar, S(stream));
+}
+
+int cle_minimum_box(const cle_tensor *src, const cle_tensor *dst, double rx, double ry, double rz, void *ws,
+                    size_t ws_bytes, void *stream) {
+    return box_entry(src, dst, rx, ry, rz, 0, ws, ws_bytes, stream);
+}
+
+int cle_maximum_box(const cle_tensor *src, const cle_tensor *dst, double rx, double ry, double rz, void *ws,
+                    size_t ws_bytes, void *stream) {
+    return box_entry(src, dst, rx, ry, rz, 1, ws, ws_bytes, stream);
+}
+
+int cle_top_hat_box(const cle_tensor *src, const cle_tensor *dst, double rx, double ry, double rz, void *ws,
+                    size_t ws_bytes, void *stream) {
+    return box_entry(src, dst, rx, ry, rz, 2, ws, ws_bytes, stream);
+}
+
 // ---- detect_maxima_box -------------------------------------------------------
 size_t cle_detect_maxima_box_workspace_bytes(const cle_tensor *src, int rx, int ry, int rz) {
     Img im;

@@ -250,3 +250,22 @@ def test_voronoi_labeling_golden(oracle):
     src[0, 1, 1] = src[0, 1, 4] = src[0, 4, 1] = src[0, 4, 4] = 1
     ref = np.array([[[1, 1, 1, 3, 3, 3]] * 3 + [[2, 2, 2, 4, 4, 4]] * 3])
     assert np.array_equal(oracle.voronoi_labeling(src), ref)
+
+
+# ---- minimum_box / maximum_box / top_hat_box -----------------------------
+def test_minimum_maximum_box_golden(oracle):
+    # tests/test_minimum_box.py:4-31, tests/test_maximum_box.py:4-31
+    t = np.zeros((5, 5), np.float32)
+    t[1:4, 1:4] = 1
+    ref = np.zeros((5, 5))
+    ref[2, 2] = 1
+    assert np.array_equal(oracle.minimum_box(t, 1, 1, 0), ref)
+    assert np.array_equal(oracle.maximum_box(ref, 1, 1, 0), t)
+
+
+def test_top_hat_box_golden(oracle):
+    # tests/test_top_hat_box.py:4-22 (min 0, max 50)
+    t = np.array([[0, 0, 0, 0, 0], [0, 50, 50, 50, 0], [0, 50, 100, 50, 0], [0, 50, 50, 50, 0],
+                  [0, 0, 0, 0, 0]], np.float32)
+    r = oracle.top_hat_box(t, 1, 1, 0)
+    assert r.min() == 0 and r.max() == 50

@@ -170,3 +170,41 @@ def test_extend_labeling_via_voronoi_any_label_values(cle, oracle, shape):
     src = cle.B200Array(torch.from_numpy(lab).cuda())
     got = cle.pull(cle.extend_labeling_via_voronoi(src, cle.create_labels_like(src)))
     assert np.array_equal(got, oracle.extend_labeling_via_voronoi(lab))
+
+
+# ---------------------------------- minimum / maximum box, top-hat -------
+def test_box_reference_tests(cle):
+    # tests/test_minimum_box.py, test_maximum_box.py, test_top_hat_box.py of the reference
+    t = np.zeros((5, 5))
+    t[1:4, 1:4] = 1
+    ref = np.zeros((5, 5))
+    ref[2, 2] = 1
+    r = cle.create(cle.push(t))
+    cle.minimum_box(cle.push(t), r, 1, 1, 0)
+    assert np.array_equal(cle.pull(r), ref)
+    cle.maximum_box(cle.push(ref), r, 1, 1, 0)
+    assert np.array_equal(cle.pull(r), t)
+    h = cle.push(np.asarray([[0, 0, 0, 0, 0], [0, 50, 50, 50, 0], [0, 50, 100, 50, 0], [0, 50, 50, 50, 0],
+                             [0, 0, 0, 0, 0]]))
+    out = cle.create(h)
+    cle.top_hat_box(h, out, 1, 1, 0)
+    a = cle.pull(out)
+    assert a.min() == 0 and a.max() == 50
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("radii", [(1, 1, 1), (2.5, 0, 3.7), (0, 4, 1), (9, 7, 5), (40, 40, 40)])
+def test_box_filters_match_oracle(cle, oracle, shape, radii):
+    a = np.random.default_rng(8).normal(100, 30, shape).astype(np.float32)
+    assert np.array_equal(cle.pull(cle.minimum_box(a, None, *radii)), oracle.minimum_box(a, *radii))
+    assert np.array_equal(cle.pull(cle.maximum_box(a, None, *radii)), oracle.maximum_box(a, *radii))
+    assert np.array_equal(cle.pull(cle.top_hat_box(a, None, *radii)), oracle.top_hat_box(a, *radii))
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16])
+def test_top_hat_box_narrow_input_and_in_place(cle, oracle, dtype):
+    a = np.random.default_rng(9).integers(0, np.iinfo(dtype).max, (13, 70, 61)).astype(dtype)
+    assert np.array_equal(cle.pull(cle.top_hat_box(a, None, 5, 5, 2)), oracle.top_hat_box(a.astype(np.float32), 5, 5, 2))
+    f = cle.push(a.astype(np.float32))
+    cle.top_hat_box(f, f, 5, 5, 2)              # destination = source
+    assert np.array_equal(cle.pull(f), oracle.top_hat_box(a.astype(np.float32), 5, 5, 2))
