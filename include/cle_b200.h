@@ -165,6 +165,17 @@ int cle_mask(const cle_tensor *src, const cle_tensor *mask, const cle_tensor *ds
  * edge; source u8/u16/u32/i32/f32, destination u8/u16/u32/f32. */
 int cle_erode_box(const cle_tensor *src, const cle_tensor *dst, void *stream);
 
+/* ---- add_image_and_scalar / replace_intensities -------------------------
+ * add_image_and_scalar replaces _tier1/_add_image_and_scalar.py (dst = src +
+ * scalar in float32, saturating conversion to an integer destination);
+ * replace_intensities replaces _tier1/_replace_intensities.py (dst = map[(int) src]
+ * with the index clamped to the map, which is read along x of its first row,
+ * float32).  Together with the statistics they make the label_*_map
+ * functions of _tier9. */
+int cle_add_image_and_scalar(const cle_tensor *src, const cle_tensor *dst, float scalar, void *stream);
+int cle_replace_intensities(const cle_tensor *src, const cle_tensor *map, const cle_tensor *dst,
+                            void *stream);
+
 /* ---- minimum_box / maximum_box / top_hat_box ----------------------------
  * minimum_box replaces _tier1/_minimum_box.py:6-55, maximum_box
  * _tier1/_maximum_box.py, top_hat_box _tier2/_top_hat_box.py:6-43 (source minus

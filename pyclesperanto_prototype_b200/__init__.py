@@ -13,6 +13,12 @@ the library or a CUDA device the ops raise; there is no CPU fallback.
 from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, create_binary_like,
                      create_labels_like, create_like, create_none, create_zyx, is_image, nparray,
                      plugin_function, pull, pull_zyx, push, push_native, push_zyx)
+from ._ops import (STATISTICS_ENTRY, add_image_and_scalar, label_maximum_extension_map,
+                   label_maximum_extension_ratio_map, label_maximum_intensity_map,
+                   label_mean_extension_map, label_mean_intensity_map, label_minimum_intensity_map,
+                   label_pixel_count_map, label_standard_deviation_intensity_map, push_regionprops,
+                   push_regionprops_column, replace_intensities,
+                   statistics_of_background_and_labelled_pixels)
 from ._ops import (binary_and, connected_components_labeling_box,
                    connected_components_labeling_diamond, detect_maxima_box,
                    erode_box, eroded_otsu_labeling, extend_labeling_via_voronoi, gauss_otsu_labeling,

@@ -5,13 +5,14 @@ creator and return value; the work is one call into libcle_b200.so on the
 current torch CUDA stream.  Reference citations are on each function.
 """
 import warnings
+from enum import Enum
 
 import numpy as np
 import torch
 
 from . import _lib
 from ._tier0 import (B200Array, Image, create, create_binary_like, create_labels_like, create_like,
-                     create_none, plugin_function, push)
+                     create_none, plugin_function, push, push_native)
 
 STAT_KEYS = [
     "bbox_min_x", "bbox_min_y", "bbox_min_z", "bbox_max_x", "bbox_max_y", "bbox_max_z",
@@ -286,6 +287,187 @@ def voronoi_labeling(binary_source: Image, labeling_destination: Image = None) -
     """Connected components (box) of the binary image, then their Voronoi
     extension over the whole image (_tier5/_voronoi_labeling.py:8-40)."""
     return _grow_call("cle_voronoi_labeling", binary_source, labeling_destination)
+
+
+# ---- measurement tables and parametric label maps ------------------------
+class STATISTICS_ENTRY(Enum):
+    """Column index of each measurement in the pushed statistics table; the
+    same names and values as the reference's enum (_tier9/_statistics_entry.py),
+    which code indexing such tables relies on."""
+    IDENTIFIER = 0
+    BOUNDING_BOX_X = 1
+    BOUNDING_BOX_Y = 2
+    BOUNDING_BOX_Z = 3
+    BOUNDING_BOX_END_X = 4
+    BOUNDING_BOX_END_Y = 5
+    BOUNDING_BOX_END_Z = 6
+    BOUNDING_BOX_WIDTH = 7
+    BOUNDING_BOX_HEIGHT = 8
+    BOUNDING_BOX_DEPTH = 9
+    MINIMUM_INTENSITY = 10
+    MAXIMUM_INTENSITY = 11
+    MEAN_INTENSITY = 12
+    SUM_INTENSITY = 13
+    STANDARD_DEVIATION_INTENSITY = 14
+    PIXEL_COUNT = 15
+    SUM_INTENSITY_TIMES_X = 16
+    SUM_INTENSITY_TIMES_Y = 17
+    SUM_INTENSITY_TIMES_Z = 18
+    MASS_CENTER_X = 19
+    MASS_CENTER_Y = 20
+    MASS_CENTER_Z = 21
+    SUM_X = 22
+    SUM_Y = 23
+    SUM_Z = 24
+    CENTROID_X = 25
+    CENTROID_Y = 26
+    CENTROID_Z = 27
+    SUM_DISTANCE_TO_MASS_CENTER = 28
+    MEAN_DISTANCE_TO_MASS_CENTER = 29
+    MAX_DISTANCE_TO_MASS_CENTER = 30
+    MAX_MEAN_DISTANCE_TO_MASS_CENTER_RATIO = 31
+    SUM_DISTANCE_TO_CENTROID = 32
+    MEAN_DISTANCE_TO_CENTROID = 33
+    MAX_DISTANCE_TO_CENTROID = 34
+    MAX_MEAN_DISTANCE_TO_CENTROID_RATIO = 35
+    NUMBER_OF_ENTRIES = 36
+
+
+# statistics dict key of each table row, in STATISTICS_ENTRY order
+_ENTRY_KEYS = [
+    "original_label", "bbox_min_x", "bbox_min_y", "bbox_min_z", "bbox_max_x", "bbox_max_y",
+    "bbox_max_z", "bbox_width", "bbox_height", "bbox_depth", "min_intensity", "max_intensity",
+    "mean_intensity", "sum_intensity", "standard_deviation_intensity", "area",
+    "sum_intensity_times_x", "sum_intensity_times_y", "sum_intensity_times_z", "mass_center_x",
+    "mass_center_y", "mass_center_z", "sum_x", "sum_y", "sum_z", "centroid_x", "centroid_y",
+    "centroid_z", "sum_distance_to_mass_center", "mean_distance_to_mass_center",
+    "max_distance_to_mass_center", "mean_max_distance_to_mass_center_ratio",
+    "sum_distance_to_centroid", "mean_distance_to_centroid", "max_distance_to_centroid",
+    "mean_max_distance_to_centroid_ratio",
+]
+
+
+@plugin_function(categories=['filter', 'in assistant'])
+def add_image_and_scalar(source: Image, destination: Image = None, scalar: float = 1) -> Image:
+    """destination = source + scalar in float32 (_tier1/_add_image_and_scalar.py)."""
+    _call("cle_add_image_and_scalar", _lib.ref(_T(source)), _lib.ref(_T(destination)), float(scalar),
+          _lib.stream_ptr())
+    return destination
+
+
+@plugin_function(categories=['bia-bob-suggestion'])
+def replace_intensities(source: Image, new_values_vector: Image, destination: Image = None) -> Image:
+    """destination = new_values_vector[(int) source], the index clamped to the
+    vector (_tier1/_replace_intensities.py)."""
+    _call("cle_replace_intensities", _lib.ref(_T(source)), _lib.ref(_T(new_values_vector)),
+          _lib.ref(_T(destination)), _lib.stream_ptr())
+    return destination
+
+
+def statistics_of_background_and_labelled_pixels(source: Image = None, labelmap: Image = None):
+    """Statistics of the background (original_label 0) and every label
+    (_tier9/_statistics_of_background_and_labelled_pixels.py:9-45): the
+    statistics of labelmap + 1."""
+    from ._tier0 import push as _push
+    temp = add_image_and_scalar(_push(labelmap), scalar=1)
+    props = statistics_of_labelled_pixels(source, temp)
+    props["original_label"] = props["label"] - 1
+    return props
+
+
+def push_regionprops(props, first_row_index: int = 0) -> B200Array:
+    """The statistics as a 36-row table image, one column per label, rows in
+    STATISTICS_ENTRY order (_tier9/_push_regionprops.py:8-135).  Accepts the
+    statistics dict; the reference's scikit-image RegionProperties input is not
+    supported here."""
+    from ._tier0 import push as _push
+    if not isinstance(props, dict):
+        raise TypeError("push_regionprops: pass the dict returned by statistics_of_labelled_pixels")
+    return _push(np.asarray([np.asarray(props[k], np.float64) for k in _ENTRY_KEYS]))
+
+
+def push_regionprops_column(regionprops, column: str) -> B200Array:
+    """One measurement as a 1-row image (_tier9/_push_regionprops_column.py): for
+    the statistics dict its column as is; for a list of objects with `label`
+    (or `original_label`) the values placed at their labels."""
+    from ._tier0 import push as _push
+    if isinstance(regionprops, dict):
+        return _push(np.asarray([regionprops[column]]))
+    labels = [getattr(r, "original_label", None) if hasattr(r, "original_label") else r.label for r in regionprops]
+    values = np.zeros([int(np.max(labels)) + 1])
+    for lab, r in zip(labels, regionprops):
+        values[int(lab)] = getattr(r, column)
+    return _push(np.asarray([values]))
+
+
+def _label_map(intensity, labels, key, destination):
+    """replace_intensities(labels, column `key` of the statistics of labels + 1
+    with entry 0 set to 0): the label_*_map functions of _tier9, on the device
+    (no host round trip of the statistics)."""
+    from ._tier0 import push as _push
+    labels = _push(labels)
+    temp = add_image_and_scalar(labels, scalar=1)
+    n = _label_max(temp)
+    inten = temp if intensity is None else push_native(intensity)
+    table = statistics_table(inten, temp, n)          # [35, n]: column j = original label j
+    vec = table[STAT_KEYS.index(key)].reshape(1, n).clone()
+    vec[0, 0] = 0
+    if destination is None:
+        destination = create_like(labels)
+    return replace_intensities(labels, B200Array(vec), destination)
+
+
+@plugin_function(categories=['label measurement', 'map', 'in assistant'])
+def label_pixel_count_map(source: Image, destination: Image = None) -> Image:
+    """Every label replaced by its voxel count (_tier9/_label_pixel_count_map.py)."""
+    return _label_map(None, source, "area", destination)
+
+
+@plugin_function(categories=['combine', 'label measurement', 'map', 'in assistant'], priority=-1)
+def label_mean_intensity_map(source: Image, label_map: Image, destination: Image = None) -> Image:
+    """Every label replaced by its mean intensity (_tier9/_label_mean_intensity_map.py)."""
+    return _label_map(source, label_map, "mean_intensity", destination)
+
+
+@plugin_function(categories=['combine', 'label measurement', 'map', 'in assistant'], priority=-1)
+def label_minimum_intensity_map(intensity_image: Image, labels: Image, minimum_intensity_map: Image = None) -> Image:
+    """Every label replaced by its minimum intensity (_tier9/_label_minimum_intensity_map.py)."""
+    return _label_map(intensity_image, labels, "min_intensity", minimum_intensity_map)
+
+
+@plugin_function(categories=['combine', 'label measurement', 'map', 'in assistant'], priority=-1)
+def label_maximum_intensity_map(intensity_image: Image, labels: Image, maximum_intensity_map: Image = None) -> Image:
+    """Every label replaced by its maximum intensity (_tier9/_label_maximum_intensity_map.py)."""
+    return _label_map(intensity_image, labels, "max_intensity", maximum_intensity_map)
+
+
+@plugin_function(categories=['combine', 'label measurement', 'map', 'in assistant'], priority=-1)
+def label_standard_deviation_intensity_map(intensity_image: Image, labels: Image,
+                                           standard_deviation_intensity_map: Image = None) -> Image:
+    """Every label replaced by the standard deviation of its intensity
+    (_tier9/_label_standard_deviation_intensity_map.py)."""
+    return _label_map(intensity_image, labels, "standard_deviation_intensity", standard_deviation_intensity_map)
+
+
+@plugin_function(categories=['label measurement', 'map', 'in assistant'])
+def label_mean_extension_map(labels: Image, destination: Image = None) -> Image:
+    """Every label replaced by the mean distance of its voxels to its centroid
+    (_tier9/_label_mean_extension_map.py)."""
+    return _label_map(None, labels, "mean_distance_to_centroid", destination)
+
+
+@plugin_function(categories=['label measurement', 'map', 'in assistant'])
+def label_maximum_extension_map(labels: Image, destination: Image = None) -> Image:
+    """Every label replaced by the largest distance of its voxels to its
+    centroid (_tier9/_label_maximum_extension_map.py)."""
+    return _label_map(None, labels, "max_distance_to_centroid", destination)
+
+
+@plugin_function(categories=['label measurement', 'map', 'in assistant'])
+def label_maximum_extension_ratio_map(labels: Image, destination: Image = None) -> Image:
+    """Every label replaced by its maximum over mean distance to the centroid
+    (_tier9/_label_maximum_extension_ratio_map.py)."""
+    return _label_map(None, labels, "mean_max_distance_to_centroid_ratio", destination)
 
 
 def _box_call(name, source, destination, rx, ry, rz):

@@ -179,6 +179,23 @@ int cle_erode_box(const cle_tensor *src, const cle_tensor *dst, void *stream) {
     return erode_box(a, d, S(stream));
 }
 
+int cle_add_image_and_scalar(const cle_tensor *src, const cle_tensor *dst, float scalar, void *stream) {
+    Img a, d;
+    CLE_TRY(to_img(src, a, "source"));
+    CLE_TRY(to_img(dst, d, "destination"));
+    CLE_TRY(set_device_of(a, src));
+    return add_image_and_scalar(a, d, scalar, S(stream));
+}
+
+int cle_replace_intensities(const cle_tensor *src, const cle_tensor *map, const cle_tensor *dst, void *stream) {
+    Img a, m, d;
+    CLE_TRY(to_img(src, a, "source"));
+    CLE_TRY(to_img(map, m, "new_values_vector"));
+    CLE_TRY(to_img(dst, d, "destination"));
+    CLE_TRY(set_device_of(a, src));
+    return replace_intensities(a, m, d, S(stream));
+}
+
 size_t cle_box_filter_workspace_bytes(const cle_tensor *src) {
     Img im;
     if (to_img(src, im, "source")) return 0;

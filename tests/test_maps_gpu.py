@@ -1,0 +1,126 @@
+"""Parametric label maps, replace_intensities, add_image_and_scalar and the
+statistics table formats on the device: the reference's own fixtures, and the
+maps against the oracle's statistics of labels + 1 on seeded label images
+(rtol 1e-5 like every statistics comparison, same NaN / inf positions)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def cle():
+    import pyclesperanto_prototype_b200 as m
+    from pyclesperanto_prototype_b200 import _build
+    _build.build()
+    return m
+
+
+LAB2 = np.asarray([[1, 1, 2], [1, 0, 0], [3, 3, 0]])
+INT2 = np.asarray([[1, 1, 2], [4, 0, 0], [5, 3, 0]])
+
+
+def _close(a, b, rtol=1e-3):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.array_equal(np.isnan(a), np.isnan(b)) and np.allclose(a[~np.isnan(a)], b[~np.isnan(b)], rtol)
+
+
+# ---- the reference's fixtures (tests/test_label_*_map.py and friends) -----
+def test_replace_intensities_reference_test(cle):
+    src = cle.push(np.asarray([[0, 0, 0, 0, 0], [0, 1, 2, 3, 0], [0, 2, 3, 4, 0], [0, 4, 4, 5, 0],
+                               [0, 0, 0, 0, 0]]))
+    vec = cle.push(np.asarray([[0, 9, 8, 7, 6, 5]]))
+    out = cle.create(src)
+    cle.replace_intensities(src, vec, out)
+    ref = [[0, 0, 0, 0, 0], [0, 9, 8, 7, 0], [0, 8, 7, 6, 0], [0, 6, 6, 5, 0], [0, 0, 0, 0, 0]]
+    assert np.allclose(cle.pull(out), ref)
+
+
+@pytest.mark.parametrize("three_d", [False, True])
+def test_label_maps_reference_tests(cle, three_d):
+    lab, inten = LAB2, INT2
+    if three_d:                         # the 3D fixtures are the 2D ones as 3 planes of one row
+        lab, inten = lab[:, None, :], inten[:, None, :]
+    lab_r = lab.copy()
+    lab_r[1, ..., 2] = 2                # the extension-ratio fixture's labels
+    cases = [
+        (cle.label_mean_intensity_map(cle.push(inten), cle.push(lab)), [[2, 2, 2], [2, 0, 0], [4, 4, 0]]),
+        (cle.label_pixel_count_map(cle.push(lab)), [[3, 3, 1], [3, 0, 0], [2, 2, 0]]),
+        (cle.label_maximum_extension_map(cle.push(lab)),
+         [[0.74535596, 0.74535596, 0], [0.74535596, 0, 0], [0.5, 0.5, 0]]),
+        (cle.label_mean_extension_map(cle.push(lab)),
+         [[0.65403885, 0.65403885, 0], [0.65403885, 0, 0], [0.5, 0.5, 0]]),
+        (cle.label_maximum_extension_ratio_map(cle.push(lab_r)),
+         [[1.1396203, 1.1396203, 1], [1.1396203, 0, 1], [1, 1, 0]]),
+        (cle.label_standard_deviation_intensity_map(cle.push(inten), cle.push(lab)),
+         [[1.4142, 1.4142, 0], [1.4142, 0, 0], [1, 1, 0]]),
+    ]
+    for out, ref in cases:
+        ref = np.asarray(ref, np.float64)
+        if three_d:
+            ref = ref[:, None, :]
+        assert np.allclose(cle.pull(out), ref, 0.001)
+
+
+def test_statistics_of_background_and_labelled_pixels_reference_test(cle):
+    # tests/test_statistics_of_background_and_labelled_pixels.py: the table through push_regionprops
+    intensity = cle.push(np.asarray([[0, 1, 2], [1, 2, 3], [2, 3, 4]]))
+    labels = cle.push(np.asarray([[0, 0, 1], [0, 1, 1], [2, 2, 2]]))
+    ref = np.asarray([
+        [0, 1, 2], [0, 1, 0], [0, 0, 2], [0, 0, 0], [1, 2, 2], [1, 1, 2], [0, 0, 0], [2, 2, 3], [2, 2, 1],
+        [1, 1, 1], [0, 2, 2], [1, 3, 4], [0.6666667, 2.3333333, 3], [2, 7, 9],
+        [0.47140452, 0.4714045, 0.8164966], [3, 3, 3], [1, 12, 11], [1, 5, 18], [0, 0, 0],
+        [0.5, 1.7142857, 1.2222222], [0.5, 0.71428573, 2], [0, 0, 0], [1, 5, 3], [1, 2, 6], [0, 0, 0],
+        [0.33333334, 1.6666666, 1], [0.33333334, 0.6666667, 2], [0, 0, 0],
+        [2.1213202, 1.9426796, 2.2222223], [0.70710677, 0.6475599, 0.7407408],
+        [0.70710677, 0.7693094, 1.2222222], [1, 1.1880127, 1.6499999], [1.9621165, 1.9621165, 2],
+        [0.65403885, 0.65403885, 0.6666667], [0.74535596, 0.745356, 1], [1.1396203, 1.1396204, 1.5]])
+    props = cle.statistics_of_background_and_labelled_pixels(intensity, labels)
+    table = cle.pull(cle.push_regionprops(props, first_row_index=0))
+    assert table.shape == (36, 3)
+    assert np.allclose(table, ref, 0.0001)
+    assert cle.STATISTICS_ENTRY.MEAN_DISTANCE_TO_CENTROID.value == 33
+
+
+def test_push_regionprops_column_reference_test(cle):
+    labels = cle.push(np.asarray([[[4, 4, 2]], [[4, 1, 2]], [[3, 3, 4]]]))
+    props = cle.statistics_of_background_and_labelled_pixels(None, labels)
+    assert np.allclose(cle.pull(cle.push_regionprops_column(props, "area")), [[0, 1, 2, 2, 4]])
+
+
+def test_add_image_and_scalar(cle):
+    a = np.random.default_rng(1).normal(0, 100, (7, 33, 40)).astype(np.float32)
+    assert np.array_equal(cle.pull(cle.add_image_and_scalar(a, None, 2.5)), a + np.float32(2.5))
+
+
+# ---- maps against the oracle ---------------------------------------------
+MAPS = [("label_pixel_count_map", "area", False), ("label_mean_intensity_map", "mean_intensity", True),
+        ("label_minimum_intensity_map", "min_intensity", True),
+        ("label_maximum_intensity_map", "max_intensity", True),
+        ("label_standard_deviation_intensity_map", "standard_deviation_intensity", True),
+        ("label_mean_extension_map", "mean_distance_to_centroid", False),
+        ("label_maximum_extension_map", "max_distance_to_centroid", False),
+        ("label_maximum_extension_ratio_map", "mean_max_distance_to_centroid_ratio", False)]
+
+
+def _oracle_map(oracle, inten, lab, key):
+    temp = lab.astype(np.uint32) + 1
+    props = oracle.statistics_of_labelled_pixels(inten if inten is not None else temp.astype(np.float32), temp)
+    vec = np.asarray(props[key], np.float32).copy()
+    vec[0] = 0
+    return vec[lab.astype(np.int64)]
+
+
+@pytest.mark.parametrize("shape", [(40, 70), (6, 33, 50), (1, 5, 7), (130, 97)])
+@pytest.mark.parametrize("name,key,with_intensity", MAPS)
+def test_label_maps_match_oracle(cle, oracle, shape, name, key, with_intensity):
+    rng = np.random.default_rng(2)
+    lab = rng.integers(0, 12, shape).astype(np.uint32)
+    lab[lab == 5] = 0                   # a gap: label 5 absent
+    inten = rng.normal(200, 50, shape).astype(np.float32)
+    fn = getattr(cle, name)
+    got = cle.pull(fn(inten, lab) if with_intensity else fn(lab))
+    ref = _oracle_map(oracle, inten if with_intensity else None, lab, key)
+    assert _close(got, ref, RTOL)
