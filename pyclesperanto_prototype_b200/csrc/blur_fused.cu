@@ -14,8 +14,9 @@
 //     shared loads, for all kTY+2R rows (the y halo);
 //   * y pass: each thread produces kRY consecutive rows of one column from a
 //     register window;
-//   * z pass: a register ring of 2R+1 planes per owned column; the plane loop
-//     is unrolled by 2R+1 so every ring slot is a static register.
+//   * z pass: a register ring of 2R+1 planes per owned column, shifted by one
+//     slot per plane (the plane loop is not unrolled, which keeps the kernel's
+//     code small enough for the instruction caches).
 // Radius R (= sigma_to_kernel_size(sigma)/2) is a template parameter; radii
 // above kMaxFusedR or anisotropic sigmas use the three-pass path.
 #include "common.cuh"
@@ -113,11 +114,13 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
         for (int i = 0; i < WIN; ++i) ring[j][i] = 0.0f;
 
     load_plane(0);
-    for (int vb = 0; vb < nvirt; vb += WIN) {
-#pragma unroll
-        for (int k = 0; k < WIN; ++k) {
-            const int v = vb + k;
-            if (v < nvirt) {
+    // one plane per iteration, not unrolled (the loop body stays small enough
+    // for the instruction caches); the ring shifts by one slot per plane, so
+    // ring[j][i] holds plane v - 2R + i
+#pragma unroll 1
+    for (int v = 0; v < nvirt; ++v) {
+        {
+            {
                 __syncthreads();   // previous plane fully consumed
                 store_plane();
                 if (v + 1 < nvirt) load_plane(v + 1);
@@ -154,8 +157,13 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
                     float a = 0.f;
 #pragma unroll
                     for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], col[j + i], a);
-                    if constexpr (Z) ring[j][k] = a;
-                    else ring[j][0] = a;
+                    if constexpr (Z) {
+#pragma unroll
+                        for (int i = 0; i < WIN - 1; ++i) ring[j][i] = ring[j][i + 1];
+                        ring[j][WIN - 1] = a;
+                    } else {
+                        ring[j][0] = a;
+                    }
                 }
                 // z pass: output plane z0 + v - 2R once 2R+1 planes are held
                 if constexpr (Z) {
@@ -165,7 +173,7 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
                         for (int j = 0; j < kRY; ++j) {
                             float a = 0.f;
 #pragma unroll
-                            for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], ring[j][(k + 1 + i) % WIN], a);
+                            for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], ring[j][i], a);
                             const int y = y0 + ry0 + j;
                             if (col_ok && y < H) dst[(int64_t)zo * plane + (int64_t)y * W + x0 + tx] = a;
                         }
