@@ -147,9 +147,9 @@ __device__ __forceinline__ Seg make_seg(uint32_t l) {
     return s;
 }
 
+// 4 CTAs per SM (64 registers): more loads in flight for the latency-bound scan
 template <typename TL, typename TI>
-__global__ void // 4 CTAs per SM (64 registers): more loads in flight for the latency-bound scan
-__launch_bounds__(kST, 4)
+__global__ void __launch_bounds__(kST, 4)
 stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
             int64_t W, int64_t Lcap, Acc1 a, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
     const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
