@@ -10,11 +10,13 @@
 //     shared memory -- the next plane's raw values are loaded into registers
 //     while the current one is computed and converted to float32 only when
 //     stored, so no instruction waits on them early;
-//   * x pass: each thread produces 4 consecutive x outputs from 128-bit
-//     shared loads, for all kTY+2R rows (the y halo);
-//   * y pass: each thread produces kRY consecutive rows of one column from a
-//     register window;
-//   * z pass: a register ring of 2R+1 planes per owned column, shifted by one
+//   * x pass: each item produces 8 consecutive x outputs of one row as four
+//     packed pairs (fma.rn.f32x2: two independent round-to-nearest FMAs, the
+//     same rounding as fmaf) from 128-bit shared loads; the operand pair of an
+//     odd offset is formed from the loaded registers;
+//   * y pass: each thread produces kRY rows of a pair of adjacent columns,
+//     the pair packed, from a register window of 64-bit shared loads;
+//   * z pass: a register ring of 2R+1 planes per owned column pair, shifted by one
 //     slot per plane (the plane loop is not unrolled, which keeps the kernel's
 //     code small enough for the instruction caches).
 // Radius R (= sigma_to_kernel_size(sigma)/2) is a template parameter; radii
@@ -28,21 +30,24 @@ namespace {
 
 constexpr int kTX = 32;          // output columns per CTA
 constexpr int kTY = 32;          // output rows per CTA
-constexpr int kRY = 4;           // output rows per thread (y and z passes)
-constexpr int kThreads = kTX * (kTY / kRY);   // 256
+constexpr int kRY = 2;           // output rows per thread (y and z passes)
+constexpr int kCP = kTX / 2;     // column pairs per tile (y and z passes own a pair)
+constexpr int kXO = 8;           // x outputs per x-pass item
+constexpr int kThreads = kCP * (kTY / kRY);   // 256
 constexpr int kWarps = kThreads / 32;
 
 template <int R>
 struct Geom {
     static constexpr int ROWS = kTY + 2 * R;                     // staged rows
     static constexpr int COLS = kTX + 2 * R;                     // staged columns
-    static constexpr int QUADS = (4 + 2 * R + 3) / 4;            // float4 per x-pass thread
+    static constexpr int QUADS = (kXO + 2 * R + 3) / 4;          // float4 per x-pass item
     static constexpr int STRIDE = ((COLS + 3) / 4) * 4 + 4;      // In row stride (floats)
     static constexpr int ROWS_PER_WARP = (ROWS + kWarps - 1) / kWarps;
     static constexpr int COL_LOADS = (COLS + 31) / 32;
     static constexpr int LOADS = ROWS_PER_WARP * COL_LOADS;
     static constexpr int XO_STRIDE = kTX;                        // Xo row stride
     static constexpr size_t SMEM = sizeof(float) * (ROWS * STRIDE + ROWS * kTX);
+    static_assert(ROWS * (kTX / kXO) <= kThreads, "x pass: at most one item per thread");
 };
 
 // Two CTAs per SM (<= 128 registers, no spills) while the z ring is small.
@@ -102,16 +107,24 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
         }
     };
 
-    // y/z ownership: column tx, rows ry0 .. ry0+kRY-1
-    const int tx = tid % kTX;
-    const int ry0 = (tid / kTX) * kRY;
-    const bool col_ok = (x0 + tx) < W;
+    // y/z ownership: columns tx, tx+1 (a packed pair), rows ry0 .. ry0+kRY-1
+    const int tx = (tid % kCP) * 2;
+    const int ry0 = (tid / kCP) * kRY;
+    const bool c0_ok = (x0 + tx) < W, c1_ok = (x0 + tx + 1) < W;
+    const bool pair_store = c1_ok && (W & 1) == 0;     // 8-byte aligned float2 store
+    auto store2 = [&](int64_t off, float2 v) {
+        if (pair_store) *reinterpret_cast<float2 *>(dst + off) = v;
+        else {
+            if (c0_ok) dst[off] = v.x;
+            if (c1_ok) dst[off + 1] = v.y;
+        }
+    };
 
-    float ring[kRY][WIN];
+    float2 ring[kRY][WIN];
 #pragma unroll
     for (int j = 0; j < kRY; ++j)
 #pragma unroll
-        for (int i = 0; i < WIN; ++i) ring[j][i] = 0.0f;
+        for (int i = 0; i < WIN; ++i) ring[j][i] = make_float2(0.0f, 0.0f);
 
     load_plane(0);
     // one plane per iteration, not unrolled (the loop body stays small enough
@@ -119,72 +132,78 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
     // ring[j][i] holds plane v - 2R + i
 #pragma unroll 1
     for (int v = 0; v < nvirt; ++v) {
-        {
-            {
-                __syncthreads();   // previous plane fully consumed
-                store_plane();
-                if (v + 1 < nvirt) load_plane(v + 1);
-                __syncthreads();
-                // x pass: rows 0..ROWS-1, 4 outputs per item
-                for (int it = tid; it < G::ROWS * (kTX / 4); it += kThreads) {
-                    const int r = it / (kTX / 4);
-                    const int xq = (it - r * (kTX / 4)) * 4;
-                    float in[G::QUADS * 4];
-                    const float4 *rp = reinterpret_cast<const float4 *>(In + r * G::STRIDE + xq);
+        __syncthreads();   // previous plane fully consumed
+        store_plane();
+        if (v + 1 < nvirt) load_plane(v + 1);
+        __syncthreads();
+        // x pass: rows 0..ROWS-1, kXO outputs per item as packed pairs; the
+        // operand pair of an odd offset is formed from the loaded registers
+        if (tid < G::ROWS * (kTX / kXO)) {
+            const int r = tid / (kTX / kXO);
+            const int xq = (tid - r * (kTX / kXO)) * kXO;
+            float2 A[2 * G::QUADS];                    // A[k] = (v[xq+2k], v[xq+2k+1])
+            const float4 *pa = reinterpret_cast<const float4 *>(In + r * G::STRIDE + xq);
 #pragma unroll
-                    for (int q = 0; q < G::QUADS; ++q) {
-                        float4 f = rp[q];
-                        in[4 * q] = f.x; in[4 * q + 1] = f.y; in[4 * q + 2] = f.z; in[4 * q + 3] = f.w;
-                    }
-                    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+            for (int q = 0; q < G::QUADS; ++q) {
+                const float4 f = pa[q];
+                A[2 * q] = make_float2(f.x, f.y);
+                A[2 * q + 1] = make_float2(f.z, f.w);
+            }
+            float2 acc[kXO / 2];
 #pragma unroll
-                    for (int i = 0; i < WIN; ++i) {
-                        const float w = taps.w[i];
-                        a0 = __fmaf_rn(w, in[i], a0);
-                        a1 = __fmaf_rn(w, in[i + 1], a1);
-                        a2 = __fmaf_rn(w, in[i + 2], a2);
-                        a3 = __fmaf_rn(w, in[i + 3], a3);
-                    }
-                    *reinterpret_cast<float4 *>(Xo + r * kTX + xq) = make_float4(a0, a1, a2, a3);
+            for (int p = 0; p < kXO / 2; ++p) acc[p] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < WIN; ++i) {
+                const float2 w = make_float2(taps.w[i], taps.w[i]);
+#pragma unroll
+                for (int p = 0; p < kXO / 2; ++p) {
+                    const int o = 2 * p + i;               // operand (v[xq+o], v[xq+o+1])
+                    const float2 opnd = (o % 2 == 0) ? A[o / 2] : make_float2(A[o / 2].y, A[o / 2 + 1].x);
+                    acc[p] = __ffma2_rn(w, opnd, acc[p]);
                 }
-                __syncthreads();
-                // y pass: kRY rows of column tx into ring slot k
-                float col[kRY + 2 * R];
+            }
+            float4 *xo = reinterpret_cast<float4 *>(Xo + r * kTX + xq);
 #pragma unroll
-                for (int j = 0; j < kRY + 2 * R; ++j) col[j] = Xo[(ry0 + j) * kTX + tx];
+            for (int p = 0; p < kXO / 4; ++p)
+                xo[p] = make_float4(acc[2 * p].x, acc[2 * p].y, acc[2 * p + 1].x, acc[2 * p + 1].y);
+        }
+        __syncthreads();
+        // y pass: kRY rows of the column pair
+        float2 col[kRY + 2 * R];
+#pragma unroll
+        for (int j = 0; j < kRY + 2 * R; ++j) col[j] = *reinterpret_cast<const float2 *>(Xo + (ry0 + j) * kTX + tx);
+        float2 yv[kRY];
+#pragma unroll
+        for (int j = 0; j < kRY; ++j) {
+            float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < WIN; ++i) a = __ffma2_rn(make_float2(taps.w[i], taps.w[i]), col[j + i], a);
+            yv[j] = a;
+        }
+        if constexpr (Z) {
+#pragma unroll
+            for (int j = 0; j < kRY; ++j) {
+#pragma unroll
+                for (int i = 0; i < WIN - 1; ++i) ring[j][i] = ring[j][i + 1];
+                ring[j][WIN - 1] = yv[j];
+            }
+            // z pass: output plane z0 + v - 2R once 2R+1 planes are held
+            if (v >= 2 * R) {
+                const int zo = z0 + v - 2 * R;
 #pragma unroll
                 for (int j = 0; j < kRY; ++j) {
-                    float a = 0.f;
+                    float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-                    for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], col[j + i], a);
-                    if constexpr (Z) {
-#pragma unroll
-                        for (int i = 0; i < WIN - 1; ++i) ring[j][i] = ring[j][i + 1];
-                        ring[j][WIN - 1] = a;
-                    } else {
-                        ring[j][0] = a;
-                    }
+                    for (int i = 0; i < WIN; ++i) a = __ffma2_rn(make_float2(taps.w[i], taps.w[i]), ring[j][i], a);
+                    const int y = y0 + ry0 + j;
+                    if (c0_ok && y < H) store2((int64_t)zo * plane + (int64_t)y * W + x0 + tx, a);
                 }
-                // z pass: output plane z0 + v - 2R once 2R+1 planes are held
-                if constexpr (Z) {
-                    if (v >= 2 * R) {
-                        const int zo = z0 + v - 2 * R;
+            }
+        } else {
 #pragma unroll
-                        for (int j = 0; j < kRY; ++j) {
-                            float a = 0.f;
-#pragma unroll
-                            for (int i = 0; i < WIN; ++i) a = __fmaf_rn(taps.w[i], ring[j][i], a);
-                            const int y = y0 + ry0 + j;
-                            if (col_ok && y < H) dst[(int64_t)zo * plane + (int64_t)y * W + x0 + tx] = a;
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < kRY; ++j) {
-                        const int y = y0 + ry0 + j;
-                        if (col_ok && y < H) dst[(int64_t)y * W + x0 + tx] = ring[j][0];
-                    }
-                }
+            for (int j = 0; j < kRY; ++j) {
+                const int y = y0 + ry0 + j;
+                if (c0_ok && y < H) store2((int64_t)y * W + x0 + tx, yv[j]);
             }
         }
     }
