@@ -176,10 +176,14 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
         const bool box = (t & 1) == 0;
         // ---- phase A ---------------------------------------------------
         uint32_t changed = 0;
+        // the next round's list entry is loaded one round ahead, so a visit
+        // waits for one memory latency (its rows) instead of two
+        uint32_t bnext = (wbase + warp < nB) ? __ldcg(F + wbase + warp) : 0u;
         for (uint32_t base = wbase; base < nB; base += wstride) {
             const uint32_t idx = base + warp;
+            const uint32_t b = bnext;
+            bnext = (idx + wstride < nB) ? __ldcg(F + idx + wstride) : 0u;
             if (idx >= nB) continue;
-            const uint32_t b = __ldcg(F + idx);
             const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
             const uint32_t z = g.fH.div(r), y = r - z * g.H;
             const int x = (int)(xb * 32u) + lane;
