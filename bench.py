@@ -208,15 +208,18 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(x, world):
+    """Max of a host scalar over the ranks (NCCL: through the GPU; gloo: CPU)."""
     import torch
     if world == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -479,13 +482,14 @@ def run_batch(args):
 def run_served(args):
     import torch
     from pyclesperanto_prototype_b200 import synthetic
-    from pyclesperanto_prototype_b200.serving import Request, SegmentationServer, per_call_loop
-    torch.cuda.set_device(0)
+    from pyclesperanto_prototype_b200.serving import Request, SegmentationServer, per_call_loop, request_bytes
+    rank, world, local = dist_setup(args.gpus)
     w = WORKLOADS["served"]
     classes = [(512, 512), (64, 256, 256), (128, 512, 512), (256, 1024, 1024)]
     probs = [0.4, 0.3, 0.2, 0.1]
     pool_per_class = 3
-    pool = {c: [synthetic.blob_tile(c, 2e-4 if len(c) == 3 else 1e-3, seed=5000 + 10 * k + j)
+    pool = {c: [synthetic.blob_tile(c, 2e-4 if len(c) == 3 else 1e-3, seed=5000 + 10 * k + j,
+                                    device="cuda:%d" % torch.cuda.current_device())
                 .clamp_(0, 65535).to(torch.int32).to(torch.uint16).cpu().pin_memory()
                 for j in range(pool_per_class)] for k, c in enumerate(classes)}
     rng = np.random.default_rng(5)
@@ -506,18 +510,39 @@ def run_served(args):
     per_call_loop([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)], w["spot"],
                   w["outline"], realtime=False)
     torch.cuda.synchronize()
-    served = server.run(make(), realtime=True)
-    plain = per_call_loop(make(), w["spot"], w["outline"], realtime=True)
+    if world == 1:
+        served = server.run(make(), realtime=True)
+        plain = per_call_loop(make(), w["spot"], w["outline"], realtime=True)
+    else:
+        # replicas: every rank routes the same trace and serves its share
+        from pyclesperanto_prototype_b200.replicas import serve_replicated
+
+        class _PerCall:
+            def run(self, reqs, realtime=True):
+                return per_call_loop(reqs, w["spot"], w["outline"], realtime=realtime)
+
+        nbytes = lambda r: request_bytes(tuple(r.volume.shape), r.volume.dtype)
+        barrier(world)
+        served = serve_replicated(make(), lambda _: server, nbytes, 60e9)
+        barrier(world)
+        plain = serve_replicated(make(), lambda _: _PerCall(), nbytes, 60e9)
+        barrier(world)
+        import torch.distributed as dist
+        if rank != 0:
+            dist.destroy_process_group()
+            return
+    vox_of = {i: pool[c][j].numel() for i, (a, c, j) in enumerate(trace)}
+
     def summarize(reqs):
-        lat = np.array([r.latency for r in reqs]) * 1e3
+        lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
         span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
-        vox = sum(r.volume.numel() for r in reqs)
+        vox = sum(vox_of[r.rid] for r in reqs)
         return {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p95_ms": round(float(np.percentile(lat, 95)), 3),
                 "p99_ms": round(float(np.percentile(lat, 99)), 3), "mvoxels_per_s": round(vox / span / 1e6, 2),
                 "requests": len(reqs), "span_s": round(span, 3)}
     s, p = summarize(served), summarize(plain)
     same = all(a.num_labels == b.num_labels for a, b in zip(served, plain))
-    out = {"metric": METRIC, "value": s["mvoxels_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(trace),
+    out = {"metric": METRIC, "value": s["mvoxels_per_s"], "unit": UNIT, "n_gpus": world, "steps": len(trace),
            "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "b200",
            "form": "served (continuous batching: %d requests in flight, uploads and downloads on copy "
@@ -526,7 +551,12 @@ def run_served(args):
                       "volumes": "%d pre-generated per size class, reused" % pool_per_class},
            "served": s, "per_call_loop": p, "label_counts_equal": bool(same),
            "served_p99_below_per_call_p50": bool(s["p99_ms"] < p["p50_ms"])}
+    if world > 1:
+        out["form"] += "; %d replicas, requests routed by device memory (no data-path collective)" % world
     print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def _tissue_2d(width, height, dx, dy, seed):
