@@ -504,7 +504,7 @@ def run_served(args):
         return [Request(i, pool[c][j], arrival=a) for i, (a, c, j) in enumerate(trace)]
     warm = [Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)]
     server = SegmentationServer(budget_bytes=60e9, slots=args.lanes, compute_streams=args.compute_streams,
-                                spot_sigma=w["spot"],
+                                express_voxels=args.express_voxels, spot_sigma=w["spot"],
                                 outline_sigma=w["outline"])
     server.run(warm, realtime=False)
     per_call_loop([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)], w["spot"],
@@ -546,7 +546,8 @@ def run_served(args):
            "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "b200",
            "form": "served (continuous batching: %d requests in flight, uploads and downloads on copy "
-                   "streams overlapping %d compute stream(s), 60 GB budget)" % (args.lanes, args.compute_streams),
+                   "streams overlapping %d compute stream(s) plus an express lane for requests of <= %d "
+                   "voxels, 60 GB budget)" % (args.lanes, args.compute_streams, args.express_voxels),
            "config": {"workload": w["desc"], "rate_per_s": args.rate, "duration_s": args.duration,
                       "volumes": "%d pre-generated per size class, reused" % pool_per_class},
            "served": s, "per_call_loop": p, "label_counts_equal": bool(same),
@@ -719,6 +720,8 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0, help="served workload: trace length in s")
     ap.add_argument("--rate", type=float, default=200.0, help="served workload: arrivals per s")
     ap.add_argument("--compute-streams", type=int, default=1, help="served workload: compute streams")
+    ap.add_argument("--express-voxels", type=int, default=8 << 20,
+                    help="served workload: requests up to this size take the express lane (0: off)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

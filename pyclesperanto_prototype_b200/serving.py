@@ -16,7 +16,10 @@ at once, on three kinds of streams:
 So uploads and downloads overlap the computation of other requests, while
 the computations themselves run one after another on the whole GPU (one
 compute stream, the default) or two at a time (compute_streams=2, each
-cooperative launch then capped at half the SMs).  Device buffers (input,
+cooperative launch then capped at half the SMs).  With express_voxels > 0,
+requests of at most that many voxels take an express lane (their own upload
+and compute streams, cooperative launches on express_ctas SMs), so small
+requests do not queue behind large ones.  Device buffers (input,
 labels, workspaces, tables) are kept per shape and reused, so after warm-up
 no request allocates.  Completion is detected by polling CUDA events;
 latency = completion - arrival.  Each request's result is the same as the
@@ -93,7 +96,7 @@ def request_bytes(shape, dtype) -> int:
 class SegmentationServer:
     def __init__(self, budget_bytes: float = 60e9, slots: int = 4, spot_sigma: float = 2.0,
                  outline_sigma: float = 2.0, device=None, keep_labels: bool = False,
-                 compute_streams: int = 1):
+                 compute_streams: int = 1, express_voxels: int = 0, express_ctas: int = 16):
         _lib.load()
         self.keep_labels = keep_labels
         self.device = torch.device(device or "cuda", torch.cuda.current_device()) \
@@ -107,7 +110,18 @@ class SegmentationServer:
         self._next = 0
         self.pool = collections.defaultdict(list)    # (shape, dtype) -> [_Buffers] free
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        self.coop = max(1, sms // len(self.computes))
+        # express lane: requests of at most express_voxels get their own upload
+        # and compute streams, so they never wait behind a large request; its
+        # cooperative growth launches use express_ctas SMs, the others the rest
+        self.express_voxels = int(express_voxels)
+        self.express = None
+        reserve = 0
+        if self.express_voxels > 0:
+            self.express = (torch.cuda.Stream(device=self.device), torch.cuda.Stream(device=self.device))
+            self.express_ctas = max(1, min(int(express_ctas), sms // 2))
+            reserve = self.express_ctas
+        multi = len(self.computes) > 1 or self.express is not None
+        self.coop = max(1, (sms - reserve) // len(self.computes)) if multi else 0
 
     # -- buffers ----------------------------------------------------------
     def _take(self, shape, dtype):
@@ -123,12 +137,17 @@ class SegmentationServer:
     def _start(self, req: Request, k: int, t_ref: float):
         b = self._take(req.volume.shape, req.volume.dtype)
         lib = _lib.load()
-        with torch.cuda.stream(self.copy_in):
+        if self.express is not None and req.volume.numel() <= self.express_voxels:
+            up, s = self.express
+            lib.cle_set_cooperative_ctas(self.express_ctas)
+        else:
+            up, s = self.copy_in, self.computes[self._next]
+            self._next = (self._next + 1) % len(self.computes)
+            lib.cle_set_cooperative_ctas(self.coop)
+        with torch.cuda.stream(up):
             b.src.copy_(req.volume, non_blocking=True)
             uploaded = torch.cuda.Event()
-            uploaded.record(self.copy_in)
-        s = self.computes[self._next]
-        self._next = (self._next + 1) % len(self.computes)
+            uploaded.record(up)
         s.wait_event(uploaded)
         with torch.cuda.stream(s):
             vol_into(b.src, b.labels, b.ws, self.spot, self.outline, s.cuda_stream)
@@ -178,7 +197,7 @@ class SegmentationServer:
         not admitted before its arrival time.  Returns the requests with their
         admitted / done times (seconds since the start)."""
         lib = _lib.load()
-        lib.cle_set_cooperative_ctas(self.coop if len(self.computes) > 1 else 0)
+        lib.cle_set_cooperative_ctas(self.coop)
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         running = {}       # slot -> [req, buffers, event, bytes, stage]
         in_use = 0.0
