@@ -32,11 +32,12 @@ namespace cle {
 
 namespace {
 
-constexpr int kBT = 1024;                       // threads per CTA (one CTA per SM)
+constexpr int kBT = 1024;                       // threads per CTA
 constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kSlice = 256;                     // per-warp append slice (entries)
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
+constexpr size_t kWideBricks = size_t(4) << 20;  // 2 CTAs per SM above this many bricks
 constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 constexpr uint64_t kKernelLimitNs = 20000000000ull;
@@ -130,8 +131,10 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint
     ap.push(take, nb);
 }
 
-template <bool IS3D>
-__global__ void __launch_bounds__(kBT, 1)
+// MINB CTAs per SM: 1 (61 registers) for volumes whose labels mostly stay
+// in L2, 2 (32 registers, 2x the warps to hide DRAM latency) for larger ones.
+template <bool IS3D, int MINB>
+__global__ void __launch_bounds__(kBT, MINB)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
@@ -189,7 +192,12 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const int x = (int)(xb * 32u) + lane;
             const int xc = min(x, (int)g.W - 1);
             const bool inmask = x < (int)g.W && seg[r * g.W + (uint32_t)xc] != 0;
-            uint32_t rows[3 * (2 * ZR + 1)], lft[3 * (2 * ZR + 1)], rgt[3 * (2 * ZR + 1)];
+            // the 3x3 (3 in 2D) rows at x; the rows' values just outside the
+            // brick are loaded one per lane: lane k < K holds row k at the left
+            // neighbour (x - 1 of lane 0), lane 16 + k row k at the right one
+            // (x + 1 of lane 31), both clamped to the image
+            constexpr int K = 3 * (2 * ZR + 1);
+            uint32_t rows[K];
 #pragma unroll
             for (int dz = -ZR; dz <= ZR; ++dz)
 #pragma unroll
@@ -197,29 +205,43 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                     const int k = (dz + ZR) * 3 + (dy + 1);
                     const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
                     const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
-                    const uint32_t *row = lab + (zz * g.H + yy) * g.W;
-                    rows[k] = ld_cg(row + xc);
-                    lft[k] = (lane == 0) ? ld_cg(row + max(x - 1, 0)) : 0u;
-                    rgt[k] = (lane == 31) ? ld_cg(row + min(x + 1, (int)g.W - 1)) : 0u;
+                    rows[k] = ld_cg(lab + (zz * g.H + yy) * g.W + xc);
                 }
+            uint32_t side = 0;
+            {
+                const int k = lane & 15;
+                if (k < K) {
+                    const int dz = k / 3 - ZR, dy = k % 3 - 1;
+                    const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
+                    const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
+                    const int xs = lane < 16 ? max((int)(xb * 32u) - 1, 0) : min((int)(xb * 32u) + 32, (int)g.W - 1);
+                    side = ld_cg(lab + (zz * g.H + yy) * g.W + (uint32_t)xs);
+                }
+            }
             const int kc = ZR * 3 + 1;          // centre row
             const bool cand = inmask && rows[kc] == 0u;
             uint32_t out = 0;
             bool remain = false, pend = false;
             if (__any_sync(0xffffffffu, cand)) {
-                uint32_t bm = 0, dm = 0;
+                // outside values: the centre row's, then the maximum over the rows
+                const uint32_t sc = __shfl_sync(0xffffffffu, side, (lane & 16) + kc);
+                uint32_t ms = side;
 #pragma unroll
-                for (int k = 0; k < 3 * (2 * ZR + 1); ++k) {
-                    const uint32_t c = rows[k];
-                    const uint32_t up = __shfl_up_sync(0xffffffffu, c, 1);
-                    const uint32_t dn = __shfl_down_sync(0xffffffffu, c, 1);
-                    const uint32_t l = (lane == 0) ? lft[k] : up;
-                    const uint32_t rr = (lane == 31) ? rgt[k] : dn;
-                    bm = max(bm, max(c, max(l, rr)));
-                    const int dz = k / 3 - ZR, dy = k % 3 - 1;
-                    if (dz == 0 && dy == 0) dm = max(dm, max(l, rr));
-                    else if (dz == 0 || dy == 0) dm = max(dm, c);
-                }
+                for (int o = 8; o > 0; o >>= 1) ms = max(ms, __shfl_xor_sync(0xffffffffu, ms, o));
+                // (now lanes 0-15 hold the left maximum, lanes 16-31 the right one)
+                // box: the maximum over the rows, then over x - 1 .. x + 1
+                uint32_t mc = rows[0];
+#pragma unroll
+                for (int k = 1; k < K; ++k) mc = max(mc, rows[k]);
+                const uint32_t mu = __shfl_up_sync(0xffffffffu, mc, 1);
+                const uint32_t md = __shfl_down_sync(0xffffffffu, mc, 1);
+                const uint32_t bm = max(mc, max(lane == 0 ? ms : mu, lane == 31 ? ms : md));
+                // face: the centre row at x +- 1 and the 2 (4 in 3D) face rows at x
+                const uint32_t cu = __shfl_up_sync(0xffffffffu, rows[kc], 1);
+                const uint32_t cd = __shfl_down_sync(0xffffffffu, rows[kc], 1);
+                uint32_t dm = max(lane == 0 ? sc : cu, lane == 31 ? sc : cd);
+                dm = max(dm, max(rows[kc - 1], rows[kc + 1]));
+                if (ZR) dm = max(dm, max(rows[kc - 3 * ZR], rows[kc + 3 * ZR]));
                 bool pl = false;
                 if (cand) {
                     const uint32_t m = box ? bm : dm;
@@ -324,12 +346,15 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     G.fWB = FastDiv(G.WB);
     G.is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    const void *kern = G.is3d ? (const void *)voronoi_bricks_kernel<true>
-                              : (const void *)voronoi_bricks_kernel<false>;
-    static bool attr[2] = {false, false};
-    if (!attr[G.is3d]) {
+    const int wide = nb > kWideBricks ? 1 : 0;
+    const void *kerns[2][2] = {
+        {(const void *)voronoi_bricks_kernel<false, 1>, (const void *)voronoi_bricks_kernel<false, 2>},
+        {(const void *)voronoi_bricks_kernel<true, 1>, (const void *)voronoi_bricks_kernel<true, 2>}};
+    const void *kern = kerns[G.is3d][wide];
+    static bool attr[2][2] = {{false, false}, {false, false}};
+    if (!attr[G.is3d][wide]) {
         CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
-        attr[G.is3d] = true;
+        attr[G.is3d][wide] = true;
     }
     int dev = 0;
     CLE_CUDA(cudaGetDevice(&dev));
@@ -337,7 +362,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, kBBufBytes));
     if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
-    const int grid = (int)std::min<int64_t>(want, cooperative_ctas(dev));
+    const int grid = (int)std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev));
     unsigned long long *trace =
         (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv, &Pf,
