@@ -300,10 +300,10 @@ def run_b200(args):
         k = lib.cle_profile_stage_ms(stage_buf, 16)
         stage_ms.append([stage_buf[i] for i in range(k)])
     launches = lib.cle_kernel_launches() - n0
-    trace = (ctypes.c_uint64 * (3 * 256))()
+    trace = (ctypes.c_uint64 * (4 * 256))()
     lib.cle_profile_trace(trace, ctypes.sizeof(trace))
-    vor_trace = [(int(trace[3 * i]), int(trace[3 * i + 1]), int(trace[3 * i + 2])) for i in range(256)
-                 if trace[3 * i] or trace[3 * i + 1]]
+    vor_trace = [tuple(int(v) for v in trace[4 * i:4 * i + 4]) for i in range(256)
+                 if trace[4 * i] or trace[4 * i + 1]]
     barrier(world)
     t_pad = time.perf_counter()
     while len(clocks.lines) < 3 and time.perf_counter() - t_pad < 3.0:

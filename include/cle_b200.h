@@ -92,8 +92,9 @@ void cle_set_cooperative_ctas(int max_ctas);
 int cle_profile_enable(int flags);
 int cle_profile_stage_ms(float *out, int max);
 /* Per-step trace of the last device loop (Voronoi growth) while profiling is
- * enabled: triples of uint64 (ns since the loop started, frontier size,
- * voxels changed) per step, zero after the last step.  Synchronous; returns
+ * enabled: 4 uint64 per step (ns since the loop started at the end of the
+ * step's compute phase, frontier size, voxels changed, ns at the end of its
+ * write / queueing phase), zero after the last step.  Synchronous; returns
  * the bytes copied.  Profiling allocates its own trace buffer (outside any
  * workspace; bit 1 of cle_profile_enable). */
 int cle_profile_trace(void *host, size_t bytes);

@@ -220,8 +220,10 @@ __global__ void to_labels_kernel(const T *__restrict__ src, uint32_t *__restrict
 
 constexpr int kSeedWarps = 8;
 
-// One seed voxel per 32-voxel row brick that holds a label: its 3x3x3 brick
-// neighbourhood covers every voxel next to a label.  One global atomic per CTA.
+// One seed voxel per 8-voxel row segment (x aligned to 8) that holds a label;
+// the segment lies in one growth brick (8 x by 4 y), so the 3x3x3 brick
+// neighbourhood of the seed's brick covers every voxel next to a label of the
+// segment.  A warp reads 32 x of one row.  One global atomic per CTA.
 __global__ void __launch_bounds__(kSeedWarps * 32)
 brick_seeds_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t WB, FastDiv fWB, uint32_t nb,
                    uint32_t *__restrict__ seeds, uint32_t *__restrict__ d_count) {
@@ -236,16 +238,17 @@ brick_seeds_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t WB, Fa
         if (b < nb) {
             const uint32_t r = fWB.div(b), xb = b - r * WB, x = xb * 32u + (uint32_t)lane;
             const unsigned bal = __ballot_sync(0xffffffffu, x < W && lab[r * W + x] != 0u);
-            has = bal != 0u;
-            if (has && lane == 0) {
-                m = r * W + xb * 32u + (uint32_t)(__ffs(bal) - 1);
+            const unsigned seg8 = (bal >> (lane & 24)) & 0xFFu;   // this lane's 8-voxel segment
+            has = (lane & 7) == 0 && seg8 != 0u;
+            if (has) {
+                m = r * W + xb * 32u + (uint32_t)(lane & 24) + (uint32_t)(__ffs(seg8) - 1);
                 pos = atomicAdd(&s_n, 1u);
             }
         }
         __syncthreads();
         if (threadIdx.x == 0) s_base = s_n ? atomicAdd(d_count, s_n) : 0u;
         __syncthreads();
-        if (has && lane == 0) seeds[s_base + pos] = m;
+        if (has) seeds[s_base + pos] = m;
     }
 }
 
@@ -260,7 +263,7 @@ ExtLayout take_ext_layout(Arena &a, const Img &im) {
     ExtLayout l;
     l.sc = a.take<Scalars>(1);
     l.seg = a.take<uint8_t>(im.n());
-    l.seeds = a.take<uint32_t>((im.n() + 31) / 32 + (size_t)(im.D * im.H));
+    l.seeds = a.take<uint32_t>((im.n() + 7) / 8 + (size_t)(im.D * im.H));
     l.lab = a.take<uint32_t>(im.n());
     return l;
 }

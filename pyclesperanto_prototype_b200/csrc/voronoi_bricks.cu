@@ -6,10 +6,13 @@
 // The reference's Jacobi steps (box stencil on even steps, face stencil on odd
 // steps, a voxel rewritten only while 0 with the maximum over the stencil
 // including itself, stop at the first step that changes nothing) run on
-// "row bricks": 32 consecutive x voxels of one (z, y) row, one warp each.
+// bricks of 8 x by 4 y voxels of one z plane, one warp each (lane = 8 y + x).
 // Only active bricks are visited -- those that may hold a voxel able to change
-// in this step -- so the work per step follows the growth front, and a warp's
-// neighbour reads are 9 coalesced row segments (x +- 1 by warp shuffles).
+// in this step -- so the work per step follows the growth front.  A front
+// crosses an 8x4x1 brick in fewer steps than a 32-voxel row, so a brick is
+// visited fewer times (on the nuclei volume 0.72M visits instead of 1.26M);
+// a warp reads per z plane its 32 voxels as 4 aligned 32-byte row segments
+// plus the brick's halo, and x / y neighbours come by warp shuffles.
 //
 // A step is two phases separated by grid barriers:
 //   A  every active brick computes its candidates' new values from the state
@@ -52,12 +55,24 @@ struct BState {
     uint32_t pad[3];
 };
 
+constexpr int kBX = 8;                          // brick: 8 x ...
+constexpr int kBY = 4;                          // ... by 4 y voxels of one z plane
+static_assert(kBX == 8 && kBY == 4, "the brick-edge lane masks assume 8x4 bricks");
+
 struct BGeo {
     Geo g;
-    uint32_t WB;        // bricks per row
-    FastDiv fWB;
+    uint32_t WB, HB;    // bricks along x, along y
+    FastDiv fWB, fHB;
     int is3d;
 };
+
+// brick b -> (z, yb, xb)
+__device__ __forceinline__ void brick_zyx(const BGeo &G, uint32_t b, uint32_t &z, uint32_t &yb, uint32_t &xb) {
+    const uint32_t r = G.fWB.div(b);
+    xb = b - r * G.WB;
+    z = G.fHB.div(r);
+    yb = r - z * G.HB;
+}
 
 // Per-warp append slice in shared memory, flushed to a global list by the
 // warp alone, so no CTA barrier sits inside the brick loops.
@@ -112,19 +127,19 @@ __device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
     return s;   // thread 0
 }
 
-// Queues bricks (z+dz, y+dy, xb+dxb) for the step tagged `tag`; lane k of the
-// warp handles offset k of the 3x3x3 neighbourhood when want.  Warp-wide.
-__device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint32_t y, uint32_t xb,
+// Queues bricks (z+dz, yb+dyb, xb+dxb) for the step tagged `tag`; lane k of
+// the warp handles offset k of the 3x3x3 neighbourhood when want.  Warp-wide.
+__device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint32_t yb, uint32_t xb,
                                                  bool want, uint32_t tag, uint32_t *bstep,
                                                  WarpAppender &ap) {
     const int lane = threadIdx.x & 31;
     bool take = false;
     uint32_t nb = 0;
     if (want && lane < 27) {
-        const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
-        const int zz = (int)z + dz, yy = (int)y + dy, xx = (int)xb + dxb;
-        if (zz >= 0 && yy >= 0 && xx >= 0 && zz < (int)G.g.D && yy < (int)G.g.H && xx < (int)G.WB) {
-            nb = ((uint32_t)zz * G.g.H + (uint32_t)yy) * G.WB + (uint32_t)xx;
+        const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+        const int zz = (int)z + dz, yy = (int)yb + dyb, xx = (int)xb + dxb;
+        if (zz >= 0 && yy >= 0 && xx >= 0 && zz < (int)G.g.D && yy < (int)G.HB && xx < (int)G.WB) {
+            nb = ((uint32_t)zz * G.HB + (uint32_t)yy) * G.WB + (uint32_t)xx;
             take = atomicMax(bstep + nb, tag) < tag;
         }
     }
@@ -155,7 +170,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             uint32_t x, y, z;
             m2xyz(g, __ldcg(seeds + i), x, y, z);
             const bool want = lane < 27 && (IS3D || (lane / 9) == 1);
-            queue_neighbours(G, z, y, x >> 5, want, 1u, bstep, ap);
+            queue_neighbours(G, z, y / kBY, x / kBX, want, 1u, bstep, ap);
         }
         ap.maybe_flush(B0, &S->sizes[0]);
     }
@@ -187,61 +202,57 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const uint32_t b = bnext;
             bnext = (idx + wstride < nB) ? __ldcg(F + idx + wstride) : 0u;
             if (idx >= nB) continue;
-            const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
-            const uint32_t z = g.fH.div(r), y = r - z * g.H;
-            const int x = (int)(xb * 32u) + lane;
-            const int xc = min(x, (int)g.W - 1);
-            const bool inmask = x < (int)g.W && seg[r * g.W + (uint32_t)xc] != 0;
-            // the 3x3 (3 in 2D) rows at x; the rows' values just outside the
-            // brick are loaded one per lane: lane k < K holds row k at the left
-            // neighbour (x - 1 of lane 0), lane 16 + k row k at the right one
-            // (x + 1 of lane 31), both clamped to the image
-            constexpr int K = 3 * (2 * ZR + 1);
-            uint32_t rows[K];
+            uint32_t z, yb, xb;
+            brick_zyx(G, b, z, yb, xb);
+            const int xl = lane & (kBX - 1), yl = lane / kBX;
+            const int x = (int)(xb * kBX) + xl, y = (int)(yb * kBY) + yl;
+            const int xc = min(x, (int)g.W - 1), yc = min(y, (int)g.H - 1);
+            const bool inmask = x < (int)g.W && y < (int)g.H &&
+                                seg[((uint32_t)z * g.H + (uint32_t)yc) * g.W + (uint32_t)xc] != 0;
+            // per z plane: c the lane's voxel; h the halo row's voxel (lanes of
+            // the first / last brick row: y - 1 / y + 1); s the halo column's
+            // (lanes of the first / last brick column: x - 1 / x + 1); q the halo
+            // corner (lanes in both); all clamped to the image
+            constexpr int K = 2 * ZR + 1;
+            const bool yedge = yl == 0 || yl == kBY - 1, xedge = xl == 0 || xl == kBX - 1;
+            const uint32_t yh = (uint32_t)(yl == 0 ? max(y - 1, 0) : min(y + 1, (int)g.H - 1));
+            const uint32_t xs = (uint32_t)(xl == 0 ? max(x - 1, 0) : min(x + 1, (int)g.W - 1));
+            uint32_t c[K], h[K], sd[K], q[K];
 #pragma unroll
-            for (int dz = -ZR; dz <= ZR; ++dz)
-#pragma unroll
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const int k = (dz + ZR) * 3 + (dy + 1);
-                    const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
-                    const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
-                    rows[k] = ld_cg(lab + (zz * g.H + yy) * g.W + xc);
-                }
-            uint32_t side = 0;
-            {
-                const int k = lane & 15;
-                if (k < K) {
-                    const int dz = k / 3 - ZR, dy = k % 3 - 1;
-                    const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
-                    const uint32_t yy = (uint32_t)clampi((int)y + dy, 0, (int)g.H - 1);
-                    const int xs = lane < 16 ? max((int)(xb * 32u) - 1, 0) : min((int)(xb * 32u) + 32, (int)g.W - 1);
-                    side = ld_cg(lab + (zz * g.H + yy) * g.W + (uint32_t)xs);
-                }
+            for (int dz = -ZR; dz <= ZR; ++dz) {
+                const int k = dz + ZR;
+                const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
+                const uint32_t *P = lab + zz * g.H * g.W;
+                c[k] = ld_cg(P + (uint32_t)yc * g.W + (uint32_t)xc);
+                h[k] = yedge ? ld_cg(P + yh * g.W + (uint32_t)xc) : 0u;
+                sd[k] = xedge ? ld_cg(P + (uint32_t)yc * g.W + xs) : 0u;
+                q[k] = (yedge && xedge) ? ld_cg(P + yh * g.W + xs) : 0u;
             }
-            const int kc = ZR * 3 + 1;          // centre row
-            const bool cand = inmask && rows[kc] == 0u;
+            const int kc = ZR;                  // centre plane
+            const bool cand = inmask && c[kc] == 0u;
             uint32_t out = 0;
             bool remain = false, pend = false;
             if (__any_sync(0xffffffffu, cand)) {
-                // outside values: the centre row's, then the maximum over the rows
-                const uint32_t sc = __shfl_sync(0xffffffffu, side, (lane & 16) + kc);
-                uint32_t ms = side;
+                // box: the maximum over the planes, then over x - 1 .. x + 1 (the
+                // lane's row and its halo row), then over y - 1 .. y + 1
+                uint32_t cz = c[0], hz = h[0], sz = sd[0], qz = q[0];
 #pragma unroll
-                for (int o = 8; o > 0; o >>= 1) ms = max(ms, __shfl_xor_sync(0xffffffffu, ms, o));
-                // (now lanes 0-15 hold the left maximum, lanes 16-31 the right one)
-                // box: the maximum over the rows, then over x - 1 .. x + 1
-                uint32_t mc = rows[0];
-#pragma unroll
-                for (int k = 1; k < K; ++k) mc = max(mc, rows[k]);
-                const uint32_t mu = __shfl_up_sync(0xffffffffu, mc, 1);
-                const uint32_t md = __shfl_down_sync(0xffffffffu, mc, 1);
-                const uint32_t bm = max(mc, max(lane == 0 ? ms : mu, lane == 31 ? ms : md));
-                // face: the centre row at x +- 1 and the 2 (4 in 3D) face rows at x
-                const uint32_t cu = __shfl_up_sync(0xffffffffu, rows[kc], 1);
-                const uint32_t cd = __shfl_down_sync(0xffffffffu, rows[kc], 1);
-                uint32_t dm = max(lane == 0 ? sc : cu, lane == 31 ? sc : cd);
-                dm = max(dm, max(rows[kc - 1], rows[kc + 1]));
-                if (ZR) dm = max(dm, max(rows[kc - 3 * ZR], rows[kc + 3 * ZR]));
+                for (int k = 1; k < K; ++k) {
+                    cz = max(cz, c[k]); hz = max(hz, h[k]); sz = max(sz, sd[k]); qz = max(qz, q[k]);
+                }
+                const bool x0 = xl == 0, x1 = xl == kBX - 1, y0 = yl == 0, y1 = yl == kBY - 1;
+                const uint32_t cl = __shfl_up_sync(0xffffffffu, cz, 1), cr = __shfl_down_sync(0xffffffffu, cz, 1);
+                const uint32_t hl = __shfl_up_sync(0xffffffffu, hz, 1), hr = __shfl_down_sync(0xffffffffu, hz, 1);
+                const uint32_t rx = max(cz, max(x0 ? sz : cl, x1 ? sz : cr));
+                const uint32_t hx = max(hz, max(x0 ? qz : hl, x1 ? qz : hr));
+                const uint32_t ru = __shfl_up_sync(0xffffffffu, rx, kBX), rd = __shfl_down_sync(0xffffffffu, rx, kBX);
+                const uint32_t bm = max(rx, max(y0 ? hx : ru, y1 ? hx : rd));
+                // face: the centre plane at x +- 1 and y +- 1, the planes z +- 1 at (x, y)
+                const uint32_t v = c[kc];
+                const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1), fr = __shfl_down_sync(0xffffffffu, v, 1);
+                const uint32_t fu = __shfl_up_sync(0xffffffffu, v, kBX), fd = __shfl_down_sync(0xffffffffu, v, kBX);
+                uint32_t dm = max(max(x0 ? sd[kc] : fl, x1 ? sd[kc] : fr), max(y0 ? h[kc] : fu, y1 ? h[kc] : fd));
+                if (ZR) dm = max(dm, max(c[0], c[K - 1]));
                 bool pl = false;
                 if (cand) {
                     const uint32_t m = box ? bm : dm;
@@ -264,9 +275,9 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
         if (!ok) break;
         const uint32_t nchanged = __ldcg(&S->changes[t & 3]);
         if (trace && gtid == 0 && t < kTraceSteps) {
-            trace[3 * t] = global_ns() - t_start;
-            trace[3 * t + 1] = nB;
-            trace[3 * t + 2] = nchanged;
+            trace[4 * t] = global_ns() - t_start;
+            trace[4 * t + 1] = nB;
+            trace[4 * t + 2] = nchanged;
         }
         if (nchanged == 0u) { done = true; break; }
         // ---- phase B ---------------------------------------------------
@@ -282,25 +293,34 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                 const uint32_t b = __ldcg(F + idx);
                 const uint32_t m = Mv[(size_t)idx * 32 + lane];
                 const bool pend = __ldcg(Pf + idx) != 0u;
-                const uint32_t r = G.fWB.div(b), xb = b - r * G.WB;
-                const uint32_t z = g.fH.div(r), y = r - z * g.H;
-                if (m) st_cg(lab + r * g.W + xb * 32u + (uint32_t)lane, m);
+                uint32_t z, yb, xb;
+                brick_zyx(G, b, z, yb, xb);
+                const uint32_t x = xb * kBX + (uint32_t)(lane & (kBX - 1)), y = yb * kBY + (uint32_t)(lane / kBX);
+                if (m) st_cg(lab + ((uint32_t)z * g.H + y) * g.W + x, m);
                 const unsigned ch = __ballot_sync(0xffffffffu, m != 0u);
                 bool want = false;
                 if (lane < 27) {
-                    const int dz = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+                    const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
                     if (IS3D || dz == 0) {
-                        if (ch) want = dxb == 0 || (dxb < 0 && (ch & 1u)) || (dxb > 0 && (ch >> 31));
-                        if (pend && dz == 0 && dy == 0 && dxb == 0) want = true;
+                        // changed voxels next to brick (dyb, dxb): the first / last
+                        // brick row and column (any voxel for the planes z +- 1)
+                        unsigned sel = ch;
+                        if (dyb < 0) sel &= 0x000000FFu;
+                        else if (dyb > 0) sel &= 0xFF000000u;
+                        if (dxb < 0) sel &= 0x01010101u;
+                        else if (dxb > 0) sel &= 0x80808080u;
+                        want = sel != 0u;
+                        if (pend && dz == 0 && dyb == 0 && dxb == 0) want = true;
                     }
                 }
-                queue_neighbours(G, z, y, xb, want, tag, bstep, ap);
+                queue_neighbours(G, z, yb, xb, want, tag, bstep, ap);
             }
             ap.maybe_flush(Fn, nsize);
         }
         ap.flush(Fn, nsize);
         if (!tail) ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
         else __syncthreads();
+        if (trace && gtid == 0 && t < kTraceSteps) trace[4 * t + 3] = global_ns() - t_start;
         ++t;
     }
     if (gtid == 0) {
@@ -311,8 +331,9 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
     }
 }
 
-uint32_t bricks_per_row(const Img &im) { return (uint32_t)((im.W + 31) / 32); }
-uint32_t brick_count(const Img &im) { return (uint32_t)(im.D * im.H) * bricks_per_row(im); }
+uint32_t bricks_x(const Img &im) { return (uint32_t)((im.W + kBX - 1) / kBX); }
+uint32_t bricks_y(const Img &im) { return (uint32_t)((im.H + kBY - 1) / kBY); }
+uint32_t brick_count(const Img &im) { return (uint32_t)im.D * bricks_y(im) * bricks_x(im); }
 
 }  // namespace
 
@@ -342,8 +363,10 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     CLE_CUDA(cudaMemsetAsync(bstep, 0, sizeof(uint32_t) * nb, st));
     BGeo G;
     G.g = make_geo(im);
-    G.WB = bricks_per_row(im);
+    G.WB = bricks_x(im);
+    G.HB = bricks_y(im);
     G.fWB = FastDiv(G.WB);
+    G.fHB = FastDiv(G.HB);
     G.is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
     const int wide = nb > kWideBricks ? 1 : 0;
@@ -364,7 +387,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
     const int grid = (int)std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev));
     unsigned long long *trace =
-        (unsigned long long *)profile_trace_buffer(3 * kTraceSteps * sizeof(unsigned long long), st);
+        (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv, &Pf,
                     &bstep, &S, &d_status, &max_steps, &trace};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
