@@ -40,7 +40,6 @@ constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kSlice = 256;                     // per-warp append slice (entries)
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
-constexpr size_t kWideBricks = size_t(4) << 20;  // 2 CTAs per SM above this many bricks
 constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 constexpr uint64_t kKernelLimitNs = 20000000000ull;
@@ -146,10 +145,9 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint
     ap.push(take, nb);
 }
 
-// MINB CTAs per SM: 1 (61 registers) for volumes whose labels mostly stay
-// in L2, 2 (32 registers, 2x the warps to hide DRAM latency) for larger ones.
-template <bool IS3D, int MINB>
-__global__ void __launch_bounds__(kBT, MINB)
+// One CTA per SM: 2 CTAs (32 registers) spill and ran slower on both volumes.
+template <bool IS3D>
+__global__ void __launch_bounds__(kBT, 1)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
@@ -369,15 +367,12 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     G.fHB = FastDiv(G.HB);
     G.is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    const int wide = nb > kWideBricks ? 1 : 0;
-    const void *kerns[2][2] = {
-        {(const void *)voronoi_bricks_kernel<false, 1>, (const void *)voronoi_bricks_kernel<false, 2>},
-        {(const void *)voronoi_bricks_kernel<true, 1>, (const void *)voronoi_bricks_kernel<true, 2>}};
-    const void *kern = kerns[G.is3d][wide];
-    static bool attr[2][2] = {{false, false}, {false, false}};
-    if (!attr[G.is3d][wide]) {
+    const void *kern = G.is3d ? (const void *)voronoi_bricks_kernel<true>
+                              : (const void *)voronoi_bricks_kernel<false>;
+    static bool attr[2] = {false, false};
+    if (!attr[G.is3d]) {
         CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
-        attr[G.is3d][wide] = true;
+        attr[G.is3d] = true;
     }
     int dev = 0;
     CLE_CUDA(cudaGetDevice(&dev));
