@@ -40,6 +40,7 @@ constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kSlice = 256;                     // per-warp append slice (entries)
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
+constexpr size_t kWideBricks = size_t(2) << 20;  // 2 CTAs per SM above this many bricks
 constexpr uint32_t kTraceSteps = 256;
 constexpr uint64_t kBarrierLimitNs = 4000000000ull;
 constexpr uint64_t kKernelLimitNs = 20000000000ull;
@@ -145,9 +146,11 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint
     ap.push(take, nb);
 }
 
-// One CTA per SM: 2 CTAs (32 registers) spill and ran slower on both volumes.
-template <bool IS3D>
-__global__ void __launch_bounds__(kBT, 1)
+// MINB CTAs per SM: 1 for volumes whose labels mostly stay in L2 (a visit
+// waits on L2 hits), 2 for larger ones (2x the warps to hide DRAM latency;
+// the kernel fits 32 registers without spills).
+template <bool IS3D, int MINB>
+__global__ void __launch_bounds__(kBT, MINB)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
@@ -207,37 +210,47 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const int xc = min(x, (int)g.W - 1), yc = min(y, (int)g.H - 1);
             const bool inmask = x < (int)g.W && y < (int)g.H &&
                                 seg[((uint32_t)z * g.H + (uint32_t)yc) * g.W + (uint32_t)xc] != 0;
-            // per z plane: c the lane's voxel; h the halo row's voxel (lanes of
-            // the first / last brick row: y - 1 / y + 1); s the halo column's
-            // (lanes of the first / last brick column: x - 1 / x + 1); q the halo
-            // corner (lanes in both); all clamped to the image
+            // per z plane: c the lane's voxel, and one voxel of the brick's halo
+            // per lane (28 of them, clamped to the image): lanes 0-7 the row
+            // y - 1, 8-15 the row y + 4, 16-19 the column x - 1, 20-23 the
+            // column x + 8, 24-27 the corners; lanes that need a halo voxel
+            // fetch it by shuffle
             constexpr int K = 2 * ZR + 1;
-            const bool yedge = yl == 0 || yl == kBY - 1, xedge = xl == 0 || xl == kBX - 1;
-            const uint32_t yh = (uint32_t)(yl == 0 ? max(y - 1, 0) : min(y + 1, (int)g.H - 1));
-            const uint32_t xs = (uint32_t)(xl == 0 ? max(x - 1, 0) : min(x + 1, (int)g.W - 1));
-            uint32_t c[K], h[K], sd[K], q[K];
+            const int x0b = (int)(xb * kBX), y0b = (int)(yb * kBY);
+            int hx_ = x0b, hy_ = y0b;
+            if (lane < 8) { hx_ = x0b + lane; hy_ = y0b - 1; }
+            else if (lane < 16) { hx_ = x0b + lane - 8; hy_ = y0b + kBY; }
+            else if (lane < 24) { hx_ = lane < 20 ? x0b - 1 : x0b + kBX; hy_ = y0b + (lane & 3); }
+            else { hx_ = (lane & 1) ? x0b + kBX : x0b - 1; hy_ = (lane & 2) ? y0b + kBY : y0b - 1; }
+            const uint32_t hoff = (uint32_t)clampi(hy_, 0, (int)g.H - 1) * g.W + (uint32_t)clampi(hx_, 0, (int)g.W - 1);
+            uint32_t c[K], hv[K];
 #pragma unroll
             for (int dz = -ZR; dz <= ZR; ++dz) {
                 const int k = dz + ZR;
                 const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
                 const uint32_t *P = lab + zz * g.H * g.W;
                 c[k] = ld_cg(P + (uint32_t)yc * g.W + (uint32_t)xc);
-                h[k] = yedge ? ld_cg(P + yh * g.W + (uint32_t)xc) : 0u;
-                sd[k] = xedge ? ld_cg(P + (uint32_t)yc * g.W + xs) : 0u;
-                q[k] = (yedge && xedge) ? ld_cg(P + yh * g.W + xs) : 0u;
+                hv[k] = lane < 28 ? ld_cg(P + hoff) : 0u;
             }
             const int kc = ZR;                  // centre plane
             const bool cand = inmask && c[kc] == 0u;
             uint32_t out = 0;
             bool remain = false, pend = false;
             if (__any_sync(0xffffffffu, cand)) {
+                // the halo voxels this lane needs: h its halo row's (first /
+                // last brick row), s its halo column's (first / last brick
+                // column), q the corner (both)
+                const int src_h = yl == 0 ? xl : 8 + xl;
+                const int src_s = (xl == 0 ? 16 : 20) + (yl & 3);
+                const int src_q = 24 + (yl == kBY - 1 ? 2 : 0) + (xl == kBX - 1 ? 1 : 0);
                 // box: the maximum over the planes, then over x - 1 .. x + 1 (the
                 // lane's row and its halo row), then over y - 1 .. y + 1
-                uint32_t cz = c[0], hz = h[0], sz = sd[0], qz = q[0];
+                uint32_t cz = c[0], hm = hv[0];
 #pragma unroll
-                for (int k = 1; k < K; ++k) {
-                    cz = max(cz, c[k]); hz = max(hz, h[k]); sz = max(sz, sd[k]); qz = max(qz, q[k]);
-                }
+                for (int k = 1; k < K; ++k) { cz = max(cz, c[k]); hm = max(hm, hv[k]); }
+                const uint32_t hz = __shfl_sync(0xffffffffu, hm, src_h);
+                const uint32_t sz = __shfl_sync(0xffffffffu, hm, src_s);
+                const uint32_t qz = __shfl_sync(0xffffffffu, hm, src_q);
                 const bool x0 = xl == 0, x1 = xl == kBX - 1, y0 = yl == 0, y1 = yl == kBY - 1;
                 const uint32_t cl = __shfl_up_sync(0xffffffffu, cz, 1), cr = __shfl_down_sync(0xffffffffu, cz, 1);
                 const uint32_t hl = __shfl_up_sync(0xffffffffu, hz, 1), hr = __shfl_down_sync(0xffffffffu, hz, 1);
@@ -249,7 +262,9 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                 const uint32_t v = c[kc];
                 const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1), fr = __shfl_down_sync(0xffffffffu, v, 1);
                 const uint32_t fu = __shfl_up_sync(0xffffffffu, v, kBX), fd = __shfl_down_sync(0xffffffffu, v, kBX);
-                uint32_t dm = max(max(x0 ? sd[kc] : fl, x1 ? sd[kc] : fr), max(y0 ? h[kc] : fu, y1 ? h[kc] : fd));
+                const uint32_t hc = __shfl_sync(0xffffffffu, hv[kc], src_h);
+                const uint32_t sc = __shfl_sync(0xffffffffu, hv[kc], src_s);
+                uint32_t dm = max(max(x0 ? sc : fl, x1 ? sc : fr), max(y0 ? hc : fu, y1 ? hc : fd));
                 if (ZR) dm = max(dm, max(c[0], c[K - 1]));
                 bool pl = false;
                 if (cand) {
@@ -367,12 +382,15 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     G.fHB = FastDiv(G.HB);
     G.is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
-    const void *kern = G.is3d ? (const void *)voronoi_bricks_kernel<true>
-                              : (const void *)voronoi_bricks_kernel<false>;
-    static bool attr[2] = {false, false};
-    if (!attr[G.is3d]) {
+    const int wide = nb > kWideBricks ? 1 : 0;
+    const void *kerns[2][2] = {
+        {(const void *)voronoi_bricks_kernel<false, 1>, (const void *)voronoi_bricks_kernel<false, 2>},
+        {(const void *)voronoi_bricks_kernel<true, 1>, (const void *)voronoi_bricks_kernel<true, 2>}};
+    const void *kern = kerns[G.is3d][wide];
+    static bool attr[2][2] = {{false, false}, {false, false}};
+    if (!attr[G.is3d][wide]) {
         CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
-        attr[G.is3d] = true;
+        attr[G.is3d][wide] = true;
     }
     int dev = 0;
     CLE_CUDA(cudaGetDevice(&dev));
