@@ -20,7 +20,10 @@
 //     slot per plane (the plane loop is not unrolled, which keeps the kernel's
 //     code small enough for the instruction caches).
 // Radius R (= sigma_to_kernel_size(sigma)/2) is a template parameter; radii
-// above kMaxFusedR or anisotropic sigmas use the three-pass path.
+// above kMaxFusedR or anisotropic sigmas use the three-pass path.  Given a
+// partial buffer, each CTA also reduces the exact min / max of the values it
+// stores (the global min / max of the result in a one-CTA finish), which
+// saves threshold_otsu's separate pass over the blurred image.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -57,7 +60,7 @@ constexpr int min_ctas() { return R <= 8 ? 2 : 1; }
 template <typename Tin, int R, bool Z>
 __global__ void __launch_bounds__(kThreads, min_ctas<R>())
 blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, int H, int W,
-                  int zchunk, const __grid_constant__ Taps taps) {
+                  int zchunk, const __grid_constant__ Taps taps, float *__restrict__ mm) {
     using G = Geom<R>;
     constexpr int WIN = 2 * R + 1;
     extern __shared__ __align__(16) float smem[];
@@ -112,11 +115,17 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
     const int ry0 = (tid / kCP) * kRY;
     const bool c0_ok = (x0 + tx) < W, c1_ok = (x0 + tx + 1) < W;
     const bool pair_store = c1_ok && (W & 1) == 0;     // 8-byte aligned float2 store
+    float vmin = INFINITY, vmax = -INFINITY;   // of the stored values (when mm)
     auto store2 = [&](int64_t off, float2 v) {
         if (pair_store) *reinterpret_cast<float2 *>(dst + off) = v;
         else {
             if (c0_ok) dst[off] = v.x;
             if (c1_ok) dst[off + 1] = v.y;
+        }
+        if (mm) {
+            vmin = fminf(vmin, v.x);
+            vmax = fmaxf(vmax, v.x);
+            if (c1_ok) { vmin = fminf(vmin, v.y); vmax = fmaxf(vmax, v.y); }
         }
     };
 
@@ -207,47 +216,72 @@ blur_fused_kernel(const Tin *__restrict__ src, float *__restrict__ dst, int D, i
             }
         }
     }
+    if (mm) {
+        __shared__ float s_mn[kWarps], s_mx[kWarps];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        }
+        if (lane == 0) { s_mn[warp] = vmin; s_mx[warp] = vmax; }
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 1; w < kWarps; ++w) { vmin = fminf(vmin, s_mn[w]); vmax = fmaxf(vmax, s_mx[w]); }
+            const int64_t cta = ((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+            mm[2 * cta] = vmin;
+            mm[2 * cta + 1] = vmax;
+        }
+    }
 }
 
-template <typename Tin, int R, bool Z>
-int launch_fused_r(const Img &src, float *dst, const Taps &t, cudaStream_t st) {
-    using G = Geom<R>;
-    auto kern = blur_fused_kernel<Tin, R, Z>;
-    static bool attr_set = false;   // per instantiation
-    if (!attr_set) {
-        CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
-        attr_set = true;
-    }
+// Grid of the fused launch: (x tiles, y tiles, z chunks); the chunks give about
+// 2 x the resident CTAs while keeping the 2R halo planes below ~1/2 of a chunk.
+dim3 fused_grid(const Img &src, int R, int &zchunk) {
     const int gx = (int)((src.W + kTX - 1) / kTX);
     const int gy = (int)((src.H + kTY - 1) / kTY);
-    int zchunk = 1, gz = 1;
-    if (Z) {
+    int gz = 1;
+    zchunk = 1;
+    if (src.ndim == 3) {
         int dev = 0;
         cudaGetDevice(&dev);
-        const int64_t target = (int64_t)num_sms(dev) * 2 * min_ctas<R>();   // CTAs
+        const int64_t target = (int64_t)num_sms(dev) * 2 * (R <= 8 ? 2 : 1);   // CTAs
         int64_t chunks = (target + (int64_t)gx * gy - 1) / ((int64_t)gx * gy);
-        // keep the halo overhead (2R planes per chunk) below ~1/2
         const int64_t max_chunks = std::max<int64_t>(1, src.D / std::max(2 * R, 1));
         chunks = std::min(chunks, max_chunks);
         chunks = std::max<int64_t>(1, std::min<int64_t>(chunks, src.D));
         zchunk = (int)((src.D + chunks - 1) / chunks);
         gz = (int)((src.D + zchunk - 1) / zchunk);
     }
-    if (gy > 65535 || gz > 65535) { set_error("gaussian_blur: image too large for the fused path"); return CLE_ERR_TOO_LARGE; }
-    kern<<<dim3(gx, gy, gz), kThreads, G::SMEM, st>>>((const Tin *)src.data, dst, (int)src.D, (int)src.H,
-                                                       (int)src.W, zchunk, t);
+    return dim3(gx, gy, gz);
+}
+
+template <typename Tin, int R, bool Z>
+int launch_fused_r(const Img &src, float *dst, const Taps &t, float *mm, cudaStream_t st) {
+    using G = Geom<R>;
+    static_assert(min_ctas<R>() == (R <= 8 ? 2 : 1), "fused_grid's occupancy rule");
+    auto kern = blur_fused_kernel<Tin, R, Z>;
+    static bool attr_set = false;   // per instantiation
+    if (!attr_set) {
+        CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+        attr_set = true;
+    }
+    int zchunk = 1;
+    const dim3 grid = fused_grid(src, R, zchunk);
+    if (grid.y > 65535 || grid.z > 65535) { set_error("gaussian_blur: image too large for the fused path"); return CLE_ERR_TOO_LARGE; }
+    kern<<<grid, kThreads, G::SMEM, st>>>((const Tin *)src.data, dst, (int)src.D, (int)src.H, (int)src.W,
+                                          zchunk, t, mm);
     CLE_LAUNCH_CHECK("gaussian_blur fused");
     return CLE_OK;
 }
 
 template <typename Tin, bool Z, int R = 1>
-int dispatch_r(const Img &src, float *dst, const Taps &t, int r, cudaStream_t st) {
+int dispatch_r(const Img &src, float *dst, const Taps &t, int r, float *mm, cudaStream_t st) {
     if constexpr (R > kMaxFusedR) {
         set_error("internal: fused radius out of range");
         return CLE_ERR_ARG;
     } else {
-        if (r == R) return launch_fused_r<Tin, R, Z>(src, dst, t, st);
-        return dispatch_r<Tin, Z, R + 1>(src, dst, t, r, st);
+        if (r == R) return launch_fused_r<Tin, R, Z>(src, dst, t, mm, st);
+        return dispatch_r<Tin, Z, R + 1>(src, dst, t, r, mm, st);
     }
 }
 
@@ -261,17 +295,46 @@ bool fused_blur_applies(const Img &src, double sx, double sy, double sz) {
     return r >= 1 && r <= kMaxFusedR && src.W < (1 << 30) && src.H < (1 << 30);
 }
 
-int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st) {
+int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st, float *mm) {
     Taps t;
     CLE_TRY(make_gauss_taps(sigma, t));
     const int r = (t.n - 1) / 2;
     const bool z = src.ndim == 3;
     switch (src.dtype) {
-        case CLE_F32: return z ? dispatch_r<float, true>(src, dst, t, r, st) : dispatch_r<float, false>(src, dst, t, r, st);
-        case CLE_U16: return z ? dispatch_r<uint16_t, true>(src, dst, t, r, st) : dispatch_r<uint16_t, false>(src, dst, t, r, st);
-        case CLE_U8: return z ? dispatch_r<uint8_t, true>(src, dst, t, r, st) : dispatch_r<uint8_t, false>(src, dst, t, r, st);
+        case CLE_F32: return z ? dispatch_r<float, true>(src, dst, t, r, mm, st) : dispatch_r<float, false>(src, dst, t, r, mm, st);
+        case CLE_U16: return z ? dispatch_r<uint16_t, true>(src, dst, t, r, mm, st) : dispatch_r<uint16_t, false>(src, dst, t, r, mm, st);
+        case CLE_U8: return z ? dispatch_r<uint8_t, true>(src, dst, t, r, mm, st) : dispatch_r<uint8_t, false>(src, dst, t, r, mm, st);
         default: set_error("gaussian_blur: unsupported source dtype"); return CLE_ERR_DTYPE;
     }
+}
+
+size_t blur_minmax_workspace_bytes(const Img &src) {
+    // any sigma: the three-pass path with the separate min / max, or the
+    // fused partials (at most 4 CTAs per SM's worth of z chunks per tile)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int64_t tiles = ((src.W + kTX - 1) / kTX) * ((src.H + kTY - 1) / kTY);
+    const int64_t chunks = std::min<int64_t>(std::max<int64_t>(src.D, 1),
+                                             ((int64_t)num_sms(dev) * 4 + tiles - 1) / tiles);
+    const size_t fused = sizeof(float) * 2 * (size_t)(tiles * chunks) + 256;
+    return std::max(fused, separable_workspace_bytes(src) + minmax_workspace_bytes(src));
+}
+
+int blur_minmax(const Img &src, float *dst, double sigma, float *d_minmax, Arena &ws, cudaStream_t st) {
+    if (!fused_blur_applies(src, sigma, sigma, sigma)) {
+        CLE_TRY(gaussian_blur(src, dst, sigma, sigma, sigma, ws, st));
+        Img T = src;
+        T.data = dst;
+        T.dtype = CLE_F32;
+        return minmax(T, d_minmax, ws, st);
+    }
+    int zchunk = 1;
+    const dim3 g = fused_grid(src, (sigma_to_kernel_size(sigma) - 1) / 2, zchunk);
+    const int ctas = (int)(g.x * g.y * g.z);
+    float *partial = ws.take<float>(2 * (size_t)ctas);
+    if (!ws.ok()) { set_error("gaussian_blur: workspace too small"); return CLE_ERR_WORKSPACE; }
+    CLE_TRY(fused_blur(src, dst, sigma, st, partial));
+    return minmax_finish(partial, ctas, d_minmax, st);
 }
 
 }  // namespace cle

@@ -15,7 +15,12 @@ int gaussian_blur(const Img &src, float *dst, double sx, double sy, double sz, A
 // blur_fused.cu (isotropic sigma, radius <= kMaxFusedR, one launch)
 constexpr int kMaxFusedR = 14;
 bool fused_blur_applies(const Img &src, double sx, double sy, double sz);
-int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st);
+// mm (optional): 2 floats per CTA, the CTA's min / max of the result
+int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st, float *mm = nullptr);
+// Isotropic blur whose {min, max} lands in d_minmax (device): the fused
+// launch's CTA partials and a one-CTA finish, or blur + minmax otherwise.
+size_t blur_minmax_workspace_bytes(const Img &src);
+int blur_minmax(const Img &src, float *dst, double sigma, float *d_minmax, Arena &ws, cudaStream_t st);
 
 // reduce.cu
 struct MinMaxScratch {
@@ -25,6 +30,8 @@ struct MinMaxScratch {
 size_t minmax_workspace_bytes(const Img &im);
 // Writes {min, max} to d_out (device) without host synchronisation.
 int minmax(const Img &im, float *d_out, Arena &ws, cudaStream_t st);
+// {min, max} of `blocks` partial pairs into d_out (one CTA).
+int minmax_finish(const float *partial, int blocks, float *d_out, cudaStream_t st);
 size_t histogram_workspace_bytes(const Img &im, int bins);
 // Row-partial histogram + float32 row sum (reference order); d_minmax holds {min,max}.
 int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Arena &ws,

@@ -357,6 +357,7 @@ size_t vol_workspace_bytes(const Img &im) {
     size_t tail = 0;
     tail = std::max(tail, separable_workspace_bytes(im));
     tail = std::max(tail, minmax_workspace_bytes(im) + histogram_workspace_bytes(im, 256));
+    tail = std::max(tail, blur_minmax_workspace_bytes(im));
     tail = std::max(tail, rank_workspace_bytes(fkey_bits_for(im.n())));
     tail = std::max(tail, voronoi_frontier_workspace_bytes(im));
     return base + tail;
@@ -391,12 +392,12 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     Si.dtype = CLE_U8;
     CLE_TRY(detect_maxima(Ti, Si, st));
     stage_mark(2, st);
-    CLE_TRY(gaussian_blur(src, l.T, outline_sigma, outline_sigma, outline_sigma, ws, st));
+    // the outline blur also reduces the blurred image's min / max (step 4)
+    CLE_TRY(blur_minmax(src, l.T, outline_sigma, l.sc->minmax, ws, st));
     ws.off = tail_off;
     stage_mark(3, st);
 
     // 4-6: threshold on the device
-    CLE_TRY(minmax(Ti, l.sc->minmax, ws, st));
     CLE_TRY(histogram(Ti, 256, l.sc->minmax, l.sc->hist, ws, st));
     ws.off = tail_off;
     CLE_TRY(otsu(l.sc->hist, l.sc->minmax, &l.sc->thr, &l.sc->thr32, st));

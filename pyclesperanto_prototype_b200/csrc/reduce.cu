@@ -339,6 +339,12 @@ size_t minmax_workspace_bytes(const Img &im) {
     return a.off;
 }
 
+int minmax_finish(const float *partial, int blocks, float *d_out, cudaStream_t st) {
+    minmax_final_kernel<<<1, 1024, 0, st>>>(partial, blocks, d_out);
+    CLE_LAUNCH_CHECK("minmax finish");
+    return CLE_OK;
+}
+
 int minmax(const Img &im, float *d_out, Arena &ws, cudaStream_t st) {
     const int blocks = minmax_blocks(im.n());
     float *partial = ws.take<float>(2 * (size_t)blocks);

@@ -35,7 +35,8 @@ struct Acc1 {
 struct Acc2 {
     double *sdc, *sdm, *ssq;
     unsigned long long *mdc, *mdm;   // non-negative doubles as bit patterns
-    float *cx, *cy, *cz, *mx, *my, *mz, *mean, *area;
+    float4 *pc;                      // per label: centroid x, y, z, mean intensity
+    float4 *pm;                      // per label: mass centre x, y, z, area
 };
 
 Acc1 take_acc1(Arena &a, int64_t L) {
@@ -66,14 +67,8 @@ Acc2 take_acc2(Arena &a, int64_t L) {
     c.ssq = a.take<double>(L);
     c.mdc = a.take<unsigned long long>(L);
     c.mdm = a.take<unsigned long long>(L);
-    c.cx = a.take<float>(L);
-    c.cy = a.take<float>(L);
-    c.cz = a.take<float>(L);
-    c.mx = a.take<float>(L);
-    c.my = a.take<float>(L);
-    c.mz = a.take<float>(L);
-    c.mean = a.take<float>(L);
-    c.area = a.take<float>(L);
+    c.pc = a.take<float4>(L);
+    c.pm = a.take<float4>(L);
     return c;
 }
 
@@ -122,6 +117,30 @@ struct Seg {
         for (int o = 1; o < 32; o <<= 1) {
             float t = __shfl_up_sync(0xffffffffu, v, o);
             if (lane - o >= hl) v = fmaxf(v, t);
+        }
+        return v;
+    }
+    __device__ __forceinline__ uint32_t scan_addu(uint32_t v) const {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane - o >= hl) v += t;
+        }
+        return v;
+    }
+    __device__ __forceinline__ uint32_t scan_minu(uint32_t v) const {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane - o >= hl) v = min(v, t);
+        }
+        return v;
+    }
+    __device__ __forceinline__ uint32_t scan_maxu(uint32_t v) const {
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane - o >= hl) v = max(v, t);
         }
         return v;
     }
@@ -188,11 +207,25 @@ stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
         const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
         const float v = vb[k];
         const Seg s = make_seg(l);
-        const double dv = (double)v;
-        const double ssum = s.scan_add(dv);
-        const double ssx = s.scan_add(dv * (double)x);
-        const float smin = s.scan_min(l ? v : INFINITY);
-        const float smax = s.scan_max(l ? v : -INFINITY);
+        double ssum, ssx;
+        float smin, smax;
+        if constexpr (sizeof(TI) <= 2) {
+            // 8/16-bit intensities: exact uint32 scans of v and v * lane
+            // (at most 32 * 65535 * 31 < 2^32), x = 32 c + lane
+            const uint32_t iv = (uint32_t)v;
+            const uint32_t su = s.scan_addu(iv);
+            const uint32_t sl = s.scan_addu(iv * (uint32_t)lane);
+            ssum = (double)su;
+            ssx = (double)su * (double)(c * 32u) + (double)sl;
+            smin = (float)s.scan_minu(iv);
+            smax = (float)s.scan_maxu(iv);
+        } else {
+            const double dv = (double)v;
+            ssum = s.scan_add(dv);
+            ssx = s.scan_add(dv * (double)x);
+            smin = s.scan_min(l ? v : INFINITY);
+            smax = s.scan_max(l ? v : -INFINITY);
+        }
         if (s.tail && l) {
             const uint32_t i = l - 1;
             const uint32_t cnt = (uint32_t)(s.lane - s.hl + 1);
@@ -260,9 +293,8 @@ __global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T) {
         put(C_SUM_X, sx); put(C_CEN_X, cx);
         put(C_SUM_Y, sy); put(C_CEN_Y, cy);
         put(C_SUM_Z, sz); put(C_CEN_Z, cz);
-        b.cx[i] = cx; b.cy[i] = cy; b.cz[i] = cz;
-        b.mx[i] = mxc; b.my[i] = myc; b.mz[i] = mzc;
-        b.mean[i] = mean; b.area[i] = area;
+        b.pc[i] = make_float4(cx, cy, cz, mean);
+        b.pm[i] = make_float4(mxc, myc, mzc, area);
     }
 }
 
@@ -304,30 +336,35 @@ stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
         const uint32_t c = t - row * chunks;
         const int64_t x = (int64_t)c * 32 + lane;
         const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
-        double dc = 0.0, dm = 0.0, sq = 0.0;
+        // distances in float32 (relative error a few 1e-7), their sums and the
+        // squared deviations in float64; the squared deviations are divided
+        // by the area once per label
+        float dc = 0.0f, dm = 0.0f;
+        double sq = 0.0;
         if (l) {
             const uint32_t i = l - 1;
-            const double v = (double)vb[k];
-            const double ex = (double)x - b.cx[i], ey = (double)y - b.cy[i], ez = (double)z - b.cz[i];
-            const double fx = (double)x - b.mx[i], fy = (double)y - b.my[i], fz = (double)z - b.mz[i];
-            dc = sqrt(ex * ex + ey * ey + ez * ez);
-            dm = sqrt(fx * fx + fy * fy + fz * fz);
-            const double dv = v - (double)b.mean[i];
-            sq = dv * dv / (double)b.area[i];
+            const float4 pc = b.pc[i], pm = b.pm[i];
+            const float xf = (float)x, yf = (float)y, zf = (float)z;
+            const float ex = xf - pc.x, ey = yf - pc.y, ez = zf - pc.z;
+            const float fx = xf - pm.x, fy = yf - pm.y, fz = zf - pm.z;
+            dc = sqrtf(ex * ex + ey * ey + ez * ez);
+            dm = sqrtf(fx * fx + fy * fy + fz * fz);
+            const double dv = (double)vb[k] - (double)pc.w;
+            sq = dv * dv;
         }
         const Seg s = make_seg(l);
-        const double sdc = s.scan_add(dc);
-        const double sdm = s.scan_add(dm);
+        const double sdc = s.scan_add((double)dc);
+        const double sdm = s.scan_add((double)dm);
         const double ssq = s.scan_add(sq);
-        const double mdc = s.scan_maxd(dc);
-        const double mdm = s.scan_maxd(dm);
+        const float mdc = s.scan_max(dc);
+        const float mdm = s.scan_max(dm);
         if (s.tail && l) {
             const uint32_t i = l - 1;
             atomicAdd(b.sdc + i, sdc);
             atomicAdd(b.sdm + i, sdm);
             atomicAdd(b.ssq + i, ssq);
-            atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong(mdc));
-            atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong(mdm));
+            atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong((double)mdc));
+            atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong((double)mdm));
         }
         }
     }
@@ -337,14 +374,15 @@ __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L;
          i += (int64_t)gridDim.x * blockDim.x) {
         auto put = [&](int c, float v) { T[(int64_t)c * L + i] = v; };
-        const float area = b.area[i];
+        const float area = b.pm[i].w;
         const float sdc = (float)b.sdc[i], sdm = (float)b.sdm[i];
         const float mdc = __fdiv_rn(sdc, area), mdm = __fdiv_rn(sdm, area);
         const float xdc = (float)__longlong_as_double((long long)b.mdc[i]);
         const float xdm = (float)__longlong_as_double((long long)b.mdm[i]);
         put(C_SUM_DC, sdc); put(C_MEAN_DC, mdc);
         put(C_SUM_DM, sdm); put(C_MEAN_DM, mdm);
-        put(C_STD_I, (float)sqrt(b.ssq[i]));
+        // sum of squared deviations / area (0 for a label absent from the image)
+        put(C_STD_I, (float)sqrt(area > 0.0f ? b.ssq[i] / (double)area : b.ssq[i]));
         put(C_MAX_DC, xdc); put(C_MAX_DM, xdm);
         put(C_RATIO_C, __fdiv_rn(xdc, mdc));
         put(C_RATIO_M, __fdiv_rn(xdm, mdm));
