@@ -87,12 +87,12 @@ ALGO_BYTES = {"blur_spot": 2 + 4, "detect_maxima": 4 + 1, "blur_outline": 2 + 4,
 # one ncu --set full capture per kernel on the nuclei workload; the captures
 # are summarised in profiles/<kernel>_nuclei_128x512x512.md.
 MEASURED_TRAFFIC = {
-    "nuclei": {"voronoi_growth": (621.757e6 + 178.202e6, "voronoi_bricks_kernel_nuclei_128x512x512.md"),
-               "blur_spot": (67.244e6 + 82.811e6, "blur_fused_kernel_nuclei_128x512x512.md"),
-               "blur_outline": (67.167e6 + 83.039e6, "blur_fused_kernel_nuclei_128x512x512.md"),
+    "nuclei": {"voronoi_growth": (360.142e6 + 89.806e6, "voronoi_bricks_kernel_nuclei_128x512x512.md"),
+               "blur_spot": (67.164e6 + 81.208e6, "blur_fused_kernel_nuclei_128x512x512.md"),
+               "blur_outline": (67.155e6 + 81.081e6, "blur_fused_kernel_nuclei_128x512x512.md"),
                "detect_maxima": (135.090e6 + 19.932e6, "maxima_kernel_nuclei_128x512x512.md"),
-               "stats_pass1": (165.310e6 + 3.502e6, "stats_pass1_nuclei_128x512x512.md"),
-               "stats_pass2": (165.218e6 + 3.827e6, "stats_pass2_nuclei_128x512x512.md")},
+               "stats_pass1": (165.217e6 + 3.589e6, "stats_pass1_nuclei_128x512x512.md"),
+               "stats_pass2": (165.196e6 + 4.073e6, "stats_pass2_nuclei_128x512x512.md")},
 }
 
 # Algorithmic bytes per voxel of a whole gauss_otsu_labeling + statistics step
