@@ -164,55 +164,54 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
 // integers, so while the running sum stays below 2^24 every float32 addition
 // is exact and the result is the exact integer total.  Bins whose total
 // reaches 2^24 (at most voxels / 2^24 of them) are summed in row order by one
-// warp each; the others take their exact total.
+// warp each; the others take their exact total.  A CTA owns 32 bins: warp w
+// adds rows w, w + 32, ... of its lane's bin with 8 loads in flight, so the
+// totals take a few memory round trips instead of one per row.
+constexpr int kRowsumBins = 32;
 __global__ void __launch_bounds__(1024)
 hist_rowsum_kernel(const uint32_t *__restrict__ part, int64_t H, int bins,
                    float *__restrict__ hist) {
-    extern __shared__ unsigned long long tot[];   // bins x 4 partial totals
-    const int groups = blockDim.x / 256 > 0 ? (int)blockDim.x / 256 : 1;
-    for (int b0 = 0; b0 < bins; b0 += 256) {
-        // exact totals: 256 bins x `groups` row groups
-        const int b = b0 + (threadIdx.x & 255);
-        const int gidx = threadIdx.x >> 8;
-        unsigned long long acc = 0;
-        if (b < bins && gidx < groups)
-            for (int64_t y = gidx; y < H; y += groups) acc += part[y * bins + b];
-        __syncthreads();
-        if (gidx < groups) tot[(threadIdx.x & 255) * 4 + gidx] = acc;
-        __syncthreads();
-        if (threadIdx.x < 256 && b0 + (int)threadIdx.x < bins) {
-            unsigned long long t = 0;
-            for (int k = 0; k < groups; ++k) t += tot[threadIdx.x * 4 + k];
-            tot[threadIdx.x * 4] = t;
-            if (t < (1ull << 24)) hist[b0 + threadIdx.x] = (float)t;
-        }
-        __syncthreads();
-        // ordered float32 sums for the bins at or above 2^24
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        int seen = 0;
-        for (int j = 0; j < 256 && b0 + j < bins; ++j) {
-            if (tot[j * 4] < (1ull << 24)) continue;
-            if ((seen++ % nw) != warp) continue;
-            const int bb = b0 + j;
-            float acc32 = 0.0f;
-            for (int64_t y0 = 0; y0 < H; y0 += 128) {
-                uint32_t v[4];
+    __shared__ unsigned long long s_tot[32][kRowsumBins + 1];
+    __shared__ unsigned long long s_bin[kRowsumBins];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b = blockIdx.x * kRowsumBins + lane;
+    unsigned long long acc = 0;
+    if (b < bins) {
+        int64_t y = warp;
+        for (; y + 7 * 32 < H; y += 8 * 32) {
+            uint32_t v[8];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int64_t y = y0 + q * 32 + lane;
-                    v[q] = (y < H) ? part[y * bins + bb] : 0u;
-                }
+            for (int q = 0; q < 8; ++q) v[q] = part[(y + q * 32) * bins + b];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    for (int k = 0; k < 32; ++k) {
-                        const uint32_t x = __shfl_sync(0xffffffffu, v[q], k);
-                        if (y0 + q * 32 + k < H) acc32 = __fadd_rn(acc32, (float)x);
-                    }
-            }
-            if (lane == 0) hist[bb] = acc32;
+            for (int q = 0; q < 8; ++q) acc += v[q];
         }
-        __syncthreads();
+        for (; y < H; y += 32) acc += part[y * bins + b];
     }
+    s_tot[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < 32; ++w) t += s_tot[w][lane];
+        s_bin[lane] = t;
+        if (b < bins && t < (1ull << 24)) hist[b] = (float)t;
+    }
+    __syncthreads();
+    // ordered float32 sums: warp j takes bin j of the CTA when its total is
+    // at or above 2^24
+    const int bb = blockIdx.x * kRowsumBins + warp;
+    if (bb >= bins || s_bin[warp] < (1ull << 24)) return;
+    float acc32 = 0.0f;
+    for (int64_t y0 = 0; y0 < H; y0 += 32) {
+        const int64_t y = y0 + lane;
+        const uint32_t v = (y < H) ? part[y * bins + bb] : 0u;
+        const int n = (H - y0 < 32) ? (int)(H - y0) : 32;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            const uint32_t x = __shfl_sync(0xffffffffu, v, k);
+            if (k < n) acc32 = __fadd_rn(acc32, (float)x);
+        }
+    }
+    if (lane == 0) hist[bb] = acc32;
 }
 
 // A7: scikit-image Otsu on the histogram, float64, no contraction, numpy's
@@ -401,7 +400,7 @@ int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Are
         default: set_error("histogram: unsupported dtype %d", im.dtype); return CLE_ERR_DTYPE;
     }
     CLE_LAUNCH_CHECK("histogram rows");
-    hist_rowsum_kernel<<<1, 1024, sizeof(unsigned long long) * 256 * 4, st>>>(part, im.H, bins, d_hist);
+    hist_rowsum_kernel<<<(bins + kRowsumBins - 1) / kRowsumBins, 1024, 0, st>>>(part, im.H, bins, d_hist);
     CLE_LAUNCH_CHECK("histogram rowsum");
     return CLE_OK;
 }
