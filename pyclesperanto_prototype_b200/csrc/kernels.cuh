@@ -23,10 +23,6 @@ size_t blur_minmax_workspace_bytes(const Img &src);
 int blur_minmax(const Img &src, float *dst, double sigma, float *d_minmax, Arena &ws, cudaStream_t st);
 
 // reduce.cu
-struct MinMaxScratch {
-    float *partial;   // 2 * blocks
-    int blocks;
-};
 size_t minmax_workspace_bytes(const Img &im);
 // Writes {min, max} to d_out (device) without host synchronisation.
 int minmax(const Img &im, float *d_out, Arena &ws, cudaStream_t st);
