@@ -177,6 +177,15 @@ int cle_add_image_and_scalar(const cle_tensor *src, const cle_tensor *dst, float
 int cle_replace_intensities(const cle_tensor *src, const cle_tensor *map, const cle_tensor *dst,
                             void *stream);
 
+/* ---- euclidean_distance_from_label_centroid_map ---------------------------
+ * replaces _tier9/_euclidean_distance_from_label_centroid_map.py: every
+ * labelled voxel gets its float32 distance to its label's point in
+ * `centroids` (a float32 [d, n] point list, one row per dimension x, y(, z),
+ * column = label, as centroids_of_background_and_labels makes it); background
+ * voxels get 0.  Any label / destination dtype of the path. */
+int cle_euclidean_distance_from_label_centroid_map(const cle_tensor *labels, const cle_tensor *centroids,
+                                                   const cle_tensor *dst, void *stream);
+
 /* ---- minimum_box / maximum_box / top_hat_box ----------------------------
  * minimum_box replaces _tier1/_minimum_box.py:6-55, maximum_box
  * _tier1/_maximum_box.py, top_hat_box _tier2/_top_hat_box.py:6-43 (source minus

@@ -345,3 +345,27 @@ def statistics_of_labelled_pixels(intensity, labels) -> dict:
     for i, k in enumerate(STAT_KEYS):
         out[k] = table[i].copy()
     return out
+
+
+def euclidean_distance_from_label_centroid_map(labels) -> np.ndarray:
+    """Each labelled pixel's distance to its label's centroid, background 0
+    (_tier9/_euclidean_distance_from_label_centroid_map.py with the centroids
+    of _tier9/_centroids_of_labels.py: coordinate sums / pixel count, float32).
+    Distances in float64, returned as float32."""
+    lab = np.asarray(labels)
+    if lab.dtype.kind == "f":
+        lab = lab.astype(np.int64)
+    lab = np.clip(lab, 0, None).astype(np.int64)
+    st = statistics_of_labelled_pixels(np.zeros(lab.shape, np.float32), lab)
+    L = len(st["label"])
+    out = np.zeros(lab.shape, np.float64)
+    if L == 0:
+        return out.astype(np.float32)
+    keys = ("centroid_x", "centroid_y", "centroid_z")[:lab.ndim if lab.ndim == 3 else 2]
+    cen = [np.concatenate([[0.0], st[k].astype(np.float64)]) for k in keys]
+    coords = np.indices(lab.shape)[::-1]          # x, y(, z) grids
+    d2 = np.zeros(lab.shape, np.float64)
+    for c, grid in zip(cen, coords):
+        d2 += (grid - c[lab]) ** 2
+    out = np.where(lab > 0, np.sqrt(d2), 0.0)
+    return out.astype(np.float32)

@@ -13,7 +13,9 @@ the library or a CUDA device the ops raise; there is no CPU fallback.
 from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, create_binary_like,
                      create_labels_like, create_like, create_none, create_zyx, is_image, nparray,
                      plugin_function, pull, pull_zyx, push, push_native, push_zyx)
-from ._ops import (STATISTICS_ENTRY, add_image_and_scalar, label_maximum_extension_map,
+from ._ops import (STATISTICS_ENTRY, add_image_and_scalar, centroids_of_background_and_labels,
+                   centroids_of_labels, euclidean_distance_from_label_centroid_map,
+                   label_maximum_extension_map,
                    label_maximum_extension_ratio_map, label_maximum_intensity_map,
                    label_mean_extension_map, label_mean_intensity_map, label_minimum_intensity_map,
                    label_pixel_count_map, label_standard_deviation_intensity_map, push_regionprops,

@@ -78,6 +78,7 @@ _SIGS = {
     "cle_erode_box": (ctypes.c_int, [_T, _T, _P]),
     "cle_add_image_and_scalar": (ctypes.c_int, [_T, _T, ctypes.c_float, _P]),
     "cle_replace_intensities": (ctypes.c_int, [_T, _T, _T, _P]),
+    "cle_euclidean_distance_from_label_centroid_map": (ctypes.c_int, [_T, _T, _T, _P]),
     "cle_box_filter_workspace_bytes": (_SZ, [_T]),
     "cle_minimum_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
     "cle_maximum_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),

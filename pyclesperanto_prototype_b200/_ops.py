@@ -470,6 +470,53 @@ def label_maximum_extension_ratio_map(labels: Image, destination: Image = None) 
     return _label_map(None, labels, "mean_max_distance_to_centroid_ratio", destination)
 
 
+@plugin_function(output_creator=create_none, categories=['bia-bob-suggestion'])
+def centroids_of_labels(labels: Image, pointlist_destination: Image = None,
+                        include_background: bool = False) -> Image:
+    """Centroids of the labels as a float32 [d, n] point list: row 0 x, row 1 y
+    (row 2 z in 3D), column = label (from label 0 with include_background,
+    else from label 1); labels absent from the image get NaN
+    (_tier9/_centroids_of_labels.py).  The coordinate sums are the statistics'
+    exact integer sums, divided by the voxel count in float32."""
+    from ._tier0 import push as _push
+    labels = _push(labels)
+    temp = add_image_and_scalar(labels, scalar=1)
+    n = _label_max(temp)                                # labels 0 .. n-1
+    table = statistics_table(temp, temp, n)             # column j = original label j
+    dims = 3 if len(labels.shape) == 3 else 2
+    rows = [table[STAT_KEYS.index(k)] for k in ("centroid_x", "centroid_y", "centroid_z")[:dims]]
+    pts = torch.stack(rows)
+    if not include_background:
+        pts = pts[:, 1:]
+    pts = pts.contiguous()
+    if pointlist_destination is None:
+        return B200Array(pts)
+    pointlist_destination.tensor[:, :pts.shape[1]].copy_(pts)
+    return pointlist_destination
+
+
+@plugin_function(output_creator=create_none)
+def centroids_of_background_and_labels(source: Image, pointlist_destination: Image = None) -> Image:
+    """centroids_of_labels with the background as column 0
+    (_tier9/_centroids_of_background_and_labels.py)."""
+    return centroids_of_labels(source, pointlist_destination, True)
+
+
+@plugin_function(output_creator=create_none)
+def euclidean_distance_from_label_centroid_map(labels: Image, centroids_pointlist: Image = None,
+                                               distance_map_destination: Image = None) -> Image:
+    """Every labelled voxel replaced by its distance to its label's centroid,
+    background 0 (_tier9/_euclidean_distance_from_label_centroid_map.py); the
+    centroids come from centroids_of_background_and_labels unless given."""
+    if centroids_pointlist is None:
+        centroids_pointlist = centroids_of_background_and_labels(labels)
+    if distance_map_destination is None:
+        distance_map_destination = create_like(labels)
+    _call("cle_euclidean_distance_from_label_centroid_map", _lib.ref(_T(labels)),
+          _lib.ref(_T(centroids_pointlist)), _lib.ref(_T(distance_map_destination)), _lib.stream_ptr())
+    return distance_map_destination
+
+
 def _box_call(name, source, destination, rx, ry, rz):
     s, d = _T(source), _T(destination)
     ws = _ws("cle_box_filter_workspace_bytes", _lib.ref(s))

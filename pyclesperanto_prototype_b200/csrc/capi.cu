@@ -196,6 +196,16 @@ int cle_replace_intensities(const cle_tensor *src, const cle_tensor *map, const 
     return replace_intensities(a, m, d, S(stream));
 }
 
+int cle_euclidean_distance_from_label_centroid_map(const cle_tensor *labels, const cle_tensor *centroids,
+                                                   const cle_tensor *dst, void *stream) {
+    Img a, p, d;
+    CLE_TRY(to_img(labels, a, "labels"));
+    CLE_TRY(to_img(centroids, p, "centroids_pointlist"));
+    CLE_TRY(to_img(dst, d, "distance_map_destination"));
+    CLE_TRY(set_device_of(a, labels));
+    return centroid_distance_map(a, p, d, S(stream));
+}
+
 size_t cle_box_filter_workspace_bytes(const cle_tensor *src) {
     Img im;
     if (to_img(src, im, "source")) return 0;

@@ -45,6 +45,7 @@ int erode_box(const Img &src, const Img &dst, cudaStream_t st);
 // maps.cu
 int add_image_and_scalar(const Img &src, const Img &dst, float c, cudaStream_t st);
 int replace_intensities(const Img &src, const Img &map, const Img &dst, cudaStream_t st);
+int centroid_distance_map(const Img &labels, const Img &pts, const Img &dst, cudaStream_t st);
 
 size_t box_filter_workspace_bytes(const Img &im);
 int box_filter(const Img &src, const Img &dst, double rx, double ry, double rz, bool is_max, Arena &ws,

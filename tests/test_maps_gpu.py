@@ -124,3 +124,40 @@ def test_label_maps_match_oracle(cle, oracle, shape, name, key, with_intensity):
     got = cle.pull(fn(inten, lab) if with_intensity else fn(lab))
     ref = _oracle_map(oracle, inten if with_intensity else None, lab, key)
     assert _close(got, ref, RTOL)
+
+
+# ---- euclidean_distance_from_label_centroid_map ---------------------------
+def test_euclidean_distance_from_label_centroid_map_reference_test(cle):
+    # tests/test_euclidean_distance_from_label_centroid_map.py:4-34
+    labels = np.asarray([[1, 1, 1, 2], [1, 1, 1, 2], [1, 1, 1, 2], [2, 2, 2, 2]])
+    ref = np.asarray([[1.4142135, 1, 1.4142135, 2.3079278], [1, 0, 1, 1.4285713],
+                      [1.4142135, 1, 1.4142135, 0.86896616], [2.3079278, 1.4285713, 0.86896616, 1.2121831]])
+    got = cle.pull(cle.euclidean_distance_from_label_centroid_map(cle.push(labels)))
+    assert np.allclose(got, ref, 0.001)
+
+
+@pytest.mark.parametrize("shape", [(40, 70), (6, 33, 50), (1, 5, 7), (130, 97), (1, 1)])
+def test_euclidean_distance_from_label_centroid_map_matches_oracle(cle, oracle, shape):
+    rng = np.random.default_rng(3)
+    lab = rng.integers(0, 9, shape).astype(np.uint32)
+    lab[lab == 4] = 0                   # a gap: label 4 absent
+    got = cle.pull(cle.euclidean_distance_from_label_centroid_map(lab))
+    ref = oracle.euclidean_distance_from_label_centroid_map(lab)
+    assert got.dtype == np.float32 and got.shape == ref.shape
+    assert np.allclose(got, ref, rtol=RTOL, atol=1e-6)
+    assert np.all(got[lab == 0] == 0)
+
+
+def test_centroids_of_labels_point_lists(cle, oracle):
+    rng = np.random.default_rng(4)
+    lab = rng.integers(0, 6, (5, 20, 30)).astype(np.uint32)
+    lab[lab == 2] = 0
+    st = oracle.statistics_of_labelled_pixels(np.zeros(lab.shape, np.float32), lab)
+    ref = np.stack([st["centroid_x"], st["centroid_y"], st["centroid_z"]])
+    with_bg = cle.pull(cle.centroids_of_background_and_labels(lab))
+    without = cle.pull(cle.centroids_of_labels(lab))
+    assert with_bg.shape == (3, 6) and without.shape == (3, 5)
+    assert _close(without, ref, RTOL)
+    assert _close(with_bg[:, 1:], ref, RTOL)
+    bg = np.argwhere(lab == 0)
+    assert np.allclose(with_bg[:, 0], bg[:, ::-1].mean(axis=0), rtol=RTOL)

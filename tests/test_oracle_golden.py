@@ -269,3 +269,16 @@ def test_top_hat_box_golden(oracle):
                   [0, 0, 0, 0, 0]], np.float32)
     r = oracle.top_hat_box(t, 1, 1, 0)
     assert r.min() == 0 and r.max() == 50
+
+
+# ---- euclidean_distance_from_label_centroid_map ---------------------------
+CENTROID_DIST_LABELS = np.asarray([[1, 1, 1, 2], [1, 1, 1, 2], [1, 1, 1, 2], [2, 2, 2, 2]])
+CENTROID_DIST_REF = np.asarray([[1.4142135, 1, 1.4142135, 2.3079278], [1, 0, 1, 1.4285713],
+                                [1.4142135, 1, 1.4142135, 0.86896616],
+                                [2.3079278, 1.4285713, 0.86896616, 1.2121831]])
+
+
+def test_euclidean_distance_from_label_centroid_map_golden(oracle):
+    # tests/test_euclidean_distance_from_label_centroid_map.py:4-34 (rtol 1e-3)
+    got = oracle.euclidean_distance_from_label_centroid_map(CENTROID_DIST_LABELS)
+    assert np.allclose(got, CENTROID_DIST_REF, 0.001)
