@@ -587,9 +587,9 @@ def _spheres(n, size, radius, seed):
 
 
 def run_published(args):
-    """Times the cases the reference's notebooks publish
-    on seeded inputs of the same shape and distribution, inputs resident on the
-    device: CUDA-event time per call and wall time with a synchronize."""
+    """Times the cases the reference's notebooks publish timings for, on seeded
+    inputs of the same shape and distribution, inputs resident on the device:
+    CUDA-event time per call and wall time with a synchronize."""
     import torch
     import pyclesperanto_prototype_b200 as cle
     torch.cuda.set_device(0)
