@@ -1,29 +1,42 @@
 """Benchmark: Mvoxels/s of voronoi_otsu_labeling + statistics_of_labelled_pixels.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload nuclei|lightsheet|blobs2d]
+                    [--workload lightsheet|nuclei|lightsheet_dense|blobs2d|batch|served|published]
 
-Default workload (N=1): the 3D nuclei volume, uint16 128x512x512 (2000
-ellipsoids, PSF, Poisson noise, seed 1); one step = voronoi_otsu_labeling
-(spot_sigma=2, outline_sigma=1) followed by statistics_of_labelled_pixels on
+Default workload (N=1): the light-sheet volume, uint16 512x1024x1024 (30000
+ellipsoidal cells, slow sinusoidal background, Poisson noise, seed 2), the
+largest single-GPU configuration; one step = voronoi_otsu_labeling
+(spot_sigma=2, outline_sigma=2) followed by statistics_of_labelled_pixels on
 the same intensity volume.  Data are synthetic (seeded generator with the
 workload's shapes and value distributions).
 
   value   device-resident throughput: the input already in HBM, every step's
-          device time measured with CUDA events on the launching stream, L2
-          flushed (256 MiB write) between steps.
-  e2e     the same step through the public API with host buffers: pinned
-          host -> device copy of the uint16 volume, the two ops, the label
-          image and the statistics table copied back to pinned host memory.
+          device time measured with CUDA events on the launching stream; the
+          1 GiB input and 2 GiB of labels exceed the 126 MB L2.
+  e2e     the same step end to end through the public serving API
+          (SegmentationServer): every step uploads the uint16 volume from
+          pinned host memory and returns its label image (into a pinned host
+          buffer) and its statistics table; steps overlap (upload, compute and
+          download on their own streams), the time runs from the first upload
+          to the last result on the host.  e2e_per_call is the same with one
+          synchronous call after another (push, the two ops, pull).
   roofline   the dominant kernel stage, timed live with the library's stage
           events inside the timed steps; achieved = algorithmic bytes / time.
+  pipeline_roofline   the whole step against 36 B/voxel (read the source and
+          write the blur, read the blur for the histogram, read source + blur
+          and write mask and seeds, read them and write uint32 labels, two
+          statistics reads of labels + intensity).
+  served_vs_per_call   the serving form against the plain per-call loop on a
+          Poisson trace of mixed request sizes (p50/p95/p99 latency,
+          Mvoxels/s), and both at saturation (all requests waiting at once).
   cpu_baseline   the CPU oracle (C/OpenMP restatement of the reference's
-          algorithm, all host threads) on the same workload.
+          algorithm, all host threads) on a bounded sample of the same workload.
 
---impl reference times the reference's algorithm on the host cores: the
-reference itself cannot run here (pyopencl, a CPU OpenCL runtime and its
-clij-opencl-kernels sources are absent), so its C restatement (oracle/) runs
-instead, with every host thread.
+--impl reference times the reference's algorithm on the host cores on the
+same workload (the whole volume every step): the reference itself cannot run
+here (pyopencl, a CPU OpenCL runtime and its clij-opencl-kernels sources are
+absent), so its C restatement (oracle/) runs instead, with every host thread.
+Both arms print the same `config`.
 
 Multi-GPU: replicas (one process per GPU, each runs the full workload; no
 collective on the data path; timing = max over ranks).
@@ -45,6 +58,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mvoxels/s voronoi_otsu_labeling; p50/p99 latency served vs per-call"
 UNIT = "Mvoxels/s"
+DEFAULT_WORKLOAD = "lightsheet"
 
 WORKLOADS = {
     "nuclei": dict(desc="nuclei volume uint16 128x512x512 (2000 ellipsoids, PSF (1.5,1,1), Poisson, seed 1): "
@@ -73,6 +87,12 @@ WORKLOADS = {
                     outline=1.0),
 }
 
+
+def config_of(name, nvox):
+    """The `config` object both arms print for a workload (identical keys)."""
+    return {"workload": WORKLOADS[name]["desc"], "voxels_per_step": int(nvox)}
+
+
 # Algorithmic bytes per voxel of each stage (each input read once, each
 # output written once; uint16 source).  Index = stage event interval.
 STAGES = ["blur_spot", "detect_maxima", "blur_outline", "minmax_hist_otsu", "threshold_seeds",
@@ -81,11 +101,16 @@ STAGES = ["blur_spot", "detect_maxima", "blur_outline", "minmax_hist_otsu", "thr
 ALGO_BYTES = {"blur_spot": 2 + 4, "detect_maxima": 4 + 1, "blur_outline": 2 + 4,
               "minmax_hist_otsu": 4 + 4, "threshold_seeds": 4 + 1 + 1 + 4,
               "voronoi_growth": 1 + 1 + 4, "stats_pass1": 4 + 2, "stats_pass2": 4 + 2}
+# The pipeline's compulsory traffic per voxel (the minimal pass structure the
+# two global reductions force): read src + write blur 8, read blur for the
+# histogram 4, read src + blur and write mask + seeds 10, read mask + seeds
+# and write uint32 labels 6, statistics 2 x (labels 4 + intensity 4).
+PIPELINE_BYTES_PER_VOXEL = 8 + 4 + 10 + 6 + 8
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# one ncu --set full capture per kernel on the nuclei workload; the captures
-# are summarised in profiles/<kernel>_nuclei_128x512x512.md.
+# one ncu --set full capture per kernel; the captures are summarised in
+# profiles/<kernel>_<workload>.md.
 MEASURED_TRAFFIC = {
     "nuclei": {"voronoi_growth": (360.142e6 + 89.806e6, "voronoi_bricks_kernel_nuclei_128x512x512.md"),
                "blur_spot": (67.164e6 + 81.208e6, "blur_fused_kernel_nuclei_128x512x512.md"),
@@ -121,6 +146,9 @@ def load_peaks():
 
 
 def make_input(name, device=None):
+    """The workload's input volume: numpy (nuclei, blobs2d) or a torch uint16
+    tensor (light-sheet: generated with torch on the GPU when one is visible,
+    so both arms of the benchmark see the same volume)."""
     from pyclesperanto_prototype_b200 import synthetic
     w = WORKLOADS[name]
     if name == "nuclei":
@@ -134,57 +162,108 @@ def make_input(name, device=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons of one GPU, sampled every
+    `period` seconds through NVML (the fields nvidia-smi reports as
+    clocks.sm, clocks.max.sm and clocks_event_reasons.*) from start() to
+    stop(); nvidia-smi at 200 ms when NVML is not available."""
 
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
     FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
               "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
               "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
 
-    def __init__(self, device_index):
-        self.dev = device_index
+    def __init__(self, device_index, period=0.01):
+        self.dev = int(device_index)
+        self.period = float(period)
+        self.samples = []          # (t, sm_mhz, max_mhz, reasons bitmask)
+        self.windows = []
+        self._stop = threading.Event()
+        self.t = None
+        self.source = None
         self.proc = None
-        self.lines = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        try:
+            import pynvml
+            h = self._nvml_handle()
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.perf_counter(), float(sm), float(mx), int(rs)))
+                    except Exception:
+                        pass
+                    self._stop.wait(self.period)
+            self.t = threading.Thread(target=loop, daemon=True)
+            self.t.start()
+            self.source = "nvml every %d ms" % int(self.period * 1e3)
+        except Exception:
+            self._start_smi()
+
+    def _start_smi(self):
+        self.source = "nvidia-smi -lms 200"
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
                  "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                 text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+
+            def read():
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for line in self.proc.stdout:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < len(self.FIELDS):
+                        continue
+                    try:
+                        rs = 0
+                        for nm, v in zip(names, parts[5:9]):
+                            if v.lower() == "active":
+                                rs |= self.REASONS[nm]
+                        self.samples.append((time.perf_counter(), float(parts[1]), float(parts[2]), rs))
+                    except ValueError:
+                        continue
+            self.t = threading.Thread(target=read, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark(self, t0, t1):
+        """Records a timed window [t0, t1] (perf_counter seconds)."""
+        self.windows.append((t0, t1))
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.t.join(timeout=2)
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < len(self.FIELDS):
-                continue
+        self._stop.set()
+        if self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=2)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"],
+                    "samples": 0}
+        inside = [s for s in self.samples if any(a <= s[0] <= b for a, b in self.windows)]
+        use = inside if len(inside) >= 5 else self.samples
+        reasons = sorted(nm for nm, bit in self.REASONS.items() if any(s[3] & bit for s in use))
+        return {"sm_mhz": float(np.median([s[1] for s in use])), "sm_max_mhz": max(s[2] for s in use),
+                "reasons": reasons, "samples": len(use), "samples_in_timed_region": len(inside),
+                "source": self.source}
 
 
 def dist_setup(n_gpus):
@@ -242,6 +321,153 @@ def cpu_baseline_sample(vol, w, reps=2, max_voxels=48 * 1024 * 1024):
     return f.size / t / 1e6, cores, f.shape, t
 
 
+def e2e_served(pinned_in, w, steps, world, ref_labels=None, slots=3):
+    """Throughput through the public serving API: `steps` requests of the
+    workload's volume, all waiting at t=0; each uploads the pinned uint16
+    volume and returns its label image into a pinned host buffer plus its
+    statistics table.  Returns the e2e dict (max over ranks)."""
+    import torch
+    from pyclesperanto_prototype_b200.serving import Request, SegmentationServer
+    server = SegmentationServer(budget_bytes=60e9, slots=slots, spot_sigma=w["spot"],
+                                outline_sigma=w["outline"])
+    outs = [torch.empty(tuple(pinned_in.shape), dtype=torch.uint32).pin_memory() for _ in range(slots)]
+    server.run([Request(-1, pinned_in, 0.0, labels_out=outs[0])], realtime=False)   # warm-up
+    torch.cuda.synchronize()
+    reqs = [Request(i, pinned_in, 0.0, labels_out=outs[i % slots]) for i in range(steps)]
+    barrier(world)
+    t0 = time.perf_counter()
+    server.run(reqs, realtime=False)
+    t = max_over_ranks(time.perf_counter() - t0, world)
+    bad = [r.error for r in reqs if not r.ok]
+    if bad:
+        raise RuntimeError("e2e request failed: " + bad[0])
+    nvox = pinned_in.numel()
+    L = reqs[-1].num_labels
+    out = {"value": round(nvox * world * steps / t / 1e6, 2), "unit": UNIT,
+           "h2d_bytes_per_step": int(pinned_in.numel() * pinned_in.element_size()),
+           "d2h_bytes_per_step": int(nvox * 4 + 35 * L * 4 + 8), "ms_per_step": round(t / steps * 1e3, 3),
+           "steps": steps, "api": "pyclesperanto_prototype_b200.serving.SegmentationServer, %d slots: "
+                                  "upload / compute / download of consecutive steps overlap" % slots}
+    if ref_labels is not None:
+        out["labels_equal_device_run"] = bool(torch.equal(outs[(steps - 1) % slots], ref_labels))
+    del server, outs
+    torch.cuda.empty_cache()
+    return out
+
+
+def e2e_per_call(pinned_in, w, reps, world, flush):
+    """One synchronous public-API call after another: push, the two ops,
+    labels to pinned host memory, statistics dict."""
+    import torch
+    import pyclesperanto_prototype_b200 as cle
+    dense = w.get("op") == "gauss_otsu"
+    pinned_lab = torch.empty(tuple(pinned_in.shape), dtype=torch.uint32).pin_memory()
+    ts = []
+    for i in range(reps + 1):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img = cle.push_native(pinned_in)
+        if dense:
+            lab = cle.gauss_otsu_labeling(img, outline_sigma=w["outline"])
+        else:
+            lab = cle.voronoi_otsu_labeling(img, spot_sigma=w["spot"], outline_sigma=w["outline"])
+        stats = cle.statistics_of_labelled_pixels(img, lab)
+        pinned_lab.copy_(lab.tensor, non_blocking=True)
+        torch.cuda.synchronize()
+        if i:
+            ts.append(time.perf_counter() - t0)
+        del img, lab
+    te = max_over_ranks(st.mean(ts), world)
+    nvox = pinned_in.numel()
+    return {"value": round(nvox * world / te / 1e6, 2), "unit": UNIT,
+            "h2d_bytes_per_step": int(pinned_in.numel() * pinned_in.element_size()),
+            "d2h_bytes_per_step": int(nvox * 4 + 35 * len(stats["label"]) * 4 + 8),
+            "ms_per_step": round(te * 1e3, 3), "steps": reps}
+
+
+SERVED_CLASSES = [(512, 512), (64, 256, 256), (128, 512, 512), (256, 1024, 1024)]
+SERVED_PROBS = [0.4, 0.3, 0.2, 0.1]
+
+
+def served_pools(pool_per_class):
+    """Pinned uint16 request volumes per size class (blob tiles, per-volume seeds)."""
+    import torch
+    from pyclesperanto_prototype_b200 import synthetic
+    dev = "cuda:%d" % torch.cuda.current_device()
+    return {c: [synthetic.blob_tile(c, 2e-4 if len(c) == 3 else 1e-3, seed=5000 + 10 * k + j, device=dev)
+                .clamp_(0, 65535).to(torch.int32).to(torch.uint16).cpu().pin_memory()
+                for j in range(pool_per_class)] for k, c in enumerate(SERVED_CLASSES)}
+
+
+def served_trace(rate, duration, pool_per_class, seed=5):
+    rng = np.random.default_rng(seed)
+    t, trace = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        c = SERVED_CLASSES[rng.choice(len(SERVED_CLASSES), p=SERVED_PROBS)]
+        trace.append((t, c, int(rng.integers(pool_per_class))))
+    return trace
+
+
+def _summarize(reqs, vox_of):
+    lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
+    span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
+    vox = sum(vox_of[r.rid] for r in reqs)
+    return {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p95_ms": round(float(np.percentile(lat, 95)), 3),
+            "p99_ms": round(float(np.percentile(lat, 99)), 3), "mvoxels_per_s": round(vox / span / 1e6, 2),
+            "requests": len(reqs), "span_s": round(span, 3)}
+
+
+def served_vs_per_call(rate, duration, lanes, pool_per_class=3, closed_requests=120, spot=2.0, outline=2.0,
+                       compute_streams=1, express_voxels=8 << 20):
+    """The served form against the per-call loop: (1) on a Poisson trace at
+    `rate` req/s for `duration` s, (2) at saturation (closed_requests
+    requests all waiting at t=0).  Single GPU."""
+    import torch
+    from pyclesperanto_prototype_b200.serving import Request, SegmentationServer, per_call_loop
+    pool = served_pools(pool_per_class)
+    trace = served_trace(rate, duration, pool_per_class)
+    rng = np.random.default_rng(55)
+    closed = [(0.0, SERVED_CLASSES[rng.choice(len(SERVED_CLASSES), p=SERVED_PROBS)],
+               int(rng.integers(pool_per_class))) for _ in range(closed_requests)]
+
+    def make(tr):
+        return [Request(i, pool[c][j], arrival=a) for i, (a, c, j) in enumerate(tr)]
+
+    server = SegmentationServer(budget_bytes=60e9, slots=lanes, compute_streams=compute_streams,
+                                express_voxels=express_voxels, spot_sigma=spot, outline_sigma=outline)
+    warm = [Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(SERVED_CLASSES)]
+    server.run(warm, realtime=False)
+    per_call_loop([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(SERVED_CLASSES)], spot, outline,
+                  realtime=False)
+    torch.cuda.synchronize()
+    out = {}
+    for name, tr, realtime in (("trace", trace, True), ("saturation", closed, False)):
+        vox_of = {i: pool[c][j].numel() for i, (a, c, j) in enumerate(tr)}
+        served = server.run(make(tr), realtime=realtime)
+        plain = per_call_loop(make(tr), spot, outline, realtime=realtime)
+        s, p = _summarize(served, vox_of), _summarize(plain, vox_of)
+        same = all(a.num_labels == b.num_labels and np.array_equal(a.table, b.table)
+                   for a, b in zip(served, plain))
+        out[name] = {"served": s, "per_call": p, "results_equal": bool(same),
+                     "throughput_ratio": round(s["mvoxels_per_s"] / p["mvoxels_per_s"], 3)}
+    out["trace"]["desc"] = ("Poisson arrivals at %g req/s for %g s; request sizes {512x512, 64x256x256, "
+                            "128x512x512, 256x1024x1024} with p {0.4,0.3,0.2,0.1}; %d volumes per size class"
+                            % (rate, duration, pool_per_class))
+    out["saturation"]["desc"] = "%d requests of the same size mix, all waiting at t=0" % closed_requests
+    out["served_p99_below_per_call_p50"] = bool(out["trace"]["served"]["p99_ms"] <
+                                                out["trace"]["per_call"]["p50_ms"])
+    out["form"] = ("served: %d requests in flight, uploads and downloads on copy streams, %d compute "
+                   "stream(s), express lane for requests of <= %d voxels, 60 GB budget"
+                   % (lanes, compute_streams, express_voxels))
+    del server, pool
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_b200(args):
     import torch
     import pyclesperanto_prototype_b200 as cle
@@ -253,7 +479,7 @@ def run_b200(args):
     w = WORKLOADS[args.workload]
     host = make_input(args.workload, device=dev)
     if isinstance(host, torch.Tensor):
-        # generated on the device; a host copy feeds the end-to-end leg
+        # generated on the device; a host copy feeds the end-to-end legs
         src = cle.B200Array(host.contiguous())
         host_np = host.cpu().numpy()
     else:
@@ -261,6 +487,8 @@ def run_b200(args):
         src = cle.push_native(host_np)
     nvox = int(np.prod(src.shape))
     stream = torch.cuda.current_stream()
+    # between steps a 256 MiB write evicts the 126 MB L2 (the light-sheet
+    # inputs exceed it anyway)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     labels = cle.create_labels_like(src)
 
@@ -277,8 +505,6 @@ def run_b200(args):
     # correctness of the loop status once (not timed)
     if not dense:
         cle._ops._vol(src, labels, w["spot"], w["outline"], check=True)
-    # clocks are sampled from the start of the warm-up (under load) through
-    # the timed region; short runs add untimed steps until 3 samples exist
     clocks = ClockSampler(local)
     clocks.start()
     for _ in range(args.warmup):
@@ -289,6 +515,7 @@ def run_b200(args):
     barrier(world)
     n0 = lib.cle_kernel_launches()
     times, stage_ms = [], []
+    t_timed0 = time.perf_counter()
     for _ in range(args.steps):
         flush.fill_(1)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -299,48 +526,27 @@ def run_b200(args):
         times.append(e0.elapsed_time(e1))
         k = lib.cle_profile_stage_ms(stage_buf, 16)
         stage_ms.append([stage_buf[i] for i in range(k)])
+    clocks.mark(t_timed0, time.perf_counter())
     launches = lib.cle_kernel_launches() - n0
     trace = (ctypes.c_uint64 * (4 * 256))()
     lib.cle_profile_trace(trace, ctypes.sizeof(trace))
     vor_trace = [tuple(int(v) for v in trace[4 * i:4 * i + 4]) for i in range(256)
                  if trace[4 * i] or trace[4 * i + 1]]
     barrier(world)
-    t_pad = time.perf_counter()
-    while len(clocks.lines) < 3 and time.perf_counter() - t_pad < 3.0:
-        step()
-        torch.cuda.synchronize()
     clk = clocks.stop()
     lib.cle_profile_enable(0)
     total_ms = max_over_ranks(sum(times), world)
     ms_per_step = total_ms / args.steps
     value = nvox * world * args.steps / (total_ms / 1e3) / 1e6
+    labels_dev = labels.tensor.cpu() if not dense else None
 
     # end to end through the public API with pinned host buffers
-    e2e = None
-    if host_np is not None:
-        pinned_in = torch.from_numpy(host_np).pin_memory()
-        pinned_lab = torch.empty(src.shape, dtype=torch.uint32).pin_memory()
-        t_e2e = []
-        for i in range(max(2, args.steps // 2) + 1):
-            flush.fill_(1)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            img = cle.push_native(pinned_in)
-            if dense:
-                lab = cle.gauss_otsu_labeling(img, outline_sigma=w["outline"])
-            else:
-                lab = cle.voronoi_otsu_labeling(img, spot_sigma=w["spot"], outline_sigma=w["outline"])
-            stats = cle.statistics_of_labelled_pixels(img, lab)
-            pinned_lab.copy_(lab.tensor, non_blocking=True)
-            torch.cuda.synchronize()
-            if i:
-                t_e2e.append(time.perf_counter() - t0)
-        te = max_over_ranks(st.mean(t_e2e), world)
-        L_e2e = len(stats["label"])
-        e2e = {"value": nvox * world / te / 1e6, "unit": UNIT,
-               "h2d_bytes_per_step": int(host_np.nbytes),
-               "d2h_bytes_per_step": int(nvox * 4 + 35 * L_e2e * 4 + 8),
-               "ms_per_step": te * 1e3}
+    pinned_in = torch.from_numpy(host_np).pin_memory()
+    e2e = None if dense else e2e_served(pinned_in, w, args.steps, world, ref_labels=labels_dev)
+    e2e_serial = e2e_per_call(pinned_in, w, max(2, min(5, args.steps // 4)), world, flush)
+    if e2e is None:
+        e2e = e2e_serial
+    del labels_dev
 
     # roofline: the dominant kernel stage
     sm = np.array([s + [0.0] * (12 - len(s)) for s in stage_ms])[:, :12]
@@ -356,7 +562,7 @@ def run_b200(args):
     achieved = bpv * nvox / (t_dom / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes_per_voxel": bpv}
+                "traffic": None, "algorithmic_bytes_per_voxel": bpv, "ms": round(float(t_dom), 4)}
     tr = MEASURED_TRAFFIC.get(args.workload, {}).get(dom)
     if tr:
         roofline["traffic"] = tr[0]
@@ -364,14 +570,21 @@ def run_b200(args):
     stages = {STAGES[i]: round(float(mean_stage[i]), 4) for i in range(12) if STAGES[i]}
     stage_roofline = {name: round(ALGO_BYTES[name] * nvox / (stages[name] / 1e3) / 1e9 / peak, 4)
                       for name in ALGO_BYTES if stages.get(name)}
-    # the whole pipeline against the same peak: every stage's algorithmic
-    # bytes over the step time
-    bpv_pipe = DENSE_BYTES_PER_VOXEL if dense else sum(ALGO_BYTES.values())
+    # the whole pipeline against the same peak at the compulsory bytes per voxel
+    bpv_pipe = DENSE_BYTES_PER_VOXEL if dense else PIPELINE_BYTES_PER_VOXEL
     pipe_bytes = bpv_pipe * nvox
     pipeline_roofline = {"bytes_per_voxel": bpv_pipe,
                          "achieved": round(pipe_bytes / (ms_per_step / 1e3) / 1e9, 1),
                          "frac": round(pipe_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4)}
     lat = np.array(times)
+
+    served = None
+    if world == 1 and args.served_duration > 0 and not dense:
+        del src, labels, host
+        torch.cuda.empty_cache()
+        served = served_vs_per_call(args.rate, args.served_duration, args.lanes,
+                                    closed_requests=args.closed_requests,
+                                    compute_streams=args.compute_streams, express_voxels=args.express_voxels)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and host_np is not None:
@@ -384,14 +597,17 @@ def run_b200(args):
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                "data": "synthetic", "impl": "b200",
-               "config": {"workload": w["desc"], "voxels_per_step": nvox, "labels": int(L),
-                          "l2": "flushed between steps (256 MiB write)", "parallelism": "replicas",
-                          "input_dtype": str(src.dtype)},
+               "config": config_of(args.workload, nvox),
+               "run": {"labels": int(L), "input_dtype": str(host_np.dtype), "parallelism": "replicas",
+                       "l2": "inputs (1 GiB u16) and labels (2 GiB) exceed the 126 MB L2; a 256 MiB "
+                             "write between steps as well"},
                "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 4),
                               "p99": round(float(np.percentile(lat, 99)), 4)},
-               "stages_ms": stages, "stage_roofline_frac": stage_roofline, "voronoi_trace": vor_trace if args.trace else None, "e2e": e2e, "gpu_launches": int(launches),
-               "roofline": roofline, "pipeline_roofline": pipeline_roofline, "cpu_baseline": cpu,
-               "clocks": clk}
+               "stages_ms": stages, "stage_roofline_frac": stage_roofline,
+               "voronoi_trace": vor_trace if args.trace else None,
+               "e2e": e2e, "e2e_per_call": e2e_serial, "gpu_launches": int(launches),
+               "roofline": roofline, "pipeline_roofline": pipeline_roofline,
+               "served_vs_per_call": served, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -480,84 +696,62 @@ def run_batch(args):
 
 
 def run_served(args):
+    """The served form alone: the Poisson trace (default 200 req/s for 60 s)
+    and saturation, served against the per-call loop; under torchrun the
+    trace is routed over replicas."""
     import torch
-    from pyclesperanto_prototype_b200 import synthetic
     from pyclesperanto_prototype_b200.serving import Request, SegmentationServer, per_call_loop, request_bytes
     rank, world, local = dist_setup(args.gpus)
     w = WORKLOADS["served"]
-    classes = [(512, 512), (64, 256, 256), (128, 512, 512), (256, 1024, 1024)]
-    probs = [0.4, 0.3, 0.2, 0.1]
-    pool_per_class = 3
-    pool = {c: [synthetic.blob_tile(c, 2e-4 if len(c) == 3 else 1e-3, seed=5000 + 10 * k + j,
-                                    device="cuda:%d" % torch.cuda.current_device())
-                .clamp_(0, 65535).to(torch.int32).to(torch.uint16).cpu().pin_memory()
-                for j in range(pool_per_class)] for k, c in enumerate(classes)}
-    rng = np.random.default_rng(5)
-    t, trace = 0.0, []
-    while True:
-        t += rng.exponential(1.0 / args.rate)
-        if t >= args.duration:
-            break
-        c = classes[rng.choice(len(classes), p=probs)]
-        trace.append((t, c, int(rng.integers(pool_per_class))))
+    if world == 1:
+        res = served_vs_per_call(args.rate, args.duration, args.lanes, pool_per_class=args.pool,
+                                 closed_requests=args.closed_requests, spot=w["spot"], outline=w["outline"],
+                                 compute_streams=args.compute_streams, express_voxels=args.express_voxels)
+        s = res["trace"]["served"]
+        out = {"metric": METRIC, "value": s["mvoxels_per_s"], "unit": UNIT, "n_gpus": 1,
+               "steps": s["requests"], "warmup": len(SERVED_CLASSES), "ms_per_step": None,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic", "impl": "b200", "form": res["form"],
+               "config": {"workload": w["desc"], "rate_per_s": args.rate, "duration_s": args.duration,
+                          "volumes": "%d pre-generated per size class, reused" % args.pool},
+               "served_vs_per_call": res}
+        print(json.dumps(out), flush=True)
+        return
+    # replicas: every rank routes the same trace and serves its share
+    from pyclesperanto_prototype_b200.replicas import serve_replicated
+    pool = served_pools(args.pool)
+    trace = served_trace(args.rate, args.duration, args.pool)
+
     def make():
         return [Request(i, pool[c][j], arrival=a) for i, (a, c, j) in enumerate(trace)]
-    warm = [Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)]
     server = SegmentationServer(budget_bytes=60e9, slots=args.lanes, compute_streams=args.compute_streams,
                                 express_voxels=args.express_voxels, spot_sigma=w["spot"],
                                 outline_sigma=w["outline"])
-    server.run(warm, realtime=False)
-    per_call_loop([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(classes)], w["spot"],
-                  w["outline"], realtime=False)
-    torch.cuda.synchronize()
-    if world == 1:
-        served = server.run(make(), realtime=True)
-        plain = per_call_loop(make(), w["spot"], w["outline"], realtime=True)
-    else:
-        # replicas: every rank routes the same trace and serves its share
-        from pyclesperanto_prototype_b200.replicas import serve_replicated
+    server.run([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(SERVED_CLASSES)], realtime=False)
 
-        class _PerCall:
-            def run(self, reqs, realtime=True):
-                return per_call_loop(reqs, w["spot"], w["outline"], realtime=realtime)
+    class _PerCall:
+        def run(self, reqs, realtime=True):
+            return per_call_loop(reqs, w["spot"], w["outline"], realtime=realtime)
 
-        nbytes = lambda r: request_bytes(tuple(r.volume.shape), r.volume.dtype)
-        barrier(world)
-        served = serve_replicated(make(), lambda _: server, nbytes, 60e9)
-        barrier(world)
-        plain = serve_replicated(make(), lambda _: _PerCall(), nbytes, 60e9)
-        barrier(world)
-        import torch.distributed as dist
-        if rank != 0:
-            dist.destroy_process_group()
-            return
-    vox_of = {i: pool[c][j].numel() for i, (a, c, j) in enumerate(trace)}
-
-    def summarize(reqs):
-        lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
-        span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
-        vox = sum(vox_of[r.rid] for r in reqs)
-        return {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p95_ms": round(float(np.percentile(lat, 95)), 3),
-                "p99_ms": round(float(np.percentile(lat, 99)), 3), "mvoxels_per_s": round(vox / span / 1e6, 2),
-                "requests": len(reqs), "span_s": round(span, 3)}
-    s, p = summarize(served), summarize(plain)
-    same = all(a.num_labels == b.num_labels for a, b in zip(served, plain))
-    out = {"metric": METRIC, "value": s["mvoxels_per_s"], "unit": UNIT, "n_gpus": world, "steps": len(trace),
-           "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "b200",
-           "form": "served (continuous batching: %d requests in flight, uploads and downloads on copy "
-                   "streams overlapping %d compute stream(s) plus an express lane for requests of <= %d "
-                   "voxels, 60 GB budget)" % (args.lanes, args.compute_streams, args.express_voxels),
-           "config": {"workload": w["desc"], "rate_per_s": args.rate, "duration_s": args.duration,
-                      "volumes": "%d pre-generated per size class, reused" % pool_per_class},
-           "served": s, "per_call_loop": p, "label_counts_equal": bool(same),
-           "served_p99_below_per_call_p50": bool(s["p99_ms"] < p["p50_ms"])}
-    if world > 1:
-        out["form"] += "; %d replicas, requests routed by device memory (no data-path collective)" % world
-    print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    nbytes = lambda r: request_bytes(tuple(r.volume.shape), r.volume.dtype)
+    barrier(world)
+    served = serve_replicated(make(), lambda _: server, nbytes, 60e9)
+    barrier(world)
+    plain = serve_replicated(make(), lambda _: _PerCall(), nbytes, 60e9)
+    barrier(world)
+    import torch.distributed as dist
+    if rank == 0:
+        vox_of = {i: pool[c][j].numel() for i, (a, c, j) in enumerate(trace)}
+        s, p = _summarize(served, vox_of), _summarize(plain, vox_of)
+        out = {"metric": METRIC, "value": s["mvoxels_per_s"], "unit": UNIT, "n_gpus": world,
+               "steps": len(trace), "warmup": len(SERVED_CLASSES), "ms_per_step": None,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic", "impl": "b200",
+               "form": "served, %d replicas, requests routed by device memory (no data-path collective)" % world,
+               "config": {"workload": w["desc"], "rate_per_s": args.rate, "duration_s": args.duration},
+               "served": s, "per_call_loop": p}
+        print(json.dumps(out), flush=True)
+    dist.destroy_process_group()
 
 
 def _tissue_2d(width, height, dx, dy, seed):
@@ -660,6 +854,9 @@ def run_published(args):
 
 
 def run_reference(args):
+    """The reference arm: the oracle (the reference's algorithm restated in C,
+    OpenMP on every host thread) on the same workload and volume, the whole
+    volume every timed step; warm-up steps run on a slab of it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -668,25 +865,18 @@ def run_reference(args):
     w = WORKLOADS[args.workload]
     if args.workload in ("batch", "served", "published"):
         print(json.dumps({"impl": "reference", "workload": args.workload,
-                          "note": "the CPU arm times the single-volume workloads (nuclei, lightsheet, "
+                          "note": "the CPU arm times the single-volume workloads (lightsheet, nuclei, "
                                   "lightsheet_dense, blobs2d); run it with one of those"}), flush=True)
         return
     host = make_input(args.workload)
     if hasattr(host, "cpu"):
         host = host.cpu().numpy()
     f = host.astype(np.float32)
+    del host
     cores = oracle.num_threads()
-    # one untimed full step sizes the per-step sample so the run stays short
-    t0 = time.perf_counter()
-    cpu_step(f if f.ndim == 2 or f.shape[0] <= 128 else f[:32], w)
-    t_full = (time.perf_counter() - t0) * (1 if f.ndim == 2 or f.shape[0] <= 128 else f.shape[0] / 32)
-    budget = 150.0
-    if f.ndim == 3 and t_full * (args.steps + args.warmup) > budget:
-        planes = max(8, int(f.shape[0] * budget / (t_full * (args.steps + args.warmup))))
-        f = np.ascontiguousarray(f[:planes])
-    sample = f"{f.shape} slab of the workload per step" if f.shape != host.shape else "full workload per step"
+    warm = f if f.ndim == 2 or f.shape[0] <= 32 else np.ascontiguousarray(f[:32])
     for _ in range(args.warmup):
-        cpu_step(f, w)
+        cpu_step(warm, w)
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -698,9 +888,10 @@ def run_reference(args):
         "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "impl": "reference", "config": {"workload": w["desc"], "voxels_per_step": int(f.size)},
+        "impl": "reference", "config": config_of(args.workload, f.size),
         "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": "the whole volume (%s voxels) every timed step; warm-up steps on %s "
+                                   "voxels" % ("x".join(map(str, f.shape)), "x".join(map(str, warm.shape)))},
         "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference CPU OpenCL path unavailable (no pyopencl / CPU OpenCL runtime / kernel sources); "
                 "its C restatement runs on all host threads"}), flush=True)
@@ -712,12 +903,18 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="nuclei", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--trace", action="store_true", help="include the Voronoi per-step trace")
     ap.add_argument("--tiles", type=int, default=512, help="batch workload: number of tiles")
     ap.add_argument("--lanes", type=int, default=8, help="batch/served: concurrent lanes (slots)")
     ap.add_argument("--duration", type=float, default=60.0, help="served workload: trace length in s")
+    ap.add_argument("--served-duration", type=float, default=10.0,
+                    help="single-volume workloads: length (s) of the served-vs-per-call trace in the "
+                         "line (0: leave it out)")
+    ap.add_argument("--closed-requests", type=int, default=120,
+                    help="served comparison at saturation: requests waiting at t=0")
+    ap.add_argument("--pool", type=int, default=6, help="served workload: volumes per size class")
     ap.add_argument("--rate", type=float, default=200.0, help="served workload: arrivals per s")
     ap.add_argument("--compute-streams", type=int, default=1, help="served workload: compute streams")
     ap.add_argument("--express-voxels", type=int, default=8 << 20,

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define CLE_B200_ABI_VERSION 1
+#define CLE_B200_ABI_VERSION 2
 
 typedef enum cle_dtype {
     CLE_U8 = 1,
@@ -51,7 +51,8 @@ typedef enum cle_status {
     CLE_ERR_WORKSPACE = 4,  /* workspace missing or too small -> RuntimeError */
     CLE_ERR_ITER_LIMIT = 5, /* device loop hit its step/time limit          */
     CLE_ERR_CUDA = 6,       /* CUDA runtime error             -> RuntimeError */
-    CLE_ERR_TOO_LARGE = 7   /* image exceeds the 2^31-2 voxel index range   */
+    CLE_ERR_TOO_LARGE = 7,  /* image exceeds the 2^31-2 voxel index range   */
+    CLE_ERR_CANCELLED = 8   /* the caller's cancel word stopped a device loop */
 } cle_status;
 
 typedef struct cle_tensor {
@@ -63,6 +64,28 @@ typedef struct cle_tensor {
     int32_t device;     /* CUDA device ordinal                              */
 } cle_tensor;
 
+/* Per-call limits of the device loops (the Voronoi growth of the composite
+ * ops runs until a step changes nothing; the reference's host loops,
+ * _tier5/_masked_voronoi_labeling.py:62-69, have no bound).  Passed by the
+ * entry points that run such a loop; NULL means every field at its default.
+ * A loop that reaches a limit stops, and the call's status word (see
+ * cle_workspace_status) reads CLE_ERR_ITER_LIMIT.  Nothing here is stored
+ * between calls: two calls with different options may run at once. */
+typedef struct cle_call_options {
+    uint32_t struct_bytes;          /* sizeof(cle_call_options); 0 = this version's size */
+    uint32_t max_loop_steps;        /* 0 = voxels + 16 (every step that does not stop
+                                       the loop labels at least one voxel) */
+    uint32_t loop_time_limit_ms;    /* 0 = 20000: wall-clock bound of one loop launch */
+    uint32_t barrier_time_limit_ms; /* 0 = 4000: bound of one grid-barrier wait */
+    int32_t cooperative_ctas;       /* 0 = one CTA per SM; n > 0 caps the loop's grid at n
+                                       CTAs (several pipelines sharing the GPU) */
+    int32_t reserved;               /* must be 0 */
+    const volatile int32_t *cancel; /* NULL, or a word in page-locked host memory
+                                       (cudaHostAlloc / cudaHostRegister): the loop reads it
+                                       once per step and stops with CLE_ERR_CANCELLED once
+                                       it is nonzero (per-request cancellation) */
+} cle_call_options;
+
 /* Number of float32 columns of the statistics table (see
  * cle_statistics_of_labelled_pixels). */
 #define CLE_STATS_NCOLS 35
@@ -73,13 +96,8 @@ const char *cle_version(void);
 const char *cle_last_error_message(void);
 /* Number of kernel launches this library has issued in this process. */
 unsigned long long cle_kernel_launches(void);
-/* Several pipelines on one GPU at once (batched and served forms): caps the
- * CTAs of each cooperative launch (the growth loops) at max_ctas so that the
- * concurrent grids fit on the GPU together; 0 restores one CTA per SM.
- * Process-wide. */
-void cle_set_cooperative_ctas(int max_ctas);
-
-/* Profiling (off by default).  flags bit 0: the composite ops record a CUDA
+/* Profiling (off by default; the setting belongs to the calling host thread
+ * and covers the calls that thread makes).  flags bit 0: the composite ops record a CUDA
  * event at each stage boundary on their stream; bit 1: the Voronoi loop also
  * writes a per-step trace to a buffer allocated here (not in the compute
  * calls).  0 turns profiling off.
@@ -143,9 +161,11 @@ int cle_threshold_otsu(const cle_tensor *src, const cle_tensor *dst, double *d_t
  * cle_threshold_otsu; the scratch is an array built into the library
  * (cle_threshold_otsu_noalloc_scratch_bytes(), about 4 MiB, held on every
  * GPU that loads the library until the process exits), which limits the
- * image to 4096 rows (y); larger images return CLE_ERR_TOO_LARGE.  The first
- * call on each device looks up the array's device address -- make that call
- * before any stream capture.  All calls share the array: calls that overlap
+ * image to 4096 rows (y); larger images return CLE_ERR_TOO_LARGE.  Every
+ * call looks up the array's device address on its device (no cached pointer
+ * survives a device reset); the first call on each device is its set-up and
+ * loads the library's code there -- make that call before any stream
+ * capture.  All calls share the array: calls that overlap
  * on the GPU (different streams or threads) race and must be serialised by
  * the caller.  Allocates nothing. */
 int cle_threshold_otsu_noalloc(const cle_tensor *src, const cle_tensor *dst, void *stream);
@@ -242,8 +262,8 @@ int cle_relabel_sequential(const cle_tensor *src, const cle_tensor *dst, uint32_
  * seeds anywhere (dense Jacobi on the device, exact reference semantics). */
 size_t cle_masked_voronoi_labeling_workspace_bytes(const cle_tensor *binary);
 int cle_masked_voronoi_labeling(const cle_tensor *binary, const cle_tensor *mask,
-                                const cle_tensor *dst, void *workspace, size_t workspace_bytes,
-                                void *stream);
+                                const cle_tensor *dst, const cle_call_options *options,
+                                void *workspace, size_t workspace_bytes, void *stream);
 
 /* Fast form of masked_voronoi_labeling for the case voronoi_otsu_labeling
  * produces: mask values in {0, 1} and every seed inside the mask (then the
@@ -253,8 +273,8 @@ int cle_masked_voronoi_labeling(const cle_tensor *binary, const cle_tensor *mask
  * workspace (cle_workspace_status) reports the loop outcome. */
 size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *binary);
 int cle_masked_voronoi_labeling_binary(const cle_tensor *binary, const cle_tensor *mask,
-                                       const cle_tensor *dst, void *workspace,
-                                       size_t workspace_bytes, void *stream);
+                                       const cle_tensor *dst, const cle_call_options *options,
+                                       void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- extend_labeling_via_voronoi / voronoi_labeling -------------------
  * extend_labeling_via_voronoi replaces _tier4/_extend_labeling_via_voronoi.py:13-60:
@@ -265,10 +285,12 @@ int cle_masked_voronoi_labeling_binary(const cle_tensor *binary, const cle_tenso
  * The status word of the workspace (cle_workspace_status) reports the loop
  * outcome. */
 size_t cle_extend_labeling_via_voronoi_workspace_bytes(const cle_tensor *src);
-int cle_extend_labeling_via_voronoi(const cle_tensor *src, const cle_tensor *dst, void *workspace,
+int cle_extend_labeling_via_voronoi(const cle_tensor *src, const cle_tensor *dst,
+                                    const cle_call_options *options, void *workspace,
                                     size_t workspace_bytes, void *stream);
 size_t cle_voronoi_labeling_workspace_bytes(const cle_tensor *binary);
-int cle_voronoi_labeling(const cle_tensor *binary, const cle_tensor *dst, void *workspace,
+int cle_voronoi_labeling(const cle_tensor *binary, const cle_tensor *dst,
+                         const cle_call_options *options, void *workspace,
                          size_t workspace_bytes, void *stream);
 
 /* ---- voronoi_otsu_labeling ---------------------------------------------
@@ -277,8 +299,8 @@ int cle_voronoi_labeling(const cle_tensor *binary, const cle_tensor *dst, void *
  * dst: u32 (or f32).  No host synchronisation inside. */
 size_t cle_voronoi_otsu_labeling_workspace_bytes(const cle_tensor *src);
 int cle_voronoi_otsu_labeling(const cle_tensor *src, const cle_tensor *dst, double spot_sigma,
-                              double outline_sigma, void *workspace, size_t workspace_bytes,
-                              void *stream);
+                              double outline_sigma, const cle_call_options *options,
+                              void *workspace, size_t workspace_bytes, void *stream);
 
 /* Device pointer to the label count (= maximum label) written by the last
  * voronoi_otsu_labeling / masked_voronoi_labeling_binary call that used this

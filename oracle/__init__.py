@@ -348,24 +348,32 @@ def statistics_of_labelled_pixels(intensity, labels) -> dict:
 
 
 def euclidean_distance_from_label_centroid_map(labels) -> np.ndarray:
-    """Each labelled pixel's distance to its label's centroid, background 0
-    (_tier9/_euclidean_distance_from_label_centroid_map.py with the centroids
-    of _tier9/_centroids_of_labels.py: coordinate sums / pixel count, float32).
-    Distances in float64, returned as float32."""
+    """Each labelled pixel's distance to its label's point in the centroid list
+    of _tier9/_centroids_of_background_and_labels.py (column 0 the background's
+    centroid, column k label k's: coordinate sums / pixel count, float32),
+    label-0 pixels 0 (_tier9/_euclidean_distance_from_label_centroid_map.py).
+    The label is read like an image read of the list: (int) of the value,
+    clamped to the list's columns, so a negative label reads column 0 (the
+    background centroid) and gets its distance to it.  Distances in float64,
+    returned as float32."""
     lab = np.asarray(labels)
     if lab.dtype.kind == "f":
-        lab = lab.astype(np.int64)
-    lab = np.clip(lab, 0, None).astype(np.int64)
-    st = statistics_of_labelled_pixels(np.zeros(lab.shape, np.float32), lab)
-    L = len(st["label"])
+        lab = np.nan_to_num(lab, nan=0.0).astype(np.int64)
+    lab = lab.astype(np.int64)
+    # the point list: statistics of labels + 1 (label 1 = the background);
+    # negative labels (+1 <= 0) are in no column's sums
+    lab1 = np.where(lab >= 0, lab + 1, 0)
+    st = statistics_of_labelled_pixels(np.zeros(lab.shape, np.float32), lab1)
+    m = len(st["label"])                          # columns 0 .. m-1 = labels 0 .. m-1
     out = np.zeros(lab.shape, np.float64)
-    if L == 0:
+    if m == 0:
         return out.astype(np.float32)
     keys = ("centroid_x", "centroid_y", "centroid_z")[:lab.ndim if lab.ndim == 3 else 2]
-    cen = [np.concatenate([[0.0], st[k].astype(np.float64)]) for k in keys]
+    cen = [st[k].astype(np.float32) for k in keys]
+    col = np.clip(lab, 0, m - 1)
     coords = np.indices(lab.shape)[::-1]          # x, y(, z) grids
     d2 = np.zeros(lab.shape, np.float64)
     for c, grid in zip(cen, coords):
-        d2 += (grid - c[lab]) ** 2
-    out = np.where(lab > 0, np.sqrt(d2), 0.0)
+        d2 += (grid - c[col].astype(np.float64)) ** 2
+    out = np.where(lab != 0, np.sqrt(d2), 0.0)
     return out.astype(np.float32)

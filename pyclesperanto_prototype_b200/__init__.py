@@ -21,7 +21,7 @@ from ._ops import (STATISTICS_ENTRY, add_image_and_scalar, centroids_of_backgrou
                    label_pixel_count_map, label_standard_deviation_intensity_map, push_regionprops,
                    push_regionprops_column, replace_intensities,
                    statistics_of_background_and_labelled_pixels)
-from ._ops import (binary_and, connected_components_labeling_box,
+from ._ops import (binary_and, call_options, connected_components_labeling_box,
                    connected_components_labeling_diamond, detect_maxima_box,
                    erode_box, eroded_otsu_labeling, extend_labeling_via_voronoi, gauss_otsu_labeling,
                    voronoi_labeling,

@@ -34,7 +34,10 @@ ERRORS = {
     5: RuntimeError,    # device loop limit
     6: RuntimeError,    # CUDA
     7: ValueError,      # too large
+    8: RuntimeError,    # cancelled through the call's cancel word
 }
+CLE_ERR_ITER_LIMIT = 5
+CLE_ERR_CANCELLED = 8
 
 
 class CleTensor(ctypes.Structure):
@@ -48,18 +51,46 @@ class CleTensor(ctypes.Structure):
     ]
 
 
+class CallOptions(ctypes.Structure):
+    """cle_call_options: per-call limits of the device loops (0 = default)."""
+    _fields_ = [
+        ("struct_bytes", ctypes.c_uint32),
+        ("max_loop_steps", ctypes.c_uint32),
+        ("loop_time_limit_ms", ctypes.c_uint32),
+        ("barrier_time_limit_ms", ctypes.c_uint32),
+        ("cooperative_ctas", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("cancel", ctypes.c_void_p),
+    ]
+
+
+def call_options(max_loop_steps: int = 0, loop_time_limit_ms: int = 0, barrier_time_limit_ms: int = 0,
+                 cooperative_ctas: int = 0, cancel_ptr: int = 0) -> CallOptions:
+    """cancel_ptr: address of an int32 in pinned host memory (or 0): a nonzero
+    value there stops the call's device loop with CLE_ERR_CANCELLED."""
+    o = CallOptions()
+    o.struct_bytes = ctypes.sizeof(CallOptions)
+    o.max_loop_steps = int(max_loop_steps)
+    o.loop_time_limit_ms = int(loop_time_limit_ms)
+    o.barrier_time_limit_ms = int(barrier_time_limit_ms)
+    o.cooperative_ctas = int(cooperative_ctas)
+    o.reserved = 0
+    o.cancel = int(cancel_ptr) or None
+    return o
+
+
 _lib = None
 
 # name: (restype, argtypes)
 _P = ctypes.c_void_p
 _T = ctypes.POINTER(CleTensor)
 _SZ = ctypes.c_size_t
+_O = ctypes.POINTER(CallOptions)
 _SIGS = {
     "cle_abi_version": (ctypes.c_int, []),
     "cle_version": (ctypes.c_char_p, []),
     "cle_last_error_message": (ctypes.c_char_p, []),
     "cle_kernel_launches": (ctypes.c_ulonglong, []),
-    "cle_set_cooperative_ctas": (None, [ctypes.c_int]),
     "cle_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "cle_profile_stage_ms": (ctypes.c_int, [_P, ctypes.c_int]),
     "cle_profile_trace": (ctypes.c_int, [_P, _SZ]),
@@ -91,17 +122,17 @@ _SIGS = {
     "cle_relabel_sequential_workspace_bytes": (_SZ, [_T, ctypes.c_uint32]),
     "cle_relabel_sequential": (ctypes.c_int, [_T, _T, ctypes.c_uint32, _P, _SZ, _P]),
     "cle_masked_voronoi_labeling_workspace_bytes": (_SZ, [_T]),
-    "cle_masked_voronoi_labeling": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
+    "cle_masked_voronoi_labeling": (ctypes.c_int, [_T, _T, _T, _O, _P, _SZ, _P]),
     "cle_connected_components_labeling_diamond_workspace_bytes": (_SZ, [_T]),
     "cle_connected_components_labeling_diamond": (ctypes.c_int, [_T, _T, _P, _SZ, _P]),
     "cle_extend_labeling_via_voronoi_workspace_bytes": (_SZ, [_T]),
-    "cle_extend_labeling_via_voronoi": (ctypes.c_int, [_T, _T, _P, _SZ, _P]),
+    "cle_extend_labeling_via_voronoi": (ctypes.c_int, [_T, _T, _O, _P, _SZ, _P]),
     "cle_voronoi_labeling_workspace_bytes": (_SZ, [_T]),
-    "cle_voronoi_labeling": (ctypes.c_int, [_T, _T, _P, _SZ, _P]),
+    "cle_voronoi_labeling": (ctypes.c_int, [_T, _T, _O, _P, _SZ, _P]),
     "cle_masked_voronoi_labeling_binary_workspace_bytes": (_SZ, [_T]),
-    "cle_masked_voronoi_labeling_binary": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
+    "cle_masked_voronoi_labeling_binary": (ctypes.c_int, [_T, _T, _T, _O, _P, _SZ, _P]),
     "cle_voronoi_otsu_labeling_workspace_bytes": (_SZ, [_T]),
-    "cle_voronoi_otsu_labeling": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
+    "cle_voronoi_otsu_labeling": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, _O, _P, _SZ, _P]),
     "cle_workspace_status": (ctypes.c_int, [_P, _SZ, _P]),
     "cle_workspace_label_count": (_P, [_P]),
     "cle_statistics_of_labelled_pixels_device_count": (ctypes.c_int, [_T, _T, _P, ctypes.c_int64, _P, _P, _SZ, _P]),

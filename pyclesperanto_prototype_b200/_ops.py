@@ -4,6 +4,8 @@ Each function keeps the reference's name, parameter names, defaults, output
 creator and return value; the work is one call into libcle_b200.so on the
 current torch CUDA stream.  Reference citations are on each function.
 """
+import contextlib
+import threading
 import warnings
 from enum import Enum
 
@@ -31,6 +33,35 @@ assert len(STAT_KEYS) == _lib.STATS_NCOLS
 
 def _T(a: B200Array):
     return _lib.tensor_desc(a.tensor)
+
+
+_tls = threading.local()
+
+
+@contextlib.contextmanager
+def call_options(max_loop_steps: int = 0, loop_time_limit_ms: int = 0, barrier_time_limit_ms: int = 0,
+                 cooperative_ctas: int = 0):
+    """Limits of the device loops (the Voronoi growth) for the cle.* calls this
+    thread makes inside the block; 0 keeps a field's default.  A loop that
+    reaches a limit raises RuntimeError from the call.  The setting belongs to
+    the calling thread only; each call passes it to the library as an
+    argument (nothing is stored in the library).
+
+        with cle.call_options(max_loop_steps=1000):
+            labels = cle.voronoi_otsu_labeling(image)
+    """
+    prev = getattr(_tls, "options", None)
+    _tls.options = _lib.call_options(max_loop_steps, loop_time_limit_ms, barrier_time_limit_ms,
+                                     cooperative_ctas)
+    try:
+        yield _tls.options
+    finally:
+        _tls.options = prev
+
+
+def _opts():
+    o = getattr(_tls, "options", None)
+    return _lib.ref(o) if o is not None else None
 
 
 def _call(name, *args):
@@ -230,8 +261,11 @@ def masked_voronoi_labeling(binary_source: Image, mask_image: Image,
     seeds anywhere)."""
     b, m, d = _T(binary_source), _T(mask_image), _T(labeling_destination)
     ws = _ws("cle_masked_voronoi_labeling_workspace_bytes", _lib.ref(b))
-    _call("cle_masked_voronoi_labeling", _lib.ref(b), _lib.ref(m), _lib.ref(d), _ptr(ws), ws.numel(),
-          _lib.stream_ptr())
+    stream = _lib.stream_ptr()
+    _call("cle_masked_voronoi_labeling", _lib.ref(b), _lib.ref(m), _lib.ref(d), _opts(), _ptr(ws),
+          ws.numel(), stream)
+    _lib.check(_lib.load().cle_workspace_status(ws.data_ptr(), ws.numel(), stream),
+               "masked_voronoi_labeling")
     return labeling_destination
 
 
@@ -247,8 +281,8 @@ def masked_voronoi_labeling_binary(binary_source, mask_image, labeling_destinati
     bd, md, dd = _T(b), _T(m), _T(labeling_destination)
     ws = _ws("cle_masked_voronoi_labeling_binary_workspace_bytes", _lib.ref(bd))
     stream = _lib.stream_ptr()
-    _call("cle_masked_voronoi_labeling_binary", _lib.ref(bd), _lib.ref(md), _lib.ref(dd), _ptr(ws),
-          ws.numel(), stream)
+    _call("cle_masked_voronoi_labeling_binary", _lib.ref(bd), _lib.ref(md), _lib.ref(dd), _opts(),
+          _ptr(ws), ws.numel(), stream)
     _lib.check(_lib.load().cle_workspace_status(ws.data_ptr(), ws.numel(), stream),
                "masked_voronoi_labeling")
     return labeling_destination
@@ -270,7 +304,7 @@ def _grow_call(name, src: B200Array, dst: B200Array):
     s, d = _T(src), _T(dst)
     ws = _ws(name + "_workspace_bytes", _lib.ref(s))
     stream = _lib.stream_ptr()
-    _call(name, _lib.ref(s), _lib.ref(d), _ptr(ws), ws.numel(), stream)
+    _call(name, _lib.ref(s), _lib.ref(d), _opts(), _ptr(ws), ws.numel(), stream)
     _lib.check(_lib.load().cle_workspace_status(ws.data_ptr(), ws.numel(), stream), name[4:])
     return dst
 
@@ -622,7 +656,7 @@ def _vol(source: B200Array, dest: B200Array, spot_sigma, outline_sigma, check=Tr
     s, d = _T(source), _T(dest)
     stream = _lib.stream_ptr()
     _call("cle_voronoi_otsu_labeling", _lib.ref(s), _lib.ref(d), float(spot_sigma),
-          float(outline_sigma), ws.data_ptr(), ws.numel(), stream)
+          float(outline_sigma), _opts(), ws.data_ptr(), ws.numel(), stream)
     if check:
         _lib.check(_lib.load().cle_workspace_status(ws.data_ptr(), ws.numel(), stream),
                    "voronoi_otsu_labeling")

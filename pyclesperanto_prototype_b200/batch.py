@@ -42,12 +42,15 @@ def vol_workspace_bytes(shape, dtype=torch.float32) -> int:
 
 
 def vol_into(src: torch.Tensor, dst: torch.Tensor, ws: torch.Tensor, spot_sigma: float,
-             outline_sigma: float, stream: int) -> None:
-    """One voronoi_otsu_labeling on `stream` with an explicit workspace."""
+             outline_sigma: float, stream: int, options: "_lib.CallOptions" = None) -> None:
+    """One voronoi_otsu_labeling on `stream` with an explicit workspace and
+    per-call loop options (None: defaults)."""
     s, d = _desc(src), _desc(dst)
     lib = _lib.load()
     _lib.check(lib.cle_voronoi_otsu_labeling(_lib.ref(s), _lib.ref(d), float(spot_sigma),
-                                             float(outline_sigma), ws.data_ptr(), ws.numel(), stream),
+                                             float(outline_sigma),
+                                             _lib.ref(options) if options is not None else None,
+                                             ws.data_ptr(), ws.numel(), stream),
                "voronoi_otsu_labeling")
 
 
@@ -76,7 +79,7 @@ class VolBatch:
     """
 
     def __init__(self, inputs, spot_sigma: float = 2.0, outline_sigma: float = 2.0,
-                 lanes: int = 8, use_graph: bool = True):
+                 lanes: int = 8, use_graph: bool = True, max_loop_steps: int = 0):
         _lib.load()
         self.inputs = [x.tensor if isinstance(x, B200Array) else x for x in inputs]
         for t in self.inputs:
@@ -100,7 +103,11 @@ class VolBatch:
         self.graph = None
         self.use_graph = use_graph
         self.launches_per_run = 0     # library kernels one run launches
-        self._coop = max(1, torch.cuda.get_device_properties(self.device).multi_processor_count // self.lanes)
+        # while several lanes run, each lane's cooperative growth launch is
+        # capped at its share of the SMs (passed with every call)
+        coop = max(1, torch.cuda.get_device_properties(self.device).multi_processor_count // self.lanes)
+        self.options = _lib.call_options(max_loop_steps=max_loop_steps,
+                                         cooperative_ctas=coop if self.lanes > 1 else 0)
 
     def _issue(self):
         main = torch.cuda.current_stream(self.device)
@@ -111,46 +118,39 @@ class VolBatch:
             with torch.cuda.stream(s):
                 word = ws[:4].view(torch.int32)
                 for i in p:
-                    vol_into(self.inputs[i], self.outputs[i], ws, self.spot, self.outline, s.cuda_stream)
+                    vol_into(self.inputs[i], self.outputs[i], ws, self.spot, self.outline, s.cuda_stream,
+                             self.options)
                     torch.maximum(self.status[k:k + 1], word, out=self.status[k:k + 1])
         for s in self.streams:
             main.wait_stream(s)
 
     def capture(self):
         lib = _lib.load()
-        lib.cle_set_cooperative_ctas(self._coop if self.lanes > 1 else 0)
-        try:
-            self._issue()                       # uncaptured warm-up (sets kernel attributes)
-            torch.cuda.synchronize(self.device)
-            self.check()
-            if self.use_graph:
-                g = torch.cuda.CUDAGraph()
-                cap = torch.cuda.Stream(device=self.device)
-                cap.wait_stream(torch.cuda.current_stream(self.device))
-                n0 = lib.cle_kernel_launches()
-                with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
-                    self._issue()
-                self.launches_per_run = int(lib.cle_kernel_launches() - n0)
-                self.graph = g
-        finally:
-            lib.cle_set_cooperative_ctas(0)
+        self._issue()                       # uncaptured warm-up (sets kernel attributes)
+        torch.cuda.synchronize(self.device)
+        self.check()
+        if self.use_graph:
+            g = torch.cuda.CUDAGraph()
+            cap = torch.cuda.Stream(device=self.device)
+            cap.wait_stream(torch.cuda.current_stream(self.device))
+            n0 = lib.cle_kernel_launches()
+            with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
+                self._issue()
+            self.launches_per_run = int(lib.cle_kernel_launches() - n0)
+            self.graph = g
         return self
 
     def run(self):
         """One batch on the current stream (graph replay when captured)."""
         lib = _lib.load()
-        lib.cle_set_cooperative_ctas(self._coop if self.lanes > 1 else 0)
-        try:
-            if self.graph is None and self.use_graph:
-                self.capture()
-            if self.graph is not None:
-                self.graph.replay()
-            else:
-                n0 = lib.cle_kernel_launches()
-                self._issue()
-                self.launches_per_run = int(lib.cle_kernel_launches() - n0)
-        finally:
-            lib.cle_set_cooperative_ctas(0)
+        if self.graph is None and self.use_graph:
+            self.capture()
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            n0 = lib.cle_kernel_launches()
+            self._issue()
+            self.launches_per_run = int(lib.cle_kernel_launches() - n0)
         return self.outputs
 
     def check(self):

@@ -260,11 +260,8 @@ int launch_fused_r(const Img &src, float *dst, const Taps &t, float *mm, cudaStr
     using G = Geom<R>;
     static_assert(min_ctas<R>() == (R <= 8 ? 2 : 1), "fused_grid's occupancy rule");
     auto kern = blur_fused_kernel<Tin, R, Z>;
-    static bool attr_set = false;   // per instantiation
-    if (!attr_set) {
-        CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
-        attr_set = true;
-    }
+    // set on every call: the attribute belongs to the current device's context
+    CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
     int zchunk = 1;
     const dim3 grid = fused_grid(src, R, zchunk);
     if (grid.y > 65535 || grid.z > 65535) { set_error("gaussian_blur: image too large for the fused path"); return CLE_ERR_TOO_LARGE; }

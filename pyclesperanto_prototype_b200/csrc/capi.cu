@@ -37,7 +37,6 @@ const char *cle_version(void) { return "cle_b200 1.0 (sm_100a)"; }
 const char *cle_last_error_message(void) { return last_error(); }
 unsigned long long cle_kernel_launches(void) { return launches_issued(); }
 int cle_profile_enable(int flags) { return profile_enable(flags); }
-void cle_set_cooperative_ctas(int max_ctas) { set_cooperative_ctas(max_ctas); }
 int cle_profile_stage_ms(float *out, int max) { return stage_ms(out, max); }
 int cle_profile_trace(void *host, size_t bytes) { return profile_trace_read(host, bytes); }
 
@@ -330,8 +329,10 @@ size_t cle_masked_voronoi_labeling_workspace_bytes(const cle_tensor *bin) {
 }
 
 int cle_masked_voronoi_labeling(const cle_tensor *bin, const cle_tensor *msk, const cle_tensor *dst,
-                                void *ws, size_t ws_bytes, void *stream) {
+                                const cle_call_options *opts, void *ws, size_t ws_bytes, void *stream) {
     Img a, m, d;
+    Limits lim;
+    CLE_TRY(limits_from(opts, lim));
     CLE_TRY(to_img(bin, a, "binary_source"));
     CLE_TRY(to_img(msk, m, "mask_image"));
     CLE_TRY(to_img(dst, d, "labeling_destination"));
@@ -341,7 +342,7 @@ int cle_masked_voronoi_labeling(const cle_tensor *bin, const cle_tensor *msk, co
     Arena ar(ws, ws_bytes);
     int *status = ar.take<int>(64);
     CLE_CUDA(cudaMemsetAsync(status, 0, sizeof(int), S(stream)));
-    return masked_voronoi_dense(a, m, d, status, ar, S(stream));
+    return masked_voronoi_dense(a, m, d, status, ar, S(stream), lim);
 }
 
 size_t cle_connected_components_labeling_diamond_workspace_bytes(const cle_tensor *bin) {
@@ -373,15 +374,17 @@ size_t cle_extend_labeling_via_voronoi_workspace_bytes(const cle_tensor *src) {
     return extend_voronoi_workspace_bytes(im);
 }
 
-int cle_extend_labeling_via_voronoi(const cle_tensor *src, const cle_tensor *dst, void *ws, size_t ws_bytes,
-                                    void *stream) {
+int cle_extend_labeling_via_voronoi(const cle_tensor *src, const cle_tensor *dst,
+                                    const cle_call_options *opts, void *ws, size_t ws_bytes, void *stream) {
     Img a, d;
+    Limits lim;
+    CLE_TRY(limits_from(opts, lim));
     CLE_TRY(to_img(src, a, "labeling_source"));
     CLE_TRY(to_img(dst, d, "labeling_destination"));
     CLE_TRY(ws_check(ws, ws_bytes, extend_voronoi_workspace_bytes(a), "extend_labeling_via_voronoi"));
     CLE_TRY(set_device_of(a, src));
     Arena ar(ws, ws_bytes);
-    return extend_labeling_via_voronoi(a, d, ar, S(stream));
+    return extend_labeling_via_voronoi(a, d, ar, S(stream), lim);
 }
 
 size_t cle_voronoi_labeling_workspace_bytes(const cle_tensor *bin) {
@@ -390,15 +393,17 @@ size_t cle_voronoi_labeling_workspace_bytes(const cle_tensor *bin) {
     return extend_voronoi_workspace_bytes(im);
 }
 
-int cle_voronoi_labeling(const cle_tensor *bin, const cle_tensor *dst, void *ws, size_t ws_bytes,
-                         void *stream) {
+int cle_voronoi_labeling(const cle_tensor *bin, const cle_tensor *dst, const cle_call_options *opts,
+                         void *ws, size_t ws_bytes, void *stream) {
     Img a, d;
+    Limits lim;
+    CLE_TRY(limits_from(opts, lim));
     CLE_TRY(to_img(bin, a, "binary_source"));
     CLE_TRY(to_img(dst, d, "labeling_destination"));
     CLE_TRY(ws_check(ws, ws_bytes, extend_voronoi_workspace_bytes(a), "voronoi_labeling"));
     CLE_TRY(set_device_of(a, bin));
     Arena ar(ws, ws_bytes);
-    return voronoi_labeling(a, d, ar, S(stream));
+    return voronoi_labeling(a, d, ar, S(stream), lim);
 }
 
 size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *bin) {
@@ -408,16 +413,18 @@ size_t cle_masked_voronoi_labeling_binary_workspace_bytes(const cle_tensor *bin)
 }
 
 int cle_masked_voronoi_labeling_binary(const cle_tensor *bin, const cle_tensor *msk,
-                                       const cle_tensor *dst, void *ws, size_t ws_bytes,
-                                       void *stream) {
+                                       const cle_tensor *dst, const cle_call_options *opts, void *ws,
+                                       size_t ws_bytes, void *stream) {
     Img a, m, d;
+    Limits lim;
+    CLE_TRY(limits_from(opts, lim));
     CLE_TRY(to_img(bin, a, "binary_source"));
     CLE_TRY(to_img(msk, m, "mask_image"));
     CLE_TRY(to_img(dst, d, "labeling_destination"));
     CLE_TRY(ws_check(ws, ws_bytes, masked_voronoi_binary_workspace_bytes(a), "masked_voronoi_labeling"));
     CLE_TRY(set_device_of(a, bin));
     Arena ar(ws, ws_bytes);
-    return masked_voronoi_binary(a, m, d, ar, S(stream));
+    return masked_voronoi_binary(a, m, d, ar, S(stream), lim);
 }
 
 // ---- voronoi_otsu_labeling ----------------------------------------------------------
@@ -428,14 +435,17 @@ size_t cle_voronoi_otsu_labeling_workspace_bytes(const cle_tensor *src) {
 }
 
 int cle_voronoi_otsu_labeling(const cle_tensor *src, const cle_tensor *dst, double spot_sigma,
-                              double outline_sigma, void *ws, size_t ws_bytes, void *stream) {
+                              double outline_sigma, const cle_call_options *opts, void *ws,
+                              size_t ws_bytes, void *stream) {
     Img a, d;
+    Limits lim;
+    CLE_TRY(limits_from(opts, lim));
     CLE_TRY(to_img(src, a, "source"));
     CLE_TRY(to_img(dst, d, "label_image_destination"));
     CLE_TRY(ws_check(ws, ws_bytes, vol_workspace_bytes(a), "voronoi_otsu_labeling"));
     CLE_TRY(set_device_of(a, src));
     Arena ar(ws, ws_bytes);
-    return voronoi_otsu_labeling(a, d, spot_sigma, outline_sigma, ar, S(stream));
+    return voronoi_otsu_labeling(a, d, spot_sigma, outline_sigma, ar, S(stream), lim);
 }
 
 const uint32_t *cle_workspace_label_count(const void *ws) {

@@ -235,12 +235,40 @@ int num_sms(int device) {
     return cache[device];
 }
 
-static std::atomic<int> g_coop_ctas{0};
-void set_cooperative_ctas(int n) { g_coop_ctas.store(n > 0 ? n : 0); }
-int cooperative_ctas(int device) {
+int limits_from(const cle_call_options *o, Limits &out) {
+    out = Limits();
+    if (!o) return CLE_OK;
+    if (o->struct_bytes != 0 && o->struct_bytes < sizeof(cle_call_options)) {
+        set_error("call options: struct_bytes %u is smaller than this library's %zu", o->struct_bytes,
+                  sizeof(cle_call_options));
+        return CLE_ERR_ARG;
+    }
+    if (o->cooperative_ctas < 0 || o->reserved != 0) {
+        set_error("call options: cooperative_ctas must be >= 0 and reserved 0 (got %d, %d)",
+                  o->cooperative_ctas, o->reserved);
+        return CLE_ERR_ARG;
+    }
+    out.max_steps = o->max_loop_steps;
+    if (o->loop_time_limit_ms) out.loop_ns = (uint64_t)o->loop_time_limit_ms * 1000000ull;
+    if (o->barrier_time_limit_ms) out.barrier_ns = (uint64_t)o->barrier_time_limit_ms * 1000000ull;
+    out.coop_ctas = o->cooperative_ctas;
+    if (o->cancel) {
+        // the word must be page-locked host memory the device can read
+        void *dptr = nullptr;
+        cudaError_t e = cudaHostGetDevicePointer(&dptr, (void *)o->cancel, 0);
+        if (e != cudaSuccess || !dptr) {
+            (void)cudaGetLastError();
+            set_error("call options: the cancel word is not page-locked host memory the device can map");
+            return CLE_ERR_ARG;
+        }
+        out.cancel = (const volatile int *)dptr;
+    }
+    return CLE_OK;
+}
+
+int cooperative_ctas(int device, const Limits &lim) {
     const int sms = num_sms(device);
-    const int cap = g_coop_ctas.load();
-    return (cap > 0 && cap < sms) ? cap : sms;
+    return (lim.coop_ctas > 0 && lim.coop_ctas < sms) ? lim.coop_ctas : sms;
 }
 
 int launch_blocks(int64_t items, int threads, int max_blocks_per_sm) {

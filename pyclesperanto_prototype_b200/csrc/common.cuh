@@ -227,13 +227,29 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, int *err, uint64_t lim
     return *(volatile int *)err == 0;
 }
 
+// Per-call limits of the device loops (cle_call_options); a value, passed
+// down each call, never stored between calls.
+struct Limits {
+    uint32_t max_steps = 0;                     // 0: voxels + 16
+    uint64_t loop_ns = 20000000000ull;          // wall-clock bound of one loop launch
+    uint64_t barrier_ns = 4000000000ull;        // bound of one grid-barrier wait
+    int coop_ctas = 0;                          // 0: one CTA per SM
+    const volatile int *cancel = nullptr;       // device view of the caller's cancel word
+    // step bound of a loop over n voxels
+    uint32_t steps_for(int64_t n) const {
+        const uint64_t dflt = (uint64_t)n + 16u;
+        const uint64_t s = max_steps ? std::min<uint64_t>(max_steps, dflt) : dflt;
+        return (uint32_t)std::min<uint64_t>(s, 0xFFFFFFF0ull);
+    }
+};
+// Validates options (NULL = defaults) into a Limits.
+int limits_from(const cle_call_options *o, Limits &out);
+
 // Launch helpers
 int num_sms(int device);
-// Upper bound on the CTAs of one cooperative launch (0 = one per SM).  Set
-// when several pipelines run concurrently (batched / served forms) so their
-// cooperative grids fit on the GPU together.
-void set_cooperative_ctas(int n);
-int cooperative_ctas(int device);
+// CTAs one cooperative launch may use on `device` under lim (one per SM
+// unless lim caps it).
+int cooperative_ctas(int device, const Limits &lim);
 int launch_blocks(int64_t items, int threads, int max_blocks_per_sm = 8);
 
 }  // namespace cle

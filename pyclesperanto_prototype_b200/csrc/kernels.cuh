@@ -81,10 +81,10 @@ size_t voronoi_frontier_workspace_bytes(const Img &im);
 // d_seed_count).  d_status receives 0 or an error.
 int voronoi_frontier(const Img &shape, uint32_t *labels, const uint8_t *seg,
                      const uint32_t *seeds, const uint32_t *d_seed_count, int *d_status,
-                     Arena &ws, cudaStream_t st);
+                     Arena &ws, cudaStream_t st, const Limits &lim);
 size_t voronoi_dense_workspace_bytes(const Img &im);
 int masked_voronoi_dense(const Img &binary, const Img &mask, const Img &dst, int *d_status,
-                         Arena &ws, cudaStream_t st);
+                         Arena &ws, cudaStream_t st, const Limits &lim);
 
 // stats.cu
 size_t stats_workspace_bytes(const Img &labels, int64_t L);
@@ -94,16 +94,18 @@ int statistics(const Img &inten, const Img &labels, int64_t L, float *d_table, A
 // pipeline.cu
 size_t vol_workspace_bytes(const Img &im);
 int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma,
-                          double outline_sigma, Arena &ws, cudaStream_t st);
+                          double outline_sigma, Arena &ws, cudaStream_t st, const Limits &lim);
 
 // masked_voronoi_labeling for a 0/1 mask with every seed inside it (the
 // composite's case), on the active-brick growth.
 size_t masked_voronoi_binary_workspace_bytes(const Img &im);
-int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st);
+int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st,
+                          const Limits &lim);
 // extend_labeling_via_voronoi / voronoi_labeling (status word at workspace offset 0)
 size_t extend_voronoi_workspace_bytes(const Img &im);
-int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaStream_t st);
-int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st);
+int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaStream_t st,
+                                const Limits &lim);
+int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st, const Limits &lim);
 
 // noalloc.cu: threshold_otsu with a built-in scratch array
 size_t threshold_otsu_noalloc_capacity();

@@ -11,17 +11,17 @@
 // that loads the library holds until the process exits.
 //
 // Host code never uses the array's name as a pointer (on the host it only
-// stands for the symbol); the first call on each device, with that device
-// current, resolves the array's device address with cudaGetSymbolAddress and
-// caches it.  That first call should therefore come before any stream
-// capture.  All calls share the one array and each call rewrites every part
+// stands for the symbol): every call, with the call's device current,
+// resolves the array's device address with cudaGetSymbolAddress.  The first
+// call on a device also loads the library's code onto it (set-up), so that
+// first call should come before any stream capture; later look-ups are cheap.
+// Nothing is cached, so a device reset (which reloads the code at a new
+// address) leaves no stale pointer behind.  All calls share the one array and each call rewrites every part
 // of it it reads (the row partials are cleared on the stream first), so a
 // call sees nothing of the previous one; calls that overlap on the GPU (other
 // streams, other host threads) race on it and must be serialised by the
 // caller.  No allocation happens here: no cudaMalloc, no cudaFree, no
 // allocating library routine.
-#include <mutex>
-
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -32,34 +32,20 @@ namespace {
 // 4 MiB of row partials (4096 rows x 256 bins x 4 B) plus 64 KiB for the
 // min/max partials, the histogram and the threshold.
 constexpr size_t kScratchBytes = (size_t(4) << 20) + (size_t(64) << 10);
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-std::mutex g_mu;
-void *g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch array on the current device (set-up once
-// per device).
+// Device address of the scratch array on the current device, looked up on
+// each call (the first look-up on a device is its set-up).
 int scratch_address(void **out) {
-    int dev = 0;
-    CLE_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) {
-        set_error("threshold_otsu_noalloc: device ordinal %d out of range", dev);
-        return CLE_ERR_ARG;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(noalloc scratch)");
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 255)) {
+        set_error("threshold_otsu_noalloc: scratch array address is not 256-byte aligned");
+        return CLE_ERR_CUDA;
     }
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(noalloc scratch)");
-        if (!p || (reinterpret_cast<uintptr_t>(p) & 255)) {
-            set_error("threshold_otsu_noalloc: scratch array address is not 256-byte aligned");
-            return CLE_ERR_CUDA;
-        }
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    *out = p;
     return CLE_OK;
 }
 

@@ -162,7 +162,8 @@ size_t masked_voronoi_binary_workspace_bytes(const Img &im) {
     return a.off + tail;
 }
 
-int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st) {
+int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena &ws, cudaStream_t st,
+                          const Limits &lim) {
     CLE_TRY(same_shape(bin, mask, "binary_source", "mask_image"));
     CLE_TRY(same_shape(bin, dst, "binary_source", "labeling_destination"));
     if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
@@ -186,7 +187,7 @@ int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena
     }
     CLE_TRY(ccl_list(g, bin.n(), lab, l.seeds, &l.sc->seed_count, bin.n(), ws, st, &l.sc->nlabels));
     ws.off = tail_off;
-    CLE_TRY(voronoi_frontier(bin, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st));
+    CLE_TRY(voronoi_frontier(bin, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st, lim));
     if (dst.dtype == CLE_F32) {
         u32_to_f32<<<launch_blocks(dst.n(), 256), 256, 0, st>>>(lab, (float *)dst.data, dst.n());
         CLE_LAUNCH_CHECK("labels to f32");
@@ -269,14 +270,15 @@ ExtLayout take_ext_layout(Arena &a, const Img &im) {
 }
 
 // Grows `lab` in place over the whole image; status in l.sc.
-int grow_everywhere(const Img &im, uint32_t *lab, ExtLayout &l, Arena &tail, cudaStream_t st) {
+int grow_everywhere(const Img &im, uint32_t *lab, ExtLayout &l, Arena &tail, cudaStream_t st,
+                    const Limits &lim) {
     CLE_CUDA(cudaMemsetAsync(l.seg, 1, (size_t)im.n(), st));
     const uint32_t WB = (uint32_t)((im.W + 31) / 32);
     const uint32_t nb = (uint32_t)(im.D * im.H) * WB;
     brick_seeds_kernel<<<launch_blocks((int64_t)nb * 32, kSeedWarps * 32), kSeedWarps * 32, 0, st>>>(
         lab, (uint32_t)im.W, WB, FastDiv(WB), nb, l.seeds, &l.sc->seed_count);
     CLE_LAUNCH_CHECK("brick seeds");
-    return voronoi_frontier(im, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, tail, st);
+    return voronoi_frontier(im, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, tail, st, lim);
 }
 
 }  // namespace
@@ -288,7 +290,8 @@ size_t extend_voronoi_workspace_bytes(const Img &im) {
     return a.off + tail;
 }
 
-int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaStream_t st) {
+int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaStream_t st,
+                                const Limits &lim) {
     CLE_TRY(same_shape(src, dst, "labeling_source", "labeling_destination"));
     if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
         set_error("extend_labeling_via_voronoi: destination must be uint32 or float32");
@@ -314,7 +317,7 @@ int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaS
         default: set_error("extend_labeling_via_voronoi: unsupported source dtype %d", src.dtype); return CLE_ERR_DTYPE;
     }
     CLE_LAUNCH_CHECK("labels");
-    CLE_TRY(grow_everywhere(src, lab, l, ws, st));
+    CLE_TRY(grow_everywhere(src, lab, l, ws, st, lim));
     if (dst.dtype == CLE_F32) {
         u32_to_f32<<<launch_blocks(n, 256), 256, 0, st>>>(lab, (float *)dst.data, n);
         CLE_LAUNCH_CHECK("labels to f32");
@@ -322,7 +325,7 @@ int extend_labeling_via_voronoi(const Img &src, const Img &dst, Arena &ws, cudaS
     return CLE_OK;
 }
 
-int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st) {
+int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st, const Limits &lim) {
     CLE_TRY(same_shape(bin, dst, "binary_source", "labeling_destination"));
     if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
         set_error("voronoi_labeling: destination must be uint32 or float32");
@@ -338,7 +341,7 @@ int voronoi_labeling(const Img &bin, const Img &dst, Arena &ws, cudaStream_t st)
     uint32_t *lab = dst.dtype == CLE_U32 ? (uint32_t *)dst.data : l.lab;
     CLE_TRY(ccl_dense(bin, lab, ws, st));
     ws.off = tail_off;
-    CLE_TRY(grow_everywhere(bin, lab, l, ws, st));
+    CLE_TRY(grow_everywhere(bin, lab, l, ws, st, lim));
     if (dst.dtype == CLE_F32) {
         u32_to_f32<<<launch_blocks(dst.n(), 256), 256, 0, st>>>(lab, (float *)dst.data, dst.n());
         CLE_LAUNCH_CHECK("labels to f32");
@@ -364,7 +367,7 @@ size_t vol_workspace_bytes(const Img &im) {
 }
 
 int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, double outline_sigma,
-                          Arena &ws, cudaStream_t st) {
+                          Arena &ws, cudaStream_t st, const Limits &lim) {
     CLE_TRY(same_shape(src, dst, "source", "label_image_destination"));
     if (dst.dtype != CLE_U32 && dst.dtype != CLE_F32) {
         set_error("voronoi_otsu_labeling: destination must be uint32 or float32 (got %d)", dst.dtype);
@@ -380,8 +383,16 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     stage_mark(0, st);
     CLE_CUDA(cudaMemsetAsync(l.sc, 0, sizeof(Scalars), st));
 
-    // 1-3: blurs and maxima (the blur's temporaries live in the tail)
-    CLE_TRY(gaussian_blur(src, l.T, spot_sigma, spot_sigma, spot_sigma, ws, st));
+    // 1-3: blurs and maxima (the blur's temporaries live in the tail).  The
+    // two blurs build their taps from the float32 sigma and the kernel size
+    // int(8 sigma)|1, so equal float32 sigmas with equal kernel sizes give the
+    // same image bit for bit: then it is computed once (with the min / max the
+    // outline blur reduces) and serves both the spot detection and the
+    // threshold, as the reference's second blur would have recomputed it.
+    const bool same_blur = (float)spot_sigma == (float)outline_sigma &&
+                           sigma_to_kernel_size(spot_sigma) == sigma_to_kernel_size(outline_sigma);
+    if (same_blur) CLE_TRY(blur_minmax(src, l.T, spot_sigma, l.sc->minmax, ws, st));
+    else CLE_TRY(gaussian_blur(src, l.T, spot_sigma, spot_sigma, spot_sigma, ws, st));
     stage_mark(1, st);
     ws.off = tail_off;
     Img Ti = src;
@@ -393,7 +404,7 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     CLE_TRY(detect_maxima(Ti, Si, st));
     stage_mark(2, st);
     // the outline blur also reduces the blurred image's min / max (step 4)
-    CLE_TRY(blur_minmax(src, l.T, outline_sigma, l.sc->minmax, ws, st));
+    if (!same_blur) CLE_TRY(blur_minmax(src, l.T, outline_sigma, l.sc->minmax, ws, st));
     ws.off = tail_off;
     stage_mark(3, st);
 
@@ -422,7 +433,7 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     stage_mark(6, st);
 
     // 9: grow inside the segmentation
-    CLE_TRY(voronoi_frontier(src, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st));
+    CLE_TRY(voronoi_frontier(src, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st, lim));
     ws.off = tail_off;
     stage_mark(7, st);
 

@@ -20,8 +20,6 @@ namespace cle {
 namespace {
 
 constexpr int kVT = 512;
-constexpr uint64_t kBarrierLimitNs = 4000000000ull;   // 4 s per barrier wait
-constexpr uint64_t kKernelLimitNs = 20000000000ull;   // 20 s per launch
 
 __device__ __forceinline__ uint32_t block_sum(uint32_t v) {
     __shared__ uint32_t red[32];
@@ -54,7 +52,8 @@ __global__ void vor_dense_init(const Tb *__restrict__ bin_unused, const Tm *__re
 
 __global__ void __launch_bounds__(kVT)
 vor_dense_kernel(float *A, float *B, Geo g, int is3d, int64_t n, DenseState *S, int *d_status,
-                 int *d_parity, uint32_t max_steps) {
+                 int *d_parity, uint32_t max_steps, uint64_t loop_ns, uint64_t barrier_ns,
+                 const volatile int *cancel) {
     const int64_t gtid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
     const int zr = is3d ? 1 : 0;
@@ -62,7 +61,10 @@ vor_dense_kernel(float *A, float *B, Geo g, int is3d, int64_t n, DenseState *S, 
     uint32_t t = 0;
     const uint64_t t_start = global_ns();
     while (ok && t < max_steps) {
-        if (gtid == 0 && global_ns() - t_start > kKernelLimitNs) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
+        if (gtid == 0) {
+            if (global_ns() - t_start > loop_ns) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
+            else if (cancel && *cancel) atomicExch(&S->err, (int)CLE_ERR_CANCELLED);
+        }
         const float *cur = (t & 1) ? B : A;
         float *nxt = (t & 1) ? A : B;
         const bool box = (t & 1) == 0;
@@ -87,7 +89,7 @@ vor_dense_kernel(float *A, float *B, Geo g, int is3d, int64_t n, DenseState *S, 
         }
         uint32_t bs = block_sum(changed);
         if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
-        ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
+        ok = grid_sync(&S->bar, &S->err, barrier_ns);
         if (!ok) break;
         const uint32_t c = __ldcg(&S->changes[t & 3]);
         if (gtid == 0) S->changes[(t + 2) & 3] = 0u;
@@ -117,7 +119,8 @@ __global__ void vor_dense_out(const float *__restrict__ A, const float *__restri
     }
 }
 
-int coop_grid(const void *func, int threads, size_t smem, int64_t work, int max_per_sm = 64) {
+int coop_grid(const void *func, int threads, size_t smem, int64_t work, const Limits &lim,
+              int max_per_sm = 64) {
     int dev = 0;
     cudaGetDevice(&dev);
     int per_sm = 0;
@@ -125,7 +128,7 @@ int coop_grid(const void *func, int threads, size_t smem, int64_t work, int max_
         per_sm < 1)
         per_sm = 1;
     if (per_sm > max_per_sm) per_sm = max_per_sm;
-    int64_t cap = (int64_t)per_sm * cooperative_ctas(dev);
+    int64_t cap = (int64_t)per_sm * cooperative_ctas(dev, lim);
     int64_t want = (work + threads * 4 - 1) / (threads * 4);
     if (want < 1) want = 1;
     return (int)(want < cap ? want : cap);
@@ -154,7 +157,7 @@ static int dense_out(const float *A, const float *B, const int *par, const Img &
 }
 
 int masked_voronoi_dense(const Img &bin, const Img &mask, const Img &dst, int *d_status,
-                         Arena &ws, cudaStream_t st) {
+                         Arena &ws, cudaStream_t st, const Limits &lim) {
     CLE_TRY(same_shape(bin, mask, "binary_source", "mask_image"));
     CLE_TRY(same_shape(bin, dst, "binary_source", "labeling_destination"));
     DenseState *S = ws.take<DenseState>(1);
@@ -176,10 +179,13 @@ int masked_voronoi_dense(const Img &bin, const Img &mask, const Img &dst, int *d
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(DenseState), st));
     Geo g = make_geo(bin);
     int is3d = bin.ndim == 3 ? 1 : 0;
-    uint32_t max_steps = (uint32_t)bin.n() + 16u;
+    uint32_t max_steps = lim.steps_for(bin.n());
+    uint64_t loop_ns = lim.loop_ns, barrier_ns = lim.barrier_ns;
+    const volatile int *cancel = lim.cancel;
     int64_t nn = n;
-    const int grid = coop_grid((const void *)vor_dense_kernel, kVT, 0, n);
-    void *args[] = {&A, &B, &g, &is3d, &nn, &S, &d_status, &par, &max_steps};
+    const int grid = coop_grid((const void *)vor_dense_kernel, kVT, 0, n, lim);
+    void *args[] = {&A, &B, &g, &is3d, &nn, &S, &d_status, &par, &max_steps, &loop_ns, &barrier_ns,
+                    (void *)&cancel};
     CLE_CUDA(cudaLaunchCooperativeKernel((const void *)vor_dense_kernel, dim3(grid), dim3(kVT), args,
                                          0, st));
     count_launches(1);

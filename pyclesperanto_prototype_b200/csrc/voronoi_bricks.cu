@@ -42,8 +42,6 @@ constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
 constexpr size_t kWideBricks = size_t(2) << 20;  // 2 CTAs per SM above this many bricks
 constexpr uint32_t kTraceSteps = 256;
-constexpr uint64_t kBarrierLimitNs = 4000000000ull;
-constexpr uint64_t kKernelLimitNs = 20000000000ull;
 
 struct BState {
     GridBarrier bar;
@@ -154,7 +152,8 @@ __global__ void __launch_bounds__(kBT, MINB)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
-                      uint32_t max_steps, unsigned long long *trace) {
+                      uint32_t max_steps, uint64_t loop_ns, uint64_t barrier_ns,
+                      const volatile int *cancel, unsigned long long *trace) {
     __shared__ uint32_t s_red[kWPB];
     const Geo &g = G.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -176,13 +175,16 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
         ap.maybe_flush(B0, &S->sizes[0]);
     }
     ap.flush(B0, &S->sizes[0]);
-    bool ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
+    bool ok = grid_sync(&S->bar, &S->err, barrier_ns);
 
     const uint64_t t_start = global_ns();
     uint32_t t = 0;
     bool done = false, tail = false;
     while (ok && t < max_steps) {
-        if (gtid == 0 && global_ns() - t_start > kKernelLimitNs) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
+        if (gtid == 0) {
+            if (global_ns() - t_start > loop_ns) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
+            else if (cancel && *cancel) atomicExch(&S->err, (int)CLE_ERR_CANCELLED);
+        }
         const uint32_t *F = (t & 1) ? B1 : B0;
         uint32_t *Fn = (t & 1) ? B0 : B1;
         const uint32_t nB = __ldcg(&S->sizes[t & 3]);
@@ -283,8 +285,8 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
         }
         const uint32_t bs = block_total(changed, s_red);
         if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
-        if (!tail) ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
-        else __syncthreads();
+        if (!tail) ok = grid_sync(&S->bar, &S->err, barrier_ns);
+        else { __syncthreads(); ok = *(volatile int *)&S->err == 0; }
         if (!ok) break;
         const uint32_t nchanged = __ldcg(&S->changes[t & 3]);
         if (trace && gtid == 0 && t < kTraceSteps) {
@@ -331,8 +333,8 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             ap.maybe_flush(Fn, nsize);
         }
         ap.flush(Fn, nsize);
-        if (!tail) ok = grid_sync(&S->bar, &S->err, kBarrierLimitNs);
-        else __syncthreads();
+        if (!tail) ok = grid_sync(&S->bar, &S->err, barrier_ns);
+        else { __syncthreads(); ok = *(volatile int *)&S->err == 0; }
         if (trace && gtid == 0 && t < kTraceSteps) trace[4 * t + 3] = global_ns() - t_start;
         ++t;
     }
@@ -363,7 +365,8 @@ size_t voronoi_frontier_workspace_bytes(const Img &im) {
 }
 
 int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uint32_t *seeds,
-                     const uint32_t *d_seed_count, int *d_status, Arena &ws, cudaStream_t st) {
+                     const uint32_t *d_seed_count, int *d_status, Arena &ws, cudaStream_t st,
+                     const Limits &lim) {
     const size_t nb = brick_count(im);
     BState *S = ws.take<BState>(1);
     uint32_t *B0 = ws.take<uint32_t>(nb);
@@ -381,28 +384,27 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     G.fWB = FastDiv(G.WB);
     G.fHB = FastDiv(G.HB);
     G.is3d = im.ndim == 3 ? 1 : 0;
-    uint32_t max_steps = (uint32_t)im.n() + 16u;   // each step that changes labels >= 1 voxel
+    uint32_t max_steps = lim.steps_for(im.n());   // each step that changes labels >= 1 voxel
+    uint64_t loop_ns = lim.loop_ns, barrier_ns = lim.barrier_ns;
+    const volatile int *cancel = lim.cancel;
     const int wide = nb > kWideBricks ? 1 : 0;
     const void *kerns[2][2] = {
         {(const void *)voronoi_bricks_kernel<false, 1>, (const void *)voronoi_bricks_kernel<false, 2>},
         {(const void *)voronoi_bricks_kernel<true, 1>, (const void *)voronoi_bricks_kernel<true, 2>}};
     const void *kern = kerns[G.is3d][wide];
-    static bool attr[2][2] = {{false, false}, {false, false}};
-    if (!attr[G.is3d][wide]) {
-        CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
-        attr[G.is3d][wide] = true;
-    }
+    // set on every call: the attribute belongs to the current device's context
+    CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
     int dev = 0;
     CLE_CUDA(cudaGetDevice(&dev));
     int per_sm = 0;
     CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, kBBufBytes));
     if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
-    const int grid = (int)std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev));
+    const int grid = (int)std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev, lim));
     unsigned long long *trace =
         (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv, &Pf,
-                    &bstep, &S, &d_status, &max_steps, &trace};
+                    &bstep, &S, &d_status, &max_steps, &loop_ns, &barrier_ns, (void *)&cancel, &trace};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
     count_launches(1);
     return CLE_OK;

@@ -35,8 +35,16 @@ def test_binding_table_matches_header():
     assert sorted(_lib.exported_symbols()) == _header_functions()
 
 
+def test_no_process_wide_setters(lib):
+    """The cooperative-CTA cap and the loop limits are per-call arguments; the
+    header declares no setter that would change them for the whole process."""
+    names = _header_functions()
+    assert "cle_set_cooperative_ctas" not in names
+    assert not [n for n in names if n.startswith("cle_set_")]
+
+
 def test_version(lib):
-    assert lib.cle_abi_version() == 1
+    assert lib.cle_abi_version() == 2
     assert b"sm_100a" in lib.cle_version()
 
 
@@ -88,7 +96,27 @@ def test_argument_validation_errors(lib):
     assert lib.cle_gaussian_blur(ref(a), ref(a), 1.0, 1.0, 0.0, None, 0, None) == 4
     huge = _desc((2048, 1024, 1025), CLE_F32)
     assert lib.cle_voronoi_otsu_labeling_workspace_bytes(ref(huge)) == 0
-    assert lib.cle_voronoi_otsu_labeling(ref(huge), ref(huge), 2.0, 2.0, None, 0, None) == 7
+    assert lib.cle_voronoi_otsu_labeling(ref(huge), ref(huge), 2.0, 2.0, None, None, 0, None) == 7
+
+
+def test_call_options_are_validated_per_call():
+    """Loop limits travel with each call (cle_call_options); malformed options
+    are rejected before anything touches a device."""
+    from pyclesperanto_prototype_b200 import _lib
+    from pyclesperanto_prototype_b200._lib import CLE_F32, ref
+    lib = _lib.load(require_gpu=False)
+    a = _desc((16, 16), CLE_F32)
+    short = _lib.call_options(max_loop_steps=1)
+    short.struct_bytes = 8          # a caller built against a smaller struct
+    assert lib.cle_voronoi_otsu_labeling(ref(a), ref(a), 2.0, 2.0, ref(short), None, 0, None) == 3
+    assert b"struct_bytes" in lib.cle_last_error_message()
+    bad = _lib.call_options(cooperative_ctas=-1)
+    assert lib.cle_masked_voronoi_labeling_binary(ref(a), ref(a), ref(a), ref(bad), None, 0, None) == 3
+    ok = _lib.call_options(max_loop_steps=5, cooperative_ctas=4)
+    assert ctypes.sizeof(ok) == 32 and ok.struct_bytes == 32
+    # with valid options the call goes on to its own checks (no workspace here)
+    assert lib.cle_voronoi_otsu_labeling(ref(a), ref(a), 2.0, 2.0, ref(ok), None, 0, None) == 4
+    assert _lib.ERRORS[8] is RuntimeError
 
 
 def test_status_maps_to_reference_exceptions():

@@ -4,6 +4,7 @@ maps against the oracle's statistics of labels + 1 on seeded label images
 (rtol 1e-5 like every statistics comparison, same NaN / inf positions)."""
 import numpy as np
 import pytest
+import torch
 
 pytestmark = pytest.mark.gpu
 
@@ -146,6 +147,20 @@ def test_euclidean_distance_from_label_centroid_map_matches_oracle(cle, oracle, 
     assert got.dtype == np.float32 and got.shape == ref.shape
     assert np.allclose(got, ref, rtol=RTOL, atol=1e-6)
     assert np.all(got[lab == 0] == 0)
+
+
+@pytest.mark.parametrize("device_int32", [False, True])
+def test_euclidean_distance_negative_labels(cle, oracle, device_int32):
+    """int32 labels below 0: the label read clamps to the point list's column 0,
+    so such a pixel gets its distance to the background's centroid (label-0
+    pixels stay 0) -- the same rule in the kernel and the oracle."""
+    rng = np.random.default_rng(5)
+    lab = rng.integers(-3, 7, (5, 21, 34)).astype(np.int32)
+    arg = cle.B200Array(torch.from_numpy(lab).cuda()) if device_int32 else lab
+    got = cle.pull(cle.euclidean_distance_from_label_centroid_map(arg))
+    ref = oracle.euclidean_distance_from_label_centroid_map(lab)
+    assert np.allclose(got, ref, rtol=RTOL, atol=1e-5)
+    assert np.all(got[lab == 0] == 0) and np.all(got[lab < 0] > 0)
 
 
 def test_centroids_of_labels_point_lists(cle, oracle):
