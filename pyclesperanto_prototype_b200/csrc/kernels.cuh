@@ -56,6 +56,11 @@ size_t label_max_workspace_bytes(const Img &im);
 
 // maxima.cu
 int detect_maxima(const Img &src, const Img &dst, cudaStream_t st);
+// detect_maxima_box(T) & (T > *d_thr32) in one pass over the float32 image T:
+// seg = T > t, lab = key + 1 on seeds (0 elsewhere), seeds listed (count in
+// *d_count, which must start at 0)
+int maxima_seeds(const Img &T, const float *d_thr32, uint8_t *seg, uint32_t *lab, uint32_t *seeds,
+                 uint32_t *d_count, cudaStream_t st);
 
 // ccl.cu
 size_t ccl_workspace_bytes(const Img &im);

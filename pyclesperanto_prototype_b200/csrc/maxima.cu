@@ -90,8 +90,95 @@ maxima_kernel(const Ts *__restrict__ src, Td *__restrict__ dst, int D, int H, in
     }
 }
 
-template <typename Ts, typename Td>
-int launch_maxima(const Img &src, const Img &dst, cudaStream_t st) {
+// voronoi_otsu_labeling's steps 2 and 7 in one pass when both blurs are the
+// same image T (equal sigmas): the maxima flag of detect_maxima_box (as
+// above), then seg = T > t (greater_constant with the float32 threshold) and
+// seed = flag & seg (binary_and), with the seeds' initial CCL keys
+// (x-major pixel index + 1) in the label buffer and the seeds listed -- the
+// spots image is never written or re-read.  Every voxel's seg and label entry
+// is written.
+__global__ void __launch_bounds__(32 * kGroups)
+maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr32, Geo g, int zchunk,
+                    uint8_t *__restrict__ seg, uint32_t *__restrict__ lab, uint32_t *__restrict__ seeds,
+                    uint32_t *__restrict__ d_count) {
+    const int D = (int)g.D, H = (int)g.H, W = (int)g.W;
+    const int lane = threadIdx.x;
+    const int x = (int)blockIdx.x * kOutX + lane - 1;
+    const int y0 = ((int)blockIdx.y * kGroups + threadIdx.y) * kRows;
+    const int z0 = (int)blockIdx.z * zchunk;
+    const int z1 = min(D, z0 + zchunk);
+    if (y0 >= H) return;   // whole warp leaves together (y0 is warp-uniform)
+    const bool xin = (x >= 0 && x < W);
+    const bool own = lane >= 1 && lane <= kOutX && xin;
+    const float NEG = -INFINITY;
+    const float t = *d_thr32;
+
+    auto load = [&](int z, int j) -> float {
+        int y = y0 - 1 + j;
+        if (!xin || z < 0 || z >= D || y < 0 || y >= H) return NEG;
+        return T[((int64_t)z * H + y) * W + x];
+    };
+
+    float vm[kWin], vc[kWin], vp[kWin];
+#pragma unroll
+    for (int j = 0; j < kWin; ++j) {
+        vm[j] = load(z0 - 1, j);
+        vc[j] = load(z0, j);
+    }
+    for (int z = z0; z < z1; ++z) {
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) vp[j] = load(z + 1, j);
+        float Tm[kWin];
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) Tm[j] = fmaxf(fmaxf(vm[j], vc[j]), vp[j]);
+        float S[kRows];
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) S[j] = fmaxf(fmaxf(Tm[j], Tm[j + 1]), Tm[j + 2]);
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) {
+            const float sl = __shfl_up_sync(0xffffffffu, S[j], 1);
+            const float sr = __shfl_down_sync(0xffffffffu, S[j], 1);
+            const int y = y0 + j;
+            const bool mine = own && y < H;
+            bool seed = false;
+            if (mine) {
+                const float v = vc[j + 1];
+                const float A = fmaxf(fmaxf(sl, Tm[j]), vm[j + 1]);
+                const float B = fmaxf(fmaxf(sr, Tm[j + 2]), vp[j + 1]);
+                bool win;
+                if (v != v) {
+                    win = true;
+                } else if (__fsub_rn(v, 1.0f) < v) {
+                    win = (v > A) && (v >= B);
+                } else {
+                    win = (v >= A) && (v >= B);
+                }
+                const bool sg = v > t;
+                seed = sg && win;
+                const int64_t m = ((int64_t)z * H + y) * W + x;
+                seg[m] = sg ? 1 : 0;
+                lab[m] = seed ? xyz2k(g, (uint32_t)x, (uint32_t)y, (uint32_t)z) + 1u : 0u;
+            }
+            const unsigned b = __ballot_sync(0xffffffffu, seed);
+            if (b) {
+                uint32_t base = 0;
+                const int leader = __ffs(b) - 1;
+                if (lane == leader) base = atomicAdd(d_count, (uint32_t)__popc(b));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (seed) seeds[base + __popc(b & ((1u << lane) - 1u))] = (uint32_t)(((int64_t)z * H + y) * W + x);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) {
+            vm[j] = vc[j];
+            vc[j] = vp[j];
+        }
+    }
+}
+
+// Grid of the z-marching kernels: 30 columns per warp, kGroups x kRows rows
+// per block, z chunks so that about 12 blocks per SM are launched.
+int maxima_grid(const Img &src, dim3 &grid, int &zchunk) {
     const int D = (int)src.D, H = (int)src.H, W = (int)src.W;
     const int gx = (W + kOutX - 1) / kOutX;
     const int gy = (H + kRows * kGroups - 1) / (kRows * kGroups);
@@ -101,11 +188,21 @@ int launch_maxima(const Img &src, const Img &dst, cudaStream_t st) {
     int64_t zchunks = (target + (int64_t)gx * gy - 1) / ((int64_t)gx * gy);
     if (zchunks > D) zchunks = D;
     if (zchunks < 1) zchunks = 1;
-    int zchunk = (int)((D + zchunks - 1) / zchunks);
+    zchunk = (int)((D + zchunks - 1) / zchunks);
     if (zchunk < 4 && D >= 4) zchunk = 4;
     zchunks = (D + zchunk - 1) / zchunk;
     if (gy > 65535 || zchunks > 65535) { set_error("detect_maxima: image too large"); return CLE_ERR_TOO_LARGE; }
-    dim3 grid(gx, gy, (unsigned)zchunks), block(32, kGroups);
+    grid = dim3(gx, gy, (unsigned)zchunks);
+    return CLE_OK;
+}
+
+template <typename Ts, typename Td>
+int launch_maxima(const Img &src, const Img &dst, cudaStream_t st) {
+    const int D = (int)src.D, H = (int)src.H, W = (int)src.W;
+    dim3 grid;
+    int zchunk = 1;
+    CLE_TRY(maxima_grid(src, grid, zchunk));
+    dim3 block(32, kGroups);
     maxima_kernel<Ts, Td><<<grid, block, 0, st>>>((const Ts *)src.data, (Td *)dst.data, D, H, W, zchunk);
     CLE_LAUNCH_CHECK("detect_maxima");
     return CLE_OK;
@@ -122,6 +219,18 @@ int maxima_dst(const Img &src, const Img &dst, cudaStream_t st) {
 }
 
 }  // namespace
+
+int maxima_seeds(const Img &T, const float *d_thr32, uint8_t *seg, uint32_t *lab, uint32_t *seeds,
+                 uint32_t *d_count, cudaStream_t st) {
+    if (T.dtype != CLE_F32) { set_error("internal: maxima_seeds needs a float32 image"); return CLE_ERR_DTYPE; }
+    dim3 grid;
+    int zchunk = 1;
+    CLE_TRY(maxima_grid(T, grid, zchunk));
+    maxima_seeds_kernel<<<grid, dim3(32, kGroups), 0, st>>>((const float *)T.data, d_thr32, make_geo(T), zchunk,
+                                                           seg, lab, seeds, d_count);
+    CLE_LAUNCH_CHECK("detect_maxima + seeds");
+    return CLE_OK;
+}
 
 int detect_maxima(const Img &src, const Img &dst, cudaStream_t st) {
     CLE_TRY(same_shape(src, dst, "source", "destination"));

@@ -401,7 +401,9 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     Img Si = src;
     Si.data = l.spots;
     Si.dtype = CLE_U8;
-    CLE_TRY(detect_maxima(Ti, Si, st));
+    // with one blur the maxima are found in the seed pass below (the spots
+    // image is never stored)
+    if (!same_blur) CLE_TRY(detect_maxima(Ti, Si, st));
     stage_mark(2, st);
     // the outline blur also reduces the blurred image's min / max (step 4)
     if (!same_blur) CLE_TRY(blur_minmax(src, l.T, outline_sigma, l.sc->minmax, ws, st));
@@ -417,14 +419,20 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     // 7: segmentation, seeds, seed keys
     uint32_t *lab = (dst.dtype == CLE_U32) ? (uint32_t *)dst.data : (uint32_t *)l.T;
     const Geo g = make_geo(src);
+    const float *Tsrc = l.T;
     if (dst.dtype == CLE_F32) {
-        // T is still needed by the seed kernel; use dst as the blurred copy
+        // the labels are built in T's buffer; the seed pass reads a copy in dst
         CLE_CUDA(cudaMemcpyAsync(dst.data, l.T, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
-        seeds_kernel<<<launch_blocks(n, 256), 256, 0, st>>>((const float *)dst.data, l.spots, &l.sc->thr32, g, n, l.seg, lab, l.seeds, &l.sc->seed_count);
-    } else {
-        seeds_kernel<<<launch_blocks(n, 256), 256, 0, st>>>(l.T, l.spots, &l.sc->thr32, g, n, l.seg, lab, l.seeds, &l.sc->seed_count);
+        Tsrc = (const float *)dst.data;
     }
-    CLE_LAUNCH_CHECK("seeds");
+    if (same_blur) {
+        Img Tc = Ti;
+        Tc.data = (void *)Tsrc;
+        CLE_TRY(maxima_seeds(Tc, &l.sc->thr32, l.seg, lab, l.seeds, &l.sc->seed_count, st));
+    } else {
+        seeds_kernel<<<launch_blocks(n, 256), 256, 0, st>>>(Tsrc, l.spots, &l.sc->thr32, g, n, l.seg, lab, l.seeds, &l.sc->seed_count);
+        CLE_LAUNCH_CHECK("seeds");
+    }
     stage_mark(5, st);
 
     // 8: label the seeds

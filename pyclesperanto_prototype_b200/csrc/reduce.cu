@@ -109,6 +109,22 @@ __device__ __forceinline__ int hist_bin(float v, float mn, float range, float bm
     return b < (uint32_t)bins ? (int)b : -1;
 }
 
+// The same bin with a multiply by the reciprocal of the range: the product
+// differs from the IEEE quotient by under 2 ulp (< 2^-15 for bins <= 256), so
+// wherever q + 0.5 lies at least 2^-8 from an integer the truncation gives
+// the same bin; everything else (near a bin edge, NaN, inf, an empty range)
+// takes the exact division.
+__device__ __forceinline__ int hist_bin_fast(float v, float mn, float range, float rr, float bm1, int bins) {
+    const float a = __fmul_rn(__fsub_rn(v, mn), bm1);
+    const float q = __fadd_rn(__fmul_rn(a, rr), 0.5f);
+    const float d = fabsf(__fsub_rn(q, rintf(q)));
+    if (d >= 0.00390625f && q >= 0.0f && q < 65536.0f) {
+        const uint32_t b = (uint32_t)q;
+        return b < (uint32_t)bins ? (int)b : -1;
+    }
+    return hist_bin(v, mn, range, bm1, bins);
+}
+
 constexpr int kHistThreads = 256;
 
 template <typename T>
@@ -125,6 +141,8 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
     const float mn = d_minmax[0];
     const float range = __fsub_rn(d_minmax[1], mn);
     const float bm1 = (float)(bins - 1);
+    const float rr = __frcp_rn(range);
+    const bool fast = bins <= 256;
     const int64_t y = blockIdx.x;
     const int64_t z0 = (int64_t)blockIdx.y * zchunk;
     const int64_t z1 = min(D, z0 + zchunk);
@@ -145,7 +163,8 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            int b = ok[k] ? hist_bin(v[k], mn, range, bm1, bins) : -1;
+            int b = !ok[k] ? -1 : (fast ? hist_bin_fast(v[k], mn, range, rr, bm1, bins)
+                                         : hist_bin(v[k], mn, range, bm1, bins));
             // warp-aggregated increment: one shared atomic per distinct bin
             unsigned peers = __match_any_sync(0xffffffffu, b);
             if (b >= 0 && (__ffs(peers) - 1) == (int)lane) atomicAdd(&mine[b], (uint32_t)__popc(peers));
