@@ -302,6 +302,30 @@ int cle_voronoi_otsu_labeling(const cle_tensor *src, const cle_tensor *dst, doub
                               double outline_sigma, const cle_call_options *options,
                               void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- batched voronoi_otsu_labeling --------------------------------------
+ * The reference has no batched form: it runs every tile as the host-driven
+ * sequence of _tier9/_voronoi_otsu_labeling.py:57-71.  A plan fixes a set of
+ * tiles (shapes and dtypes u8/u16/f32, one device), the two sigmas and the
+ * loop options; cle_vol_batch_launch then runs voronoi_otsu_labeling on every
+ * tile (labels: uint32 or float32, the tile's shape), spread over the plan's
+ * lanes -- CUDA streams forked from `stream` and joined back into it, so the
+ * batch is stream-ordered on `stream` and the caller may capture it into a
+ * CUDA graph.  lanes = 0 takes the lane count from the library's tuned table
+ * (by mean tile size); with several lanes each lane's growth loop uses its
+ * share of the SMs unless options set cooperative_ctas.  The plan owns host
+ * objects (streams, events), not device memory: the one workspace
+ * (cle_vol_batch_workspace_bytes) and the device status word (int32, receives
+ * the maximum of every tile's loop status; 0 = all finished) come from the
+ * caller.  A plan launches on one stream at a time. */
+typedef struct cle_vol_batch cle_vol_batch;   /* opaque plan */
+int cle_vol_batch_plan(const cle_tensor *tiles, int n_tiles, double spot_sigma, double outline_sigma,
+                       int lanes, const cle_call_options *options, cle_vol_batch **plan);
+size_t cle_vol_batch_workspace_bytes(const cle_vol_batch *plan);
+int cle_vol_batch_lanes(const cle_vol_batch *plan);
+int cle_vol_batch_launch(const cle_vol_batch *plan, const cle_tensor *tiles, const cle_tensor *labels,
+                         void *workspace, size_t workspace_bytes, int32_t *d_status, void *stream);
+void cle_vol_batch_free(cle_vol_batch *plan);
+
 /* Device pointer to the label count (= maximum label) written by the last
  * voronoi_otsu_labeling / masked_voronoi_labeling_binary call that used this
  * workspace; for stream-ordered consumers such as

@@ -133,6 +133,12 @@ _SIGS = {
     "cle_masked_voronoi_labeling_binary": (ctypes.c_int, [_T, _T, _T, _O, _P, _SZ, _P]),
     "cle_voronoi_otsu_labeling_workspace_bytes": (_SZ, [_T]),
     "cle_voronoi_otsu_labeling": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, _O, _P, _SZ, _P]),
+    "cle_vol_batch_plan": (ctypes.c_int, [_T, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _O,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "cle_vol_batch_workspace_bytes": (_SZ, [_P]),
+    "cle_vol_batch_lanes": (ctypes.c_int, [_P]),
+    "cle_vol_batch_launch": (ctypes.c_int, [_P, _T, _T, _P, _SZ, _P, _P]),
+    "cle_vol_batch_free": (None, [_P]),
     "cle_workspace_status": (ctypes.c_int, [_P, _SZ, _P]),
     "cle_workspace_label_count": (_P, [_P]),
     "cle_statistics_of_labelled_pixels_device_count": (ctypes.c_int, [_T, _T, _P, ctypes.c_int64, _P, _P, _SZ, _P]),

@@ -1,17 +1,21 @@
 """Batched form: many independent volumes through voronoi_otsu_labeling as one
 CUDA graph.
 
-Tiles of any mix of 2D / 3D shapes are spread over K lanes (CUDA streams) by
-a longest-first greedy schedule on voxel count; tiles in a lane run one after
-another on that lane's workspace (sized for its largest tile, reused), lanes
-run concurrently.  The whole batch is captured into one CUDA graph after one
-uncaptured warm-up run, so a batch is a single graph launch with no host
-work per tile.  While several lanes run, each cooperative launch of the
-growth loop is capped at SMs / K CTAs so the concurrent grids always fit on
-the GPU together.  Results are the same labels as the per-call path, tile by
-tile (tests/test_batch_serve_gpu.py).
+The plan and launch live in the C ABI (cle_vol_batch_plan /
+cle_vol_batch_launch): tiles of any mix of 2D / 3D shapes are spread over K
+lanes (CUDA streams forked from the caller's stream) by a longest-first
+greedy schedule on voxel count; tiles in a lane run one after another on that
+lane's workspace slice (sized for its largest tile), lanes run concurrently,
+and K comes from the library's tuned table unless given.  The whole batch is
+captured into one CUDA graph after one uncaptured warm-up run, so a batch is
+a single graph launch with no host work per tile.  While several lanes run,
+each cooperative launch of the growth loop is capped at SMs / K CTAs so the
+concurrent grids always fit on the GPU together.  Results are the same labels
+as the per-call path, tile by tile (tests/test_batch_serve_gpu.py).
 """
 from __future__ import annotations
+
+import ctypes
 
 import numpy as np
 import torch
@@ -71,16 +75,18 @@ def schedule(voxels, lanes: int):
 
 
 class VolBatch:
-    """voronoi_otsu_labeling over a fixed set of device volumes, replayed as
-    one CUDA graph.
+    """voronoi_otsu_labeling over a fixed set of device volumes through the C
+    ABI's batched form (cle_vol_batch_plan / cle_vol_batch_launch), replayed
+    as one CUDA graph.
 
-        batch = VolBatch(inputs, spot_sigma=3.5, outline_sigma=1.0, lanes=8)
+        batch = VolBatch(inputs, spot_sigma=3.5, outline_sigma=1.0)
         batch.run()                 # labels in batch.outputs[i]
-    """
+
+    lanes = 0 takes the lane count from the library's tuned table."""
 
     def __init__(self, inputs, spot_sigma: float = 2.0, outline_sigma: float = 2.0,
-                 lanes: int = 8, use_graph: bool = True, max_loop_steps: int = 0):
-        _lib.load()
+                 lanes: int = 0, use_graph: bool = True, max_loop_steps: int = 0, cooperative_ctas: int = 0):
+        lib = _lib.load()
         self.inputs = [x.tensor if isinstance(x, B200Array) else x for x in inputs]
         for t in self.inputs:
             if not t.is_cuda or not t.is_contiguous():
@@ -88,41 +94,33 @@ class VolBatch:
         self.spot, self.outline = float(spot_sigma), float(outline_sigma)
         self.device = self.inputs[0].device
         self.outputs = [torch.empty(t.shape, dtype=torch.uint32, device=self.device) for t in self.inputs]
-        vox = [t.numel() for t in self.inputs]
-        self.lanes = max(1, min(int(lanes), len(self.inputs)))
-        self.plan = [p for p in schedule(vox, self.lanes) if p]
-        self.lanes = len(self.plan)
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in self.plan]
-        self.ws = []
-        for p in self.plan:
-            need = max(vol_workspace_bytes(tuple(self.inputs[i].shape), self.inputs[i].dtype) for i in p)
-            self.ws.append(torch.empty(need, dtype=torch.uint8, device=self.device))
-        # per-lane sticky status: max over every call's status word (offset 0
-        # of its workspace), so a limit hit by any tile is reported
-        self.status = torch.zeros(len(self.plan), dtype=torch.int32, device=self.device)
+        n = len(self.inputs)
+        self._in = (_lib.CleTensor * n)(*[_desc(t) for t in self.inputs])
+        self._out = (_lib.CleTensor * n)(*[_desc(t) for t in self.outputs])
+        self.options = _lib.call_options(max_loop_steps=max_loop_steps, cooperative_ctas=cooperative_ctas)
+        self._plan = ctypes.c_void_p()
+        _lib.check(lib.cle_vol_batch_plan(self._in, n, self.spot, self.outline, int(lanes),
+                                          _lib.ref(self.options), ctypes.byref(self._plan)), "vol_batch_plan")
+        self.lanes = int(lib.cle_vol_batch_lanes(self._plan))
+        self.ws = torch.empty(max(1, int(lib.cle_vol_batch_workspace_bytes(self._plan))), dtype=torch.uint8,
+                              device=self.device)
+        # the maximum of every tile's loop status, written on the device
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.graph = None
         self.use_graph = use_graph
         self.launches_per_run = 0     # library kernels one run launches
-        # while several lanes run, each lane's cooperative growth launch is
-        # capped at its share of the SMs (passed with every call)
-        coop = max(1, torch.cuda.get_device_properties(self.device).multi_processor_count // self.lanes)
-        self.options = _lib.call_options(max_loop_steps=max_loop_steps,
-                                         cooperative_ctas=coop if self.lanes > 1 else 0)
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value and _lib._lib is not None:
+            _lib._lib.cle_vol_batch_free(plan)
+            self._plan = None
 
     def _issue(self):
-        main = torch.cuda.current_stream(self.device)
-        self.status.zero_()
-        for s in self.streams:
-            s.wait_stream(main)
-        for k, (p, s, ws) in enumerate(zip(self.plan, self.streams, self.ws)):
-            with torch.cuda.stream(s):
-                word = ws[:4].view(torch.int32)
-                for i in p:
-                    vol_into(self.inputs[i], self.outputs[i], ws, self.spot, self.outline, s.cuda_stream,
-                             self.options)
-                    torch.maximum(self.status[k:k + 1], word, out=self.status[k:k + 1])
-        for s in self.streams:
-            main.wait_stream(s)
+        lib = _lib.load()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(lib.cle_vol_batch_launch(self._plan, self._in, self._out, self.ws.data_ptr(), self.ws.numel(),
+                                            self.status.data_ptr(), stream), "vol_batch_launch")
 
     def capture(self):
         lib = _lib.load()

@@ -143,3 +143,20 @@ def test_no_cpu_fallback_without_gpu():
     import pyclesperanto_prototype_b200 as cle
     with pytest.raises(RuntimeError):
         cle.voronoi_otsu_labeling(np.zeros((8, 8), np.float32))
+
+
+def test_batch_plan_validates_before_device_use():
+    """The batched form's plan rejects bad arguments on the host."""
+    from pyclesperanto_prototype_b200 import _lib
+    from pyclesperanto_prototype_b200._lib import CLE_F32, CLE_U32
+    lib = _lib.load(require_gpu=False)
+    plan = ctypes.c_void_p()
+    tiles = (_lib.CleTensor * 2)(_desc((16, 16), CLE_F32), _desc((8, 16, 16), CLE_U32))
+    assert lib.cle_vol_batch_plan(tiles, 0, 2.0, 2.0, 0, None, ctypes.byref(plan)) == 3
+    assert lib.cle_vol_batch_plan(tiles, 1, 2.0, 2.0, 65, None, ctypes.byref(plan)) == 3
+    assert lib.cle_vol_batch_plan(tiles, 2, 2.0, 2.0, 0, None, ctypes.byref(plan)) == 1   # uint32 tile
+    assert b"tiles[1]" in lib.cle_last_error_message()
+    assert not plan.value
+    assert lib.cle_vol_batch_launch(None, tiles, tiles, None, 0, None, None) == 3
+    assert lib.cle_vol_batch_workspace_bytes(None) == 0 and lib.cle_vol_batch_lanes(None) == 0
+    lib.cle_vol_batch_free(None)

@@ -72,3 +72,23 @@ def test_served_budget_limits_concurrency(cle):
     order = sorted(reqs, key=lambda r: r.admitted)
     for a, b in zip(order, order[1:]):
         assert b.admitted >= a.done - 1e-3
+
+
+def test_batch_plan_tuned_lanes_and_shape_check(cle):
+    """lanes = 0 takes the lane count from the library's tuned table; a launch
+    with tiles of other shapes than planned is refused before any work."""
+    import ctypes
+    from pyclesperanto_prototype_b200 import _lib
+    from pyclesperanto_prototype_b200.batch import VolBatch
+    tiles = _tiles()[:6]
+    b = VolBatch(tiles, spot_sigma=3.5, outline_sigma=1.0, lanes=0, use_graph=False)
+    assert 1 <= b.lanes <= len(tiles)
+    b.run()
+    b.check()
+    for t, out in zip(tiles, b.outputs):
+        assert torch.equal(out, cle.voronoi_otsu_labeling(t, spot_sigma=3.5, outline_sigma=1.0).tensor)
+    lib = _lib.load()
+    wrong = (_lib.CleTensor * len(tiles))(*[_lib.tensor_desc(t) for t in reversed(tiles)])
+    st = lib.cle_vol_batch_launch(b._plan, wrong, b._out, b.ws.data_ptr(), b.ws.numel(), b.status.data_ptr(),
+                                  torch.cuda.current_stream().cuda_stream)
+    assert st == 2 and b"planned" in lib.cle_last_error_message()
