@@ -275,8 +275,22 @@ class Backend:
 
 
 class B200Backend:
-    """Backend object with the reference's backend interface
-    (_tier0/_opencl_backend.py:10-44)."""
+    """A backend with the reference's backend interface
+    (_tier0/_opencl_backend.py:10-44, installed the way _tier0/_device.py:62-71
+    installs the cupy backend: ``Backend.get_instance().set(B200Backend(...))``).
+
+    Its arrays are B200Array (torch CUDA tensors): once installed in the
+    reference, the reference's push / create / create_like return device
+    arrays of this package, which the cle.* functions of this package take and
+    return without a host round trip.  Kernels outside this package's path
+    arrive at execute(); they are handed to `fallback` (another backend, e.g.
+    the reference's OpenCL backend): every B200Array argument is copied into
+    the fallback's arrays, the kernel runs there, and the arrays are copied
+    back, so only those kernels pay a host round trip.  Without a fallback
+    execute raises NotImplementedError."""
+
+    def __init__(self, fallback=None):
+        self.fallback = fallback
 
     def array_type(self):
         return B200Array
@@ -293,5 +307,24 @@ class B200Backend:
     def empty_image_like(self, array):
         return create_like(array)
 
-    def execute(self, *args, **kwargs):
-        raise NotImplementedError("OpenCL kernel sources are not executed by the B200 backend")
+    def execute(self, anchor, opencl_kernel_filename, kernel_name, global_size, parameters, prog=None,
+                constants=None, image_size_independent_kernel_compilation=None, device=None):
+        if self.fallback is None:
+            raise NotImplementedError(
+                f"{kernel_name}: this kernel is outside the B200 path; construct B200Backend(fallback=...) "
+                "with the backend that runs it")
+        mine = {k: v for k, v in parameters.items() if isinstance(v, B200Array)}
+        theirs = dict(parameters)
+        for k, v in mine.items():
+            theirs[k] = self.fallback.from_array(v.get())
+        result = self.fallback.execute(anchor, opencl_kernel_filename, kernel_name, global_size, theirs,
+                                       prog=prog, constants=constants,
+                                       image_size_independent_kernel_compilation=image_size_independent_kernel_compilation,
+                                       device=device)
+        for k, v in mine.items():
+            host = np.asarray(self.fallback.asarray(theirs[k]))
+            v.tensor.copy_(torch.from_numpy(np.ascontiguousarray(host.astype(v.dtype, copy=False))).to(v.tensor.device))
+        return result
+
+    def __str__(self):
+        return "B200 backend (sm_100a kernels of pyclesperanto_prototype_b200)"

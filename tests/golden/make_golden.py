@@ -1,9 +1,9 @@
 """Regenerates the committed golden fixtures in this folder.
 
-Run in a container where the reference checkout is mounted (default path
-below, override with CLE_REFERENCE_ROOT):
+Run where a checkout of the reference is available, naming its root in
+CLE_REFERENCE_ROOT (the directory holding data/ and demo/):
 
-    python tests/golden/make_golden.py
+    CLE_REFERENCE_ROOT=/path/to/pyclesperanto_prototype python tests/golden/make_golden.py
 
 Outputs:
   blobs.npz           -- data/blobs.tif of the reference (254x256 uint8), read
@@ -21,7 +21,7 @@ import re
 import numpy as np
 from PIL import Image
 
-REF = os.environ.get("CLE_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("CLE_REFERENCE_ROOT")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -54,6 +54,8 @@ def corners(text):
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "data")):
+        raise SystemExit("set CLE_REFERENCE_ROOT to the reference checkout (the directory with data/ and demo/)")
     img = np.asarray(Image.open(os.path.join(REF, "data", "blobs.tif")))
     np.savez_compressed(os.path.join(HERE, "blobs.npz"), blobs=img)
 

@@ -208,3 +208,52 @@ def test_top_hat_box_narrow_input_and_in_place(cle, oracle, dtype):
     f = cle.push(a.astype(np.float32))
     cle.top_hat_box(f, f, 5, 5, 2)              # destination = source
     assert np.array_equal(cle.pull(f), oracle.top_hat_box(a.astype(np.float32), 5, 5, 2))
+
+
+def test_backend_installs_and_delegates(cle):
+    """B200Backend as the reference's backend: push / create give device arrays
+    the cle.* functions take directly; a kernel outside the path goes to the
+    fallback backend and its outputs come back into the device arrays."""
+    import numpy as np
+
+    class NumpyArray:
+        def __init__(self, a):
+            self.a = np.array(a)
+
+        def get(self):
+            return self.a
+
+    class FakeFallback:
+        """Stands in for the reference's OpenCL backend: runs one kernel in numpy."""
+        calls = []
+
+        def from_array(self, a):
+            return NumpyArray(a)
+
+        def asarray(self, a):
+            return a.a
+
+        def execute(self, anchor, filename, kernel_name, global_size, parameters, **kw):
+            self.calls.append(kernel_name)
+            assert kernel_name == "add_image_and_scalar"
+            parameters["dst"].a[...] = parameters["src"].a + parameters["scalar"]
+
+    be = cle.B200Backend(fallback=FakeFallback())
+    backend = cle.Backend.get_instance()
+    old = backend.get()
+    backend.set(be)
+    try:
+        assert backend.get().array_type() is cle.B200Array
+        src = be.from_array(np.arange(12, dtype=np.float32).reshape(3, 4))
+        dst = be.empty_image_like(src)
+        be.execute(None, "add_image_and_scalar_x.cl", "add_image_and_scalar", dst.shape,
+                   {"src": src, "dst": dst, "scalar": 2.0})
+        assert np.array_equal(cle.pull(dst), np.arange(12, dtype=np.float32).reshape(3, 4) + 2)
+        # hot-path functions take the backend's arrays without a host copy
+        lab = cle.voronoi_otsu_labeling(be.from_array(np.pad(np.ones((5, 5), np.float32), 4)), spot_sigma=1,
+                                        outline_sigma=1)
+        assert isinstance(lab, cle.B200Array) and cle.pull(lab).max() == 1
+        with pytest.raises(NotImplementedError):
+            cle.B200Backend().execute(None, "x.cl", "x", (1,), {})
+    finally:
+        backend.set(old)
