@@ -166,257 +166,88 @@ __device__ __forceinline__ Seg make_seg(uint32_t l) {
     return s;
 }
 
-// Tiles: a CTA aggregates a tile of kTXC x-chunks (32 voxels each) by kTY
-// rows by kTZ planes in a shared-memory table keyed by label, then adds each
-// label's totals to the global accumulators once per tile.  A label spans a
-// handful of tiles, so the global atomics fall from one set per row run to
-// one set per (label, tile).  A full table sends a run straight to the
-// global accumulators (same result, more atomics).
-constexpr int kTXC = 4;                       // x chunks of 32 voxels per tile (128 x)
-constexpr int kTY = 16;                       // rows per tile
-constexpr int kTZ = 4;                        // planes per tile
-constexpr int kTasks = kTXC * kTY * kTZ;      // row segments per tile (256)
-constexpr int kTabBits = 7;
-constexpr int kTab = 1 << kTabBits;           // table entries per CTA
-static_assert(kTasks % (kST / 32 * kBatch) == 0, "tile tasks split evenly over warps and batches");
-
-struct TileGeo {
-    uint32_t chunks, tiles_x, tiles_y, tiles_z, ntiles;
-    FastDiv f_tx, f_ty;
-};
-
-TileGeo make_tile_geo(const Img &im) {
-    TileGeo t;
-    t.chunks = (uint32_t)((im.W + 31) / 32);
-    t.tiles_x = (t.chunks + kTXC - 1) / kTXC;
-    t.tiles_y = (uint32_t)((im.H + kTY - 1) / kTY);
-    t.tiles_z = (uint32_t)((im.D + kTZ - 1) / kTZ);
-    t.ntiles = t.tiles_x * t.tiles_y * t.tiles_z;
-    t.f_tx = FastDiv(t.tiles_x);
-    t.f_ty = FastDiv(t.tiles_y);
-    return t;
-}
-
-// Slot of label l (>= 1) in a CTA table of kTab keys (0 = free), inserting it
-// if absent; -1 when the table is full.
-__device__ __forceinline__ int tab_slot(uint32_t *key, uint32_t l) {
-    volatile uint32_t *vk = key;
-    const uint32_t h = (l * 2654435761u) >> (32 - kTabBits);
-    for (int p = 0; p < kTab; ++p) {
-        const uint32_t s = (h + (uint32_t)p) & (kTab - 1);
-        uint32_t k = vk[s];
-        if (k == 0u) {
-            const uint32_t old = atomicCAS(key + s, 0u, l);
-            if (old == 0u || old == l) return (int)s;
-            k = old;
-        }
-        if (k == l) return (int)s;
-    }
-    return -1;
-}
-
-// Per-CTA accumulators of pass 1 (structure of arrays in shared memory).
-// Intensity sums are exact 64-bit integers for 8/16-bit intensities and
-// float64 otherwise (stored in the same 64-bit words).
-struct Tab1 {
-    uint32_t key[kTab], cnt[kTab];
-    unsigned long long sx[kTab], sy[kTab], sz[kTab];
-    unsigned long long sv[kTab], svx[kTab], svy[kTab], svz[kTab];
-    int vmin[kTab], vmax[kTab];
-    uint32_t xmin[kTab], xmax[kTab], ymin[kTab], ymax[kTab], zmin[kTab], zmax[kTab];
-};
-
-__device__ __forceinline__ void tab1_reset(Tab1 &T, int i) {
-    T.key[i] = 0u;
-    T.cnt[i] = 0u;
-    T.sx[i] = T.sy[i] = T.sz[i] = 0ull;
-    T.sv[i] = T.svx[i] = T.svy[i] = T.svz[i] = 0ull;
-    T.vmin[i] = 0x7FFFFFFF;
-    T.vmax[i] = (int)0x80000000;
-    T.xmin[i] = T.ymin[i] = T.zmin[i] = 0xFFFFFFFFu;
-    T.xmax[i] = T.ymax[i] = T.zmax[i] = 0u;
-}
-
-// One run's contribution: to the CTA table, or to the global accumulators
-// when the table is full.
-template <bool INT>
-__device__ __forceinline__ void add_run1(Tab1 &T, const Acc1 &a, uint32_t l, uint32_t cnt,
-                                         unsigned long long sx, uint32_t y, uint32_t z,
-                                         unsigned long long iv, unsigned long long ivx, double dv, double dvx,
-                                         int vmin, int vmax, uint32_t xh, uint32_t xt) {
-    const int s = tab_slot(T.key, l);
-    if (s >= 0) {
-        atomicAdd(T.cnt + s, cnt);
-        atomicAdd(T.sx + s, sx);
-        atomicAdd(T.sy + s, (unsigned long long)y * cnt);
-        atomicAdd(T.sz + s, (unsigned long long)z * cnt);
-        if constexpr (INT) {
-            atomicAdd(T.sv + s, iv);
-            atomicAdd(T.svx + s, ivx);
-            atomicAdd(T.svy + s, iv * (unsigned long long)y);
-            atomicAdd(T.svz + s, iv * (unsigned long long)z);
-        } else {
-            atomicAdd(reinterpret_cast<double *>(T.sv + s), dv);
-            atomicAdd(reinterpret_cast<double *>(T.svx + s), dvx);
-            atomicAdd(reinterpret_cast<double *>(T.svy + s), dv * (double)y);
-            atomicAdd(reinterpret_cast<double *>(T.svz + s), dv * (double)z);
-        }
-        atomicMin(T.vmin + s, vmin);
-        atomicMax(T.vmax + s, vmax);
-        atomicMin(T.xmin + s, xh);
-        atomicMax(T.xmax + s, xt);
-        atomicMin(T.ymin + s, y);
-        atomicMax(T.ymax + s, y);
-        atomicMin(T.zmin + s, z);
-        atomicMax(T.zmax + s, z);
-        return;
-    }
-    const uint32_t i = l - 1;
-    atomicAdd(a.cnt + i, cnt);
-    atomicAdd(a.sx + i, sx);
-    atomicAdd(a.sy + i, (unsigned long long)y * cnt);
-    atomicAdd(a.sz + i, (unsigned long long)z * cnt);
-    if constexpr (INT) {
-        atomicAdd(a.sv + i, (double)iv);
-        atomicAdd(a.svx + i, (double)ivx);
-        atomicAdd(a.svy + i, (double)(iv * (unsigned long long)y));
-        atomicAdd(a.svz + i, (double)(iv * (unsigned long long)z));
-    } else {
-        atomicAdd(a.sv + i, dv);
-        atomicAdd(a.svx + i, dvx);
-        atomicAdd(a.svy + i, dv * (double)y);
-        atomicAdd(a.svz + i, dv * (double)z);
-    }
-    atomicMin(a.vmin + i, vmin);
-    atomicMax(a.vmax + i, vmax);
-    atomicMin(a.xmin + i, xh);
-    atomicMax(a.xmax + i, xt);
-    atomicMin(a.ymin + i, y);
-    atomicMax(a.ymax + i, y);
-    atomicMin(a.zmin + i, z);
-    atomicMax(a.zmax + i, z);
-}
-
-// Adds every used table entry to the global accumulators and clears it.
-template <bool INT>
-__device__ __forceinline__ void flush1(Tab1 &T, const Acc1 &a) {
-    for (int s = threadIdx.x; s < kTab; s += blockDim.x) {
-        const uint32_t l = T.key[s];
-        if (l) {
-            const uint32_t i = l - 1;
-            atomicAdd(a.cnt + i, T.cnt[s]);
-            atomicAdd(a.sx + i, T.sx[s]);
-            atomicAdd(a.sy + i, T.sy[s]);
-            atomicAdd(a.sz + i, T.sz[s]);
-            if constexpr (INT) {
-                // exact: per-label totals stay far below 2^53
-                atomicAdd(a.sv + i, (double)T.sv[s]);
-                atomicAdd(a.svx + i, (double)T.svx[s]);
-                atomicAdd(a.svy + i, (double)T.svy[s]);
-                atomicAdd(a.svz + i, (double)T.svz[s]);
-            } else {
-                atomicAdd(a.sv + i, __longlong_as_double((long long)T.sv[s]));
-                atomicAdd(a.svx + i, __longlong_as_double((long long)T.svx[s]));
-                atomicAdd(a.svy + i, __longlong_as_double((long long)T.svy[s]));
-                atomicAdd(a.svz + i, __longlong_as_double((long long)T.svz[s]));
-            }
-            atomicMin(a.vmin + i, T.vmin[s]);
-            atomicMax(a.vmax + i, T.vmax[s]);
-            atomicMin(a.xmin + i, T.xmin[s]);
-            atomicMax(a.xmax + i, T.xmax[s]);
-            atomicMin(a.ymin + i, T.ymin[s]);
-            atomicMax(a.ymax + i, T.ymax[s]);
-            atomicMin(a.zmin + i, T.zmin[s]);
-            atomicMax(a.zmax + i, T.zmax[s]);
-        }
-        tab1_reset(T, s);
-    }
-}
-
-// Row segment j of a tile -> (row index z*H + y, chunk) or false when outside.
-__device__ __forceinline__ bool tile_task(const TileGeo &G, uint32_t tile, int j, int64_t D, int64_t H,
-                                          uint32_t &row, uint32_t &c, uint32_t &y, uint32_t &z) {
-    const uint32_t r = G.f_tx.div(tile), tx = tile - r * G.tiles_x;
-    const uint32_t tz = G.f_ty.div(r), ty = r - tz * G.tiles_y;
-    c = tx * kTXC + (uint32_t)(j % kTXC);
-    y = ty * kTY + (uint32_t)((j / kTXC) % kTY);
-    z = tz * kTZ + (uint32_t)(j / (kTXC * kTY));
-    row = z * (uint32_t)H + y;
-    return c < G.chunks && (int64_t)y < H && (int64_t)z < D;
-}
-
-// 4 CTAs per SM (64 registers); the table takes 12 KB of shared memory per CTA
+// 4 CTAs per SM (64 registers): more loads in flight for the latency-bound scan
 template <typename TL, typename TI>
 __global__ void __launch_bounds__(kST, 4)
 stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t Lcap, Acc1 a, TileGeo G, const uint32_t *__restrict__ d_L) {
-    constexpr bool INT = sizeof(TI) <= 2 && !std::is_floating_point<TI>::value;
-    __shared__ Tab1 T;
+            int64_t W, int64_t Lcap, Acc1 a, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
     const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int kWarps = kST / 32;
-    for (int s = threadIdx.x; s < kTab; s += blockDim.x) tab1_reset(T, s);
-    __syncthreads();
-    for (uint32_t tile = blockIdx.x; tile < G.ntiles; tile += gridDim.x) {
-        // kBatch row segments per round: every load is issued before its use
-        for (int j0 = warp; j0 < kTasks; j0 += kBatch * kWarps) {
-            uint32_t lb[kBatch];
-            float vb[kBatch];
+    const int lane = threadIdx.x & 31;
+    const uint32_t chunks = (uint32_t)((W + 31) / 32);
+    const uint32_t tasks = (uint32_t)(D * H) * chunks;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    // kBatch row segments per round: every load is issued before its use
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch];
+        float vb[kBatch];
 #pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                uint32_t row, c, y, z;
-                const bool in = tile_task(G, tile, j0 + k * kWarps, D, H, row, c, y, z);
-                const int64_t x = (int64_t)c * 32 + lane;
-                const uint32_t l = (in && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
-                lb[k] = (l > (uint32_t)L) ? 0u : l;
-            }
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                uint32_t row, c, y, z;
-                tile_task(G, tile, j0 + k * kWarps, D, H, row, c, y, z);
-                const int64_t x = (int64_t)c * 32 + lane;
-                vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
-            }
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                const uint32_t l = lb[k];
-                if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
-                uint32_t row, c, y, z;
-                tile_task(G, tile, j0 + k * kWarps, D, H, row, c, y, z);
-                const int64_t x = (int64_t)c * 32 + lane;
-                const float v = vb[k];
-                const Seg s = make_seg(l);
-                unsigned long long iv = 0, ivx = 0;
-                double dv = 0.0, dvx = 0.0;
-                float smin, smax;
-                if constexpr (INT) {
-                    // exact uint32 scans of v and v * lane (at most 32 * 65535 * 31 < 2^32),
-                    // x = 32 c + lane
-                    const uint32_t u = (uint32_t)v;
-                    const uint32_t su = s.scan_addu(u);
-                    const uint32_t sl = s.scan_addu(u * (uint32_t)lane);
-                    iv = su;
-                    ivx = (unsigned long long)su * (c * 32u) + sl;
-                    smin = (float)s.scan_minu(u);
-                    smax = (float)s.scan_maxu(u);
-                } else {
-                    const double d = (double)v;
-                    dv = s.scan_add(d);
-                    dvx = s.scan_add(d * (double)x);
-                    smin = s.scan_min(l ? v : INFINITY);
-                    smax = s.scan_max(l ? v : -INFINITY);
-                }
-                if (s.tail && l) {
-                    const uint32_t cnt = (uint32_t)(s.lane - s.hl + 1);
-                    const uint32_t xh = (uint32_t)(c * 32 + s.hl), xt = (uint32_t)x;
-                    add_run1<INT>(T, a, l, cnt, (unsigned long long)(xh + xt) * cnt / 2ull, y, z, iv, ivx, dv,
-                                  dvx, f2ord(smin), f2ord(smax), xh, xt);
-                }
-            }
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            const uint32_t l = (t < tasks && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
+            lb[k] = (l > (uint32_t)L) ? 0u : l;
         }
-        __syncthreads();
-        flush1<INT>(T, a);
-        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+        const uint32_t l = lb[k];
+        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+        const uint32_t t = t0 + k * nwarps;
+        const uint32_t row = fc.div(t);
+        const uint32_t c = t - row * chunks;
+        const int64_t x = (int64_t)c * 32 + lane;
+        const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
+        const float v = vb[k];
+        const Seg s = make_seg(l);
+        double ssum, ssx;
+        float smin, smax;
+        if constexpr (sizeof(TI) <= 2) {
+            // 8/16-bit intensities: exact uint32 scans of v and v * lane
+            // (at most 32 * 65535 * 31 < 2^32), x = 32 c + lane
+            const uint32_t iv = (uint32_t)v;
+            const uint32_t su = s.scan_addu(iv);
+            const uint32_t sl = s.scan_addu(iv * (uint32_t)lane);
+            ssum = (double)su;
+            ssx = (double)su * (double)(c * 32u) + (double)sl;
+            smin = (float)s.scan_minu(iv);
+            smax = (float)s.scan_maxu(iv);
+        } else {
+            const double dv = (double)v;
+            ssum = s.scan_add(dv);
+            ssx = s.scan_add(dv * (double)x);
+            smin = s.scan_min(l ? v : INFINITY);
+            smax = s.scan_max(l ? v : -INFINITY);
+        }
+        if (s.tail && l) {
+            const uint32_t i = l - 1;
+            const uint32_t cnt = (uint32_t)(s.lane - s.hl + 1);
+            const uint32_t xh = (uint32_t)(c * 32 + s.hl), xt = (uint32_t)x;
+            atomicAdd(a.cnt + i, cnt);
+            atomicAdd(a.sx + i, (unsigned long long)(xh + xt) * cnt / 2ull);
+            atomicAdd(a.sy + i, (unsigned long long)y * cnt);
+            atomicAdd(a.sz + i, (unsigned long long)z * cnt);
+            atomicAdd(a.sv + i, ssum);
+            atomicAdd(a.svx + i, ssx);
+            atomicAdd(a.svy + i, ssum * (double)y);
+            atomicAdd(a.svz + i, ssum * (double)z);
+            atomicMin(a.vmin + i, f2ord(smin));
+            atomicMax(a.vmax + i, f2ord(smax));
+            atomicMin(a.xmin + i, xh);
+            atomicMax(a.xmax + i, xt);
+            atomicMin(a.ymin + i, (uint32_t)y);
+            atomicMax(a.ymax + i, (uint32_t)y);
+            atomicMin(a.zmin + i, (uint32_t)z);
+            atomicMax(a.zmax + i, (uint32_t)z);
+        }
+        }
     }
 }
 
@@ -467,115 +298,75 @@ __global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T) {
     }
 }
 
-// Per-CTA accumulators of pass 2: distance sums and squared deviations in
-// float64, maxima as the bit patterns of non-negative float32 distances.
-struct Tab2 {
-    uint32_t key[kTab];
-    double sdc[kTab], sdm[kTab], ssq[kTab];
-    uint32_t mdc[kTab], mdm[kTab];
-};
-
-__device__ __forceinline__ void tab2_reset(Tab2 &T, int i) {
-    T.key[i] = 0u;
-    T.sdc[i] = T.sdm[i] = T.ssq[i] = 0.0;
-    T.mdc[i] = T.mdm[i] = 0u;
-}
-
-__device__ __forceinline__ void flush2(Tab2 &T, const Acc2 &b) {
-    for (int s = threadIdx.x; s < kTab; s += blockDim.x) {
-        const uint32_t l = T.key[s];
+template <typename TL, typename TI>
+__global__ void __launch_bounds__(kST)
+stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
+            int64_t W, int64_t Lcap, Acc2 b, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
+    const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
+    const int lane = threadIdx.x & 31;
+    const uint32_t chunks = (uint32_t)((W + 31) / 32);
+    const uint32_t tasks = (uint32_t)(D * H) * chunks;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    // kBatch row segments per round: every load is issued before its use
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch];
+        float vb[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            const uint32_t l = (t < tasks && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
+            lb[k] = (l > (uint32_t)L) ? 0u : l;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + k * nwarps;
+            const uint32_t row = fc.div(t);
+            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
+            vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+        const uint32_t l = lb[k];
+        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+        const uint32_t t = t0 + k * nwarps;
+        const uint32_t row = fc.div(t);
+        const uint32_t c = t - row * chunks;
+        const int64_t x = (int64_t)c * 32 + lane;
+        const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
+        // distances in float32 (relative error a few 1e-7), their sums and the
+        // squared deviations in float64; the squared deviations are divided
+        // by the area once per label
+        float dc = 0.0f, dm = 0.0f;
+        double sq = 0.0;
         if (l) {
             const uint32_t i = l - 1;
-            atomicAdd(b.sdc + i, T.sdc[s]);
-            atomicAdd(b.sdm + i, T.sdm[s]);
-            atomicAdd(b.ssq + i, T.ssq[s]);
-            atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong((double)__uint_as_float(T.mdc[s])));
-            atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong((double)__uint_as_float(T.mdm[s])));
+            const float4 pc = b.pc[i], pm = b.pm[i];
+            const float xf = (float)x, yf = (float)y, zf = (float)z;
+            const float ex = xf - pc.x, ey = yf - pc.y, ez = zf - pc.z;
+            const float fx = xf - pm.x, fy = yf - pm.y, fz = zf - pm.z;
+            dc = sqrtf(ex * ex + ey * ey + ez * ez);
+            dm = sqrtf(fx * fx + fy * fy + fz * fz);
+            const double dv = (double)vb[k] - (double)pc.w;
+            sq = dv * dv;
         }
-        tab2_reset(T, s);
-    }
-}
-
-template <typename TL, typename TI>
-__global__ void __launch_bounds__(kST, 4)
-stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t Lcap, Acc2 b, TileGeo G, const uint32_t *__restrict__ d_L) {
-    __shared__ Tab2 T;
-    const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int kWarps = kST / 32;
-    for (int s = threadIdx.x; s < kTab; s += blockDim.x) tab2_reset(T, s);
-    __syncthreads();
-    for (uint32_t tile = blockIdx.x; tile < G.ntiles; tile += gridDim.x) {
-        for (int j0 = warp; j0 < kTasks; j0 += kBatch * kWarps) {
-            uint32_t lb[kBatch];
-            float vb[kBatch];
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                uint32_t row, c, y, z;
-                const bool in = tile_task(G, tile, j0 + k * kWarps, D, H, row, c, y, z);
-                const int64_t x = (int64_t)c * 32 + lane;
-                const uint32_t l = (in && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
-                lb[k] = (l > (uint32_t)L) ? 0u : l;
-            }
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                uint32_t row, c, y, z;
-                tile_task(G, tile, j0 + k * kWarps, D, H, row, c, y, z);
-                const int64_t x = (int64_t)c * 32 + lane;
-                vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
-            }
-#pragma unroll
-            for (int k = 0; k < kBatch; ++k) {
-                const uint32_t l = lb[k];
-                if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
-                uint32_t row, c, y, z;
-                tile_task(G, tile, j0 + k * kWarps, D, H, row, c, y, z);
-                const int64_t x = (int64_t)c * 32 + lane;
-                // distances in float32 (relative error a few 1e-7), their sums and the
-                // squared deviations in float64; the squared deviations are divided
-                // by the area once per label
-                float dc = 0.0f, dm = 0.0f;
-                double sq = 0.0;
-                if (l) {
-                    const uint32_t i = l - 1;
-                    const float4 pc = b.pc[i], pm = b.pm[i];
-                    const float xf = (float)x, yf = (float)y, zf = (float)z;
-                    const float ex = xf - pc.x, ey = yf - pc.y, ez = zf - pc.z;
-                    const float fx = xf - pm.x, fy = yf - pm.y, fz = zf - pm.z;
-                    dc = sqrtf(ex * ex + ey * ey + ez * ez);
-                    dm = sqrtf(fx * fx + fy * fy + fz * fz);
-                    const double dv = (double)vb[k] - (double)pc.w;
-                    sq = dv * dv;
-                }
-                const Seg s = make_seg(l);
-                const double sdc = s.scan_add((double)dc);
-                const double sdm = s.scan_add((double)dm);
-                const double ssq = s.scan_add(sq);
-                const float mdc = s.scan_max(dc);
-                const float mdm = s.scan_max(dm);
-                if (s.tail && l) {
-                    const int t = tab_slot(T.key, l);
-                    if (t >= 0) {
-                        atomicAdd(T.sdc + t, sdc);
-                        atomicAdd(T.sdm + t, sdm);
-                        atomicAdd(T.ssq + t, ssq);
-                        atomicMax(T.mdc + t, __float_as_uint(mdc));
-                        atomicMax(T.mdm + t, __float_as_uint(mdm));
-                    } else {
-                        const uint32_t i = l - 1;
-                        atomicAdd(b.sdc + i, sdc);
-                        atomicAdd(b.sdm + i, sdm);
-                        atomicAdd(b.ssq + i, ssq);
-                        atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong((double)mdc));
-                        atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong((double)mdm));
-                    }
-                }
-            }
+        const Seg s = make_seg(l);
+        const double sdc = s.scan_add((double)dc);
+        const double sdm = s.scan_add((double)dm);
+        const double ssq = s.scan_add(sq);
+        const float mdc = s.scan_max(dc);
+        const float mdm = s.scan_max(dm);
+        if (s.tail && l) {
+            const uint32_t i = l - 1;
+            atomicAdd(b.sdc + i, sdc);
+            atomicAdd(b.sdm + i, sdm);
+            atomicAdd(b.ssq + i, ssq);
+            atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong((double)mdc));
+            atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong((double)mdm));
         }
-        __syncthreads();
-        flush2(T, b);
-        __syncthreads();
+        }
     }
 }
 
@@ -601,17 +392,17 @@ __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T) {
 template <typename TL, typename TI>
 int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a,
                 const Acc2 &b, cudaStream_t st, const uint32_t *d_L) {
-    const TileGeo G = make_tile_geo(lab);
-    // persistent CTAs over the tiles (tables flushed per tile)
-    const int blocks = (int)std::min<int64_t>((int64_t)G.ntiles, (int64_t)launch_blocks(int64_t(1) << 40, kST, 4));
+    const int64_t tasks = lab.D * lab.H * ((lab.W + 31) / 32);
+    const int blocks = launch_blocks(tasks * 32, kST, 8);
+    const FastDiv fc((uint32_t)((lab.W + 31) / 32)), fh((uint32_t)lab.H);
     stage_mark(8, st);
     stats_pass1<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, a, G, d_L);
+                                                lab.H, lab.W, L, a, fc, fh, d_L);
     stage_mark(9, st);
     stats_final1<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, T);
     stage_mark(10, st);
     stats_pass2<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, b, G, d_L);
+                                                lab.H, lab.W, L, b, fc, fh, d_L);
     stage_mark(11, st);
     stats_final2<<<launch_blocks(L, 256), 256, 0, st>>>(b, L, T);
     stage_mark(12, st);

@@ -6,13 +6,14 @@
 // The reference's Jacobi steps (box stencil on even steps, face stencil on odd
 // steps, a voxel rewritten only while 0 with the maximum over the stencil
 // including itself, stop at the first step that changes nothing) run on
-// bricks of 8 x by 4 y voxels of one z plane, one warp each (lane = 8 y + x).
-// Only active bricks are visited -- those that may hold a voxel able to change
-// in this step -- so the work per step follows the growth front.  A front
-// crosses an 8x4x1 brick in fewer steps than a 32-voxel row, so a brick is
-// visited fewer times (on the nuclei volume 0.72M visits instead of 1.26M);
-// a warp reads per z plane its 32 voxels as 4 aligned 32-byte row segments
-// plus the brick's halo, and x / y neighbours come by warp shuffles.
+// bricks of 8 x by 4 y voxels by BZ z planes (BZ = 4 in 3D, 1 in 2D), one
+// warp each (lane = 8 y + x, marching the brick's planes).  Only active
+// bricks are visited -- those that may hold a voxel able to change in this
+// step -- so the work per step follows the growth front.  A front crosses a
+// compact brick in few steps, so a brick is visited few times; a warp reads
+// per z plane its 32 voxels as 4 aligned 32-byte row segments plus the
+// brick's halo (all BZ + 2 planes issued at once), and x / y neighbours come
+// by warp shuffles.
 //
 // A step is two phases separated by grid barriers:
 //   A  every active brick computes its candidates' new values from the state
@@ -40,7 +41,10 @@ constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kSlice = 256;                     // per-warp append slice (entries)
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
-constexpr size_t kWideBricks = size_t(2) << 20;  // 2 CTAs per SM above this many bricks
+#ifndef CLE_VORONOI_WIDE_VOXELS
+#define CLE_VORONOI_WIDE_VOXELS (int64_t(64) << 20)
+#endif
+constexpr int64_t kWideVoxels = CLE_VORONOI_WIDE_VOXELS;  // 2 CTAs per SM above this many voxels
 constexpr uint32_t kTraceSteps = 256;
 
 struct BState {
@@ -57,19 +61,30 @@ constexpr int kBX = 8;                          // brick: 8 x ...
 constexpr int kBY = 4;                          // ... by 4 y voxels of one z plane
 static_assert(kBX == 8 && kBY == 4, "the brick-edge lane masks assume 8x4 bricks");
 
+// Bricks of 3D images hold kBZ planes (8 x 4 x kBZ voxels, one warp, each
+// lane owning one (x, y) column of the brick): a warp loads the kBZ + 2
+// planes a visit needs at once, so the per-visit memory latency is shared by
+// kBZ planes, and a front crosses a taller brick in fewer visits (a CPU
+// replay of the growth on light-sheet data: 0.64M visits of 8x4x4 bricks
+// against 1.46M of 8x4x1).  2D images use 8 x 4 x 1.
+#ifndef CLE_VORONOI_BZ
+#define CLE_VORONOI_BZ 4
+#endif
+constexpr int kBZ3 = CLE_VORONOI_BZ;
+
 struct BGeo {
     Geo g;
-    uint32_t WB, HB;    // bricks along x, along y
+    uint32_t WB, HB, DB; // bricks along x, y, z
     FastDiv fWB, fHB;
     int is3d;
 };
 
-// brick b -> (z, yb, xb)
-__device__ __forceinline__ void brick_zyx(const BGeo &G, uint32_t b, uint32_t &z, uint32_t &yb, uint32_t &xb) {
+// brick b -> (zb, yb, xb)
+__device__ __forceinline__ void brick_zyx(const BGeo &G, uint32_t b, uint32_t &zb, uint32_t &yb, uint32_t &xb) {
     const uint32_t r = G.fWB.div(b);
     xb = b - r * G.WB;
-    z = G.fHB.div(r);
-    yb = r - z * G.HB;
+    zb = G.fHB.div(r);
+    yb = r - zb * G.HB;
 }
 
 // Per-warp append slice in shared memory, flushed to a global list by the
@@ -127,7 +142,7 @@ __device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
 
 // Queues bricks (z+dz, yb+dyb, xb+dxb) for the step tagged `tag`; lane k of
 // the warp handles offset k of the 3x3x3 neighbourhood when want.  Warp-wide.
-__device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint32_t yb, uint32_t xb,
+__device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t zb, uint32_t yb, uint32_t xb,
                                                  bool want, uint32_t tag, uint32_t *bstep,
                                                  WarpAppender &ap) {
     const int lane = threadIdx.x & 31;
@@ -135,8 +150,8 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint
     uint32_t nb = 0;
     if (want && lane < 27) {
         const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
-        const int zz = (int)z + dz, yy = (int)yb + dyb, xx = (int)xb + dxb;
-        if (zz >= 0 && yy >= 0 && xx >= 0 && zz < (int)G.g.D && yy < (int)G.HB && xx < (int)G.WB) {
+        const int zz = (int)zb + dz, yy = (int)yb + dyb, xx = (int)xb + dxb;
+        if (zz >= 0 && yy >= 0 && xx >= 0 && zz < (int)G.DB && yy < (int)G.HB && xx < (int)G.WB) {
             nb = ((uint32_t)zz * G.HB + (uint32_t)yy) * G.WB + (uint32_t)xx;
             take = atomicMax(bstep + nb, tag) < tag;
         }
@@ -145,9 +160,9 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t z, uint
 }
 
 // MINB CTAs per SM: 1 for volumes whose labels mostly stay in L2 (a visit
-// waits on L2 hits), 2 for larger ones (2x the warps to hide DRAM latency;
-// the kernel fits 32 registers without spills).
-template <bool IS3D, int MINB>
+// waits on L2 hits), 2 for larger ones (2x the warps to hide DRAM latency).
+// BZ planes per brick.
+template <bool IS3D, int BZ, int MINB>
 __global__ void __launch_bounds__(kBT, MINB)
 voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
@@ -170,7 +185,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             uint32_t x, y, z;
             m2xyz(g, __ldcg(seeds + i), x, y, z);
             const bool want = lane < 27 && (IS3D || (lane / 9) == 1);
-            queue_neighbours(G, z, y / kBY, x / kBX, want, 1u, bstep, ap);
+            queue_neighbours(G, z / BZ, y / kBY, x / kBX, want, 1u, bstep, ap);
         }
         ap.maybe_flush(B0, &S->sizes[0]);
     }
@@ -205,19 +220,20 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const uint32_t b = bnext;
             bnext = (idx + wstride < nB) ? __ldcg(F + idx + wstride) : 0u;
             if (idx >= nB) continue;
-            uint32_t z, yb, xb;
-            brick_zyx(G, b, z, yb, xb);
+            uint32_t zb, yb, xb;
+            brick_zyx(G, b, zb, yb, xb);
+            const int z0 = (int)(zb * BZ);
             const int xl = lane & (kBX - 1), yl = lane / kBX;
             const int x = (int)(xb * kBX) + xl, y = (int)(yb * kBY) + yl;
             const int xc = min(x, (int)g.W - 1), yc = min(y, (int)g.H - 1);
-            const bool inmask = x < (int)g.W && y < (int)g.H &&
-                                seg[((uint32_t)z * g.H + (uint32_t)yc) * g.W + (uint32_t)xc] != 0;
+            const bool xyin = x < (int)g.W && y < (int)g.H;
             // per z plane: c the lane's voxel, and one voxel of the brick's halo
             // per lane (28 of them, clamped to the image): lanes 0-7 the row
             // y - 1, 8-15 the row y + 4, 16-19 the column x - 1, 20-23 the
             // column x + 8, 24-27 the corners; lanes that need a halo voxel
-            // fetch it by shuffle
-            constexpr int K = 2 * ZR + 1;
+            // fetch it by shuffle.  Planes z0 - 1 .. z0 + BZ (clamped), all
+            // loads issued before any is used.
+            constexpr int K = BZ + 2 * ZR;
             const int x0b = (int)(xb * kBX), y0b = (int)(yb * kBY);
             int hx_ = x0b, hy_ = y0b;
             if (lane < 8) { hx_ = x0b + lane; hy_ = y0b - 1; }
@@ -225,60 +241,69 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             else if (lane < 24) { hx_ = lane < 20 ? x0b - 1 : x0b + kBX; hy_ = y0b + (lane & 3); }
             else { hx_ = (lane & 1) ? x0b + kBX : x0b - 1; hy_ = (lane & 2) ? y0b + kBY : y0b - 1; }
             const uint32_t hoff = (uint32_t)clampi(hy_, 0, (int)g.H - 1) * g.W + (uint32_t)clampi(hx_, 0, (int)g.W - 1);
+            const uint32_t coff = (uint32_t)yc * g.W + (uint32_t)xc;
             uint32_t c[K], hv[K];
+            bool inm[BZ];
 #pragma unroll
-            for (int dz = -ZR; dz <= ZR; ++dz) {
-                const int k = dz + ZR;
-                const uint32_t zz = (uint32_t)clampi((int)z + dz, 0, (int)g.D - 1);
+            for (int j = 0; j < BZ; ++j)
+                inm[j] = xyin && z0 + j < (int)g.D &&
+                         seg[(uint32_t)(z0 + j) * g.H * g.W + coff] != 0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const uint32_t zz = (uint32_t)clampi(z0 - ZR + k, 0, (int)g.D - 1);
                 const uint32_t *P = lab + zz * g.H * g.W;
-                c[k] = ld_cg(P + (uint32_t)yc * g.W + (uint32_t)xc);
+                c[k] = ld_cg(P + coff);
                 hv[k] = lane < 28 ? ld_cg(P + hoff) : 0u;
             }
-            const int kc = ZR;                  // centre plane
-            const bool cand = inmask && c[kc] == 0u;
-            uint32_t out = 0;
-            bool remain = false, pend = false;
-            if (__any_sync(0xffffffffu, cand)) {
-                // the halo voxels this lane needs: h its halo row's (first /
-                // last brick row), s its halo column's (first / last brick
-                // column), q the corner (both)
-                const int src_h = yl == 0 ? xl : 8 + xl;
-                const int src_s = (xl == 0 ? 16 : 20) + (yl & 3);
-                const int src_q = 24 + (yl == kBY - 1 ? 2 : 0) + (xl == kBX - 1 ? 1 : 0);
-                // box: the maximum over the planes, then over x - 1 .. x + 1 (the
-                // lane's row and its halo row), then over y - 1 .. y + 1
-                uint32_t cz = c[0], hm = hv[0];
+            bool remain = false, pl = false;
 #pragma unroll
-                for (int k = 1; k < K; ++k) { cz = max(cz, c[k]); hm = max(hm, hv[k]); }
-                const uint32_t hz = __shfl_sync(0xffffffffu, hm, src_h);
-                const uint32_t sz = __shfl_sync(0xffffffffu, hm, src_s);
-                const uint32_t qz = __shfl_sync(0xffffffffu, hm, src_q);
-                const bool x0 = xl == 0, x1 = xl == kBX - 1, y0 = yl == 0, y1 = yl == kBY - 1;
-                const uint32_t cl = __shfl_up_sync(0xffffffffu, cz, 1), cr = __shfl_down_sync(0xffffffffu, cz, 1);
-                const uint32_t hl = __shfl_up_sync(0xffffffffu, hz, 1), hr = __shfl_down_sync(0xffffffffu, hz, 1);
-                const uint32_t rx = max(cz, max(x0 ? sz : cl, x1 ? sz : cr));
-                const uint32_t hx = max(hz, max(x0 ? qz : hl, x1 ? qz : hr));
-                const uint32_t ru = __shfl_up_sync(0xffffffffu, rx, kBX), rd = __shfl_down_sync(0xffffffffu, rx, kBX);
-                const uint32_t bm = max(rx, max(y0 ? hx : ru, y1 ? hx : rd));
-                // face: the centre plane at x +- 1 and y +- 1, the planes z +- 1 at (x, y)
-                const uint32_t v = c[kc];
-                const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1), fr = __shfl_down_sync(0xffffffffu, v, 1);
-                const uint32_t fu = __shfl_up_sync(0xffffffffu, v, kBX), fd = __shfl_down_sync(0xffffffffu, v, kBX);
-                const uint32_t hc = __shfl_sync(0xffffffffu, hv[kc], src_h);
-                const uint32_t sc = __shfl_sync(0xffffffffu, hv[kc], src_s);
-                uint32_t dm = max(max(x0 ? sc : fl, x1 ? sc : fr), max(y0 ? hc : fu, y1 ? hc : fd));
-                if (ZR) dm = max(dm, max(c[0], c[K - 1]));
-                bool pl = false;
-                if (cand) {
-                    const uint32_t m = box ? bm : dm;
-                    out = m;
-                    pl = m == 0u && bm != 0u;     // face stencil missed, the box stencil will hit
-                    changed += (m != 0u);
-                    remain = (m == 0u);
+            for (int j = 0; j < BZ; ++j) {
+                const int kc = j + ZR;              // the plane's index in c / hv
+                const bool cand = inm[j] && c[kc] == 0u;
+                uint32_t out = 0;
+                if (__any_sync(0xffffffffu, cand)) {
+                    // the halo voxels this lane needs: h its halo row's (first /
+                    // last brick row), s its halo column's (first / last brick
+                    // column), q the corner (both)
+                    const int src_h = yl == 0 ? xl : 8 + xl;
+                    const int src_s = (xl == 0 ? 16 : 20) + (yl & 3);
+                    const int src_q = 24 + (yl == kBY - 1 ? 2 : 0) + (xl == kBX - 1 ? 1 : 0);
+                    const bool x0 = xl == 0, x1 = xl == kBX - 1, y0 = yl == 0, y1 = yl == kBY - 1;
+                    // box: the maximum over the planes, then over x - 1 .. x + 1 (the
+                    // lane's row and its halo row), then over y - 1 .. y + 1
+                    uint32_t cz = c[kc], hm = hv[kc];
+                    if (ZR) {
+                        cz = max(cz, max(c[kc - ZR], c[kc + ZR]));
+                        hm = max(hm, max(hv[kc - ZR], hv[kc + ZR]));
+                    }
+                    const uint32_t hz = __shfl_sync(0xffffffffu, hm, src_h);
+                    const uint32_t sz = __shfl_sync(0xffffffffu, hm, src_s);
+                    const uint32_t qz = __shfl_sync(0xffffffffu, hm, src_q);
+                    const uint32_t cl = __shfl_up_sync(0xffffffffu, cz, 1), cr = __shfl_down_sync(0xffffffffu, cz, 1);
+                    const uint32_t hl = __shfl_up_sync(0xffffffffu, hz, 1), hr = __shfl_down_sync(0xffffffffu, hz, 1);
+                    const uint32_t rx = max(cz, max(x0 ? sz : cl, x1 ? sz : cr));
+                    const uint32_t hx = max(hz, max(x0 ? qz : hl, x1 ? qz : hr));
+                    const uint32_t ru = __shfl_up_sync(0xffffffffu, rx, kBX), rd = __shfl_down_sync(0xffffffffu, rx, kBX);
+                    const uint32_t bm = max(rx, max(y0 ? hx : ru, y1 ? hx : rd));
+                    // face: the plane at x +- 1 and y +- 1, the planes z +- 1 at (x, y)
+                    const uint32_t v = c[kc];
+                    const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1), fr = __shfl_down_sync(0xffffffffu, v, 1);
+                    const uint32_t fu = __shfl_up_sync(0xffffffffu, v, kBX), fd = __shfl_down_sync(0xffffffffu, v, kBX);
+                    const uint32_t hc = __shfl_sync(0xffffffffu, hv[kc], src_h);
+                    const uint32_t sc = __shfl_sync(0xffffffffu, hv[kc], src_s);
+                    uint32_t dm = max(max(x0 ? sc : fl, x1 ? sc : fr), max(y0 ? hc : fu, y1 ? hc : fd));
+                    if (ZR) dm = max(dm, max(c[kc - ZR], c[kc + ZR]));
+                    if (cand) {
+                        const uint32_t m = box ? bm : dm;
+                        out = m;
+                        pl |= m == 0u && bm != 0u;   // face stencil missed, the box stencil will hit
+                        changed += (m != 0u);
+                        remain |= (m == 0u);
+                    }
                 }
-                pend = __any_sync(0xffffffffu, pl);
+                Mv[((size_t)idx * BZ + j) * 32 + lane] = out;
             }
-            Mv[(size_t)idx * 32 + lane] = out;
+            const bool pend = __any_sync(0xffffffffu, pl);
             if (lane == 0) Pf[idx] = pend ? 1u : 0u;
             // no unlabelled mask voxel left after this step: never queue it again
             if (!__any_sync(0xffffffffu, remain) && lane == 0) atomicExch(bstep + b, 0xFFFFFFFFu);
@@ -306,20 +331,27 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const uint32_t idx = base + warp;
             if (idx < nB) {
                 const uint32_t b = __ldcg(F + idx);
-                const uint32_t m = Mv[(size_t)idx * 32 + lane];
+                uint32_t m[BZ];
+#pragma unroll
+                for (int j = 0; j < BZ; ++j) m[j] = Mv[((size_t)idx * BZ + j) * 32 + lane];
                 const bool pend = __ldcg(Pf + idx) != 0u;
-                uint32_t z, yb, xb;
-                brick_zyx(G, b, z, yb, xb);
+                uint32_t zb, yb, xb;
+                brick_zyx(G, b, zb, yb, xb);
                 const uint32_t x = xb * kBX + (uint32_t)(lane & (kBX - 1)), y = yb * kBY + (uint32_t)(lane / kBX);
-                if (m) st_cg(lab + ((uint32_t)z * g.H + y) * g.W + x, m);
-                const unsigned ch = __ballot_sync(0xffffffffu, m != 0u);
+                unsigned ch[BZ], chall = 0u;
+#pragma unroll
+                for (int j = 0; j < BZ; ++j) {
+                    if (m[j]) st_cg(lab + ((zb * BZ + (uint32_t)j) * g.H + y) * g.W + x, m[j]);
+                    ch[j] = __ballot_sync(0xffffffffu, m[j] != 0u);
+                    chall |= ch[j];
+                }
                 bool want = false;
                 if (lane < 27) {
                     const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
                     if (IS3D || dz == 0) {
-                        // changed voxels next to brick (dyb, dxb): the first / last
-                        // brick row and column (any voxel for the planes z +- 1)
-                        unsigned sel = ch;
+                        // changed voxels next to brick (dz, dyb, dxb): the first / last
+                        // plane, brick row and column
+                        unsigned sel = dz < 0 ? ch[0] : (dz > 0 ? ch[BZ - 1] : chall);
                         if (dyb < 0) sel &= 0x000000FFu;
                         else if (dyb > 0) sel &= 0xFF000000u;
                         if (dxb < 0) sel &= 0x01010101u;
@@ -328,7 +360,7 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                         if (pend && dz == 0 && dyb == 0 && dxb == 0) want = true;
                     }
                 }
-                queue_neighbours(G, z, yb, xb, want, tag, bstep, ap);
+                queue_neighbours(G, zb, yb, xb, want, tag, bstep, ap);
             }
             ap.maybe_flush(Fn, nsize);
         }
@@ -346,9 +378,11 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
     }
 }
 
+int brick_planes(const Img &im) { return im.ndim == 3 ? kBZ3 : 1; }
 uint32_t bricks_x(const Img &im) { return (uint32_t)((im.W + kBX - 1) / kBX); }
 uint32_t bricks_y(const Img &im) { return (uint32_t)((im.H + kBY - 1) / kBY); }
-uint32_t brick_count(const Img &im) { return (uint32_t)im.D * bricks_y(im) * bricks_x(im); }
+uint32_t bricks_z(const Img &im) { return (uint32_t)((im.D + brick_planes(im) - 1) / brick_planes(im)); }
+uint32_t brick_count(const Img &im) { return bricks_z(im) * bricks_y(im) * bricks_x(im); }
 
 }  // namespace
 
@@ -359,7 +393,7 @@ size_t voronoi_frontier_workspace_bytes(const Img &im) {
     a.take<uint32_t>(nb);        // list 0
     a.take<uint32_t>(nb);        // list 1
     a.take<uint32_t>(nb);        // per-brick step tags
-    a.take<uint32_t>(nb * 32);   // per-voxel phase-A results
+    a.take<uint32_t>(nb * 32 * (size_t)brick_planes(im));   // per-voxel phase-A results
     a.take<uint32_t>(nb);        // per-entry pending flags
     return a.off;
 }
@@ -372,7 +406,7 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     uint32_t *B0 = ws.take<uint32_t>(nb);
     uint32_t *B1 = ws.take<uint32_t>(nb);
     uint32_t *bstep = ws.take<uint32_t>(nb);
-    uint32_t *Mv = ws.take<uint32_t>(nb * 32);
+    uint32_t *Mv = ws.take<uint32_t>(nb * 32 * (size_t)brick_planes(im));
     uint32_t *Pf = ws.take<uint32_t>(nb);
     if (!ws.ok()) { set_error("masked_voronoi_labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(BState), st));
@@ -381,16 +415,20 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     G.g = make_geo(im);
     G.WB = bricks_x(im);
     G.HB = bricks_y(im);
+    G.DB = bricks_z(im);
     G.fWB = FastDiv(G.WB);
     G.fHB = FastDiv(G.HB);
     G.is3d = im.ndim == 3 ? 1 : 0;
     uint32_t max_steps = lim.steps_for(im.n());   // each step that changes labels >= 1 voxel
     uint64_t loop_ns = lim.loop_ns, barrier_ns = lim.barrier_ns;
     const volatile int *cancel = lim.cancel;
-    const int wide = nb > kWideBricks ? 1 : 0;
+    // 3D (kBZ3-plane bricks, 64 registers): one CTA per SM, the measured best
+    // (the 2-CTA form spills: light-sheet growth 6.98 vs 5.18 ms); 2D keeps
+    // 2 CTAs per SM above kWideVoxels
+    const int wide = (G.is3d == 0 && im.n() > kWideVoxels) ? 1 : 0;
     const void *kerns[2][2] = {
-        {(const void *)voronoi_bricks_kernel<false, 1>, (const void *)voronoi_bricks_kernel<false, 2>},
-        {(const void *)voronoi_bricks_kernel<true, 1>, (const void *)voronoi_bricks_kernel<true, 2>}};
+        {(const void *)voronoi_bricks_kernel<false, 1, 1>, (const void *)voronoi_bricks_kernel<false, 1, 2>},
+        {(const void *)voronoi_bricks_kernel<true, kBZ3, 1>, (const void *)voronoi_bricks_kernel<true, kBZ3, 1>}};
     const void *kern = kerns[G.is3d][wide];
     // set on every call: the attribute belongs to the current device's context
     CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
