@@ -554,11 +554,13 @@ def run_b200(args):
     labels_dev = labels.tensor.cpu() if not dense else None
 
     # end to end through the public API with pinned host buffers
-    pinned_in = torch.from_numpy(host_np).pin_memory()
-    e2e = None if dense else e2e_served(pinned_in, w, args.steps, world, ref_labels=labels_dev)
-    e2e_serial = e2e_per_call(pinned_in, w, max(2, min(5, args.steps // 4)), world, flush)
-    if e2e is None:
-        e2e = e2e_serial
+    e2e = e2e_serial = None
+    if not args.no_e2e:
+        pinned_in = torch.from_numpy(host_np).pin_memory()
+        e2e = None if dense else e2e_served(pinned_in, w, args.steps, world, ref_labels=labels_dev)
+        e2e_serial = e2e_per_call(pinned_in, w, max(2, min(5, args.steps // 4)), world, flush)
+        if e2e is None:
+            e2e = e2e_serial
     del labels_dev
 
     # roofline: the dominant kernel stage
@@ -918,6 +920,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="leave out the end-to-end legs (profiler runs)")
     ap.add_argument("--trace", action="store_true", help="include the Voronoi per-step trace")
     ap.add_argument("--tiles", type=int, default=512, help="batch workload: number of tiles")
     ap.add_argument("--lanes", type=int, default=8, help="served: requests in flight (slots)")
