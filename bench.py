@@ -507,13 +507,30 @@ def run_b200(args):
 
     dense = w.get("op") == "gauss_otsu"
 
+    # the statistics read the label count the pipeline leaves on the device
+    # (cle_statistics_of_labelled_pixels_device_count, as the served form
+    # does): no label-maximum pass over the image and no host round trip
+    # inside a step; the table is sized for one label per 64 voxels
+    stream_ptr = stream.cuda_stream
+    if not dense:
+        ws_vol = cle._ops.workspaces.get(src)
+        count_ptr = lib.cle_workspace_label_count(ws_vol.data_ptr())
+        cap = max(1024, nvox // 64)
+        table_dev = torch.empty((35, cap), dtype=torch.float32, device=dev)
+        sdesc, ldesc = _lib.tensor_desc(src.tensor), _lib.tensor_desc(labels.tensor)
+        stats_ws = torch.empty(int(lib.cle_statistics_workspace_bytes(_lib.ref(ldesc), cap)), dtype=torch.uint8,
+                               device=dev)
+
     def step():
         if dense:
             cle.gauss_otsu_labeling(src, labels, outline_sigma=w["outline"])
-        else:
-            cle._ops._vol(src, labels, w["spot"], w["outline"], check=False)
-        L = cle._ops._label_max(labels)
-        return cle.statistics_table(src, labels, L), L
+            L = cle._ops._label_max(labels)
+            return cle.statistics_table(src, labels, L), L
+        cle._ops._vol(src, labels, w["spot"], w["outline"], check=False)
+        _lib.check(lib.cle_statistics_of_labelled_pixels_device_count(
+            _lib.ref(sdesc), _lib.ref(ldesc), count_ptr, cap, table_dev.data_ptr(), stats_ws.data_ptr(),
+            stats_ws.numel(), stream_ptr), "statistics_of_labelled_pixels")
+        return table_dev, None
 
     # correctness of the loop status once (not timed)
     if not dense:
@@ -548,6 +565,8 @@ def run_b200(args):
     barrier(world)
     clk = clocks.stop()
     lib.cle_profile_enable(0)
+    if L is None:
+        L = cle._ops._label_max(labels)
     total_ms = max_over_ranks(sum(times), world)
     ms_per_step = total_ms / args.steps
     value = nvox * world * args.steps / (total_ms / 1e3) / 1e6

@@ -72,8 +72,15 @@ Acc2 take_acc2(Arena &a, int64_t L) {
     return c;
 }
 
-__global__ void stats_init(Acc1 a, Acc2 b, int64_t L) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L;
+// With a device label count (d_L) the init and finalise kernels touch only the
+// first min(count, L) labels; L stays the table's row stride.
+__device__ __forceinline__ int64_t live_labels(int64_t L, const uint32_t *d_L) {
+    return d_L ? ((int64_t)*d_L < L ? (int64_t)*d_L : L) : L;
+}
+
+__global__ void stats_init(Acc1 a, Acc2 b, int64_t L, const uint32_t *__restrict__ d_L) {
+    const int64_t n = live_labels(L, d_L);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         a.cnt[i] = 0;
         a.sx[i] = a.sy[i] = a.sz[i] = 0ull;
@@ -262,8 +269,9 @@ enum {
 };
 static_assert(C_NCOLS == CLE_STATS_NCOLS, "table width");
 
-__global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L;
+__global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T, const uint32_t *__restrict__ d_L) {
+    const int64_t n = live_labels(L, d_L);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const bool any = a.cnt[i] != 0u;
         const float area = (float)a.cnt[i];
@@ -370,8 +378,9 @@ stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D,
     }
 }
 
-__global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L;
+__global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T, const uint32_t *__restrict__ d_L) {
+    const int64_t n = live_labels(L, d_L);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         auto put = [&](int c, float v) { T[(int64_t)c * L + i] = v; };
         const float area = b.pm[i].w;
@@ -399,12 +408,12 @@ int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc
     stats_pass1<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
                                                 lab.H, lab.W, L, a, fc, fh, d_L);
     stage_mark(9, st);
-    stats_final1<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, T);
+    stats_final1<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, T, d_L);
     stage_mark(10, st);
     stats_pass2<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
                                                 lab.H, lab.W, L, b, fc, fh, d_L);
     stage_mark(11, st);
-    stats_final2<<<launch_blocks(L, 256), 256, 0, st>>>(b, L, T);
+    stats_final2<<<launch_blocks(L, 256), 256, 0, st>>>(b, L, T, d_L);
     stage_mark(12, st);
     CLE_LAUNCH_CHECK_N("statistics", 4);
     return CLE_OK;
@@ -439,7 +448,7 @@ int statistics(const Img &inten, const Img &lab, int64_t L, float *T, Arena &ws,
     Acc1 a = take_acc1(ws, L);
     Acc2 b = take_acc2(ws, L);
     if (!ws.ok()) { set_error("statistics: workspace too small"); return CLE_ERR_WORKSPACE; }
-    stats_init<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L);
+    stats_init<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, d_L);
     CLE_LAUNCH_CHECK("statistics init");
     switch (lab.dtype) {
         case CLE_U32: return stats_i<uint32_t>(inten, lab, L, T, a, b, st, d_L);

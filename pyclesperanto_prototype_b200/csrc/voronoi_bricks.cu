@@ -41,6 +41,7 @@ constexpr int kWPB = kBT / 32;                  // warps per CTA
 constexpr int kSlice = 256;                     // per-warp append slice (entries)
 constexpr size_t kBBufBytes = sizeof(uint32_t) * kSlice * kWPB;
 constexpr uint32_t kTailBricks = 128;           // single-CTA finish at or below this
+constexpr uint32_t kBitmapBricks = 16384;       // bitmap queueing at or above this (large volumes)
 #ifndef CLE_VORONOI_WIDE_VOXELS
 #define CLE_VORONOI_WIDE_VOXELS (int64_t(64) << 20)
 #endif
@@ -128,6 +129,53 @@ struct WarpAppender {
     }
 };
 
+// The next step's bricks while several CTAs run: phase B sets their bits in
+// `q` (fire-and-forget atomicOr, so repeats cost nothing), bricks without an
+// unlabelled mask voxel are set in `done`, and a two-pass grid compaction
+// turns q & ~done into the next list in brick-index order -- warps that run
+// at the same time then visit neighbouring bricks, whose halo rows and label
+// sectors they share in L2.  `ccount` holds one count per CTA.
+struct BQueue {
+    uint32_t *q, *done, *ccount;
+    uint32_t nwords;
+};
+
+// Brick at offset `lane` (0..26) of the 3x3x3 neighbourhood, if inside.
+__device__ __forceinline__ bool neighbour_brick(const BGeo &G, uint32_t zb, uint32_t yb, uint32_t xb, int lane,
+                                                uint32_t &nb) {
+    const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+    const int zz = (int)zb + dz, yy = (int)yb + dyb, xx = (int)xb + dxb;
+    if (zz < 0 || yy < 0 || xx < 0 || zz >= (int)G.DB || yy >= (int)G.HB || xx >= (int)G.WB) return false;
+    nb = ((uint32_t)zz * G.HB + (uint32_t)yy) * G.WB + (uint32_t)xx;
+    return true;
+}
+
+// Exclusive prefix of v over the CTA (kBT threads); total of the CTA in `total`.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *s_w, uint32_t &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kWPB ? s_w[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kWPB) s_w[lane] = w;
+    }
+    __syncthreads();
+    total = s_w[kWPB - 1];
+    return (warp ? s_w[warp - 1] : 0u) + x - v;
+}
+
 __device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -139,6 +187,8 @@ __device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
         for (int i = 0; i < kWPB; ++i) s += red[i];
     return s;   // thread 0
 }
+
+
 
 // Queues bricks (z+dz, yb+dyb, xb+dxb) for the step tagged `tag`; lane k of
 // the warp handles offset k of the 3x3x3 neighbourhood when want.  Warp-wide.
@@ -159,6 +209,54 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t zb, uin
     ap.push(take, nb);
 }
 
+// Two-pass grid compaction of the queue bitmap (q & ~done) into the list F in
+// brick-index order, its length in *nsize; clears q.  Grid-wide: every CTA
+// calls it; returns false when a barrier gave up.
+__device__ bool compact_queue(const BQueue &Qb, uint32_t *F, uint32_t *nsize, BState *S, uint64_t barrier_ns,
+                              uint32_t *s_red, uint32_t *s_scan, uint32_t *s_off) {
+    // pass 1: each CTA counts the queued bricks of its contiguous range of
+    // bitmap words
+    const uint32_t per = (Qb.nwords + gridDim.x - 1) / gridDim.x;
+    const uint32_t w0 = min(Qb.nwords, blockIdx.x * per), w1 = min(Qb.nwords, w0 + per);
+    uint32_t c = 0;
+    for (uint32_t w = w0 + threadIdx.x; w < w1; w += blockDim.x)
+        c += (uint32_t)__popc(ld_cg(Qb.q + w) & ~ld_cg(Qb.done + w));
+    const uint32_t cs = block_total(c, s_red);
+    if (threadIdx.x == 0) st_cg(Qb.ccount + blockIdx.x, cs);
+    if (!grid_sync(&S->bar, &S->err, barrier_ns)) return false;
+    // pass 2: the CTA's offset, then its bricks in index order
+    uint32_t before = 0, all = 0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+        const uint32_t v = ld_cg(Qb.ccount + i);
+        all += v;
+        if (i < blockIdx.x) before += v;
+    }
+    const uint32_t before_t = block_total(before, s_red);
+    if (threadIdx.x == 0) s_off[0] = before_t;
+    const uint32_t all_t = block_total(all, s_red);
+    if (threadIdx.x == 0) s_off[1] = all_t;
+    __syncthreads();
+    uint32_t off = s_off[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nsize = s_off[1];
+    for (uint32_t base = w0; base < w1; base += blockDim.x) {
+        const uint32_t w = base + threadIdx.x;
+        uint32_t bits = 0;
+        if (w < w1) {
+            bits = ld_cg(Qb.q + w) & ~ld_cg(Qb.done + w);
+            st_cg(Qb.q + w, 0u);
+        }
+        uint32_t total = 0;
+        uint32_t pos = off + block_excl_scan((uint32_t)__popc(bits), s_scan, total);
+        while (bits) {
+            const uint32_t bit = (uint32_t)(__ffs(bits) - 1);
+            bits &= bits - 1u;
+            F[pos++] = w * 32u + bit;
+        }
+        off += total;
+    }
+    return grid_sync(&S->bar, &S->err, barrier_ns);
+}
+
 // MINB CTAs per SM: 1 for volumes whose labels mostly stay in L2 (a visit
 // waits on L2 hits), 2 for larger ones (2x the warps to hide DRAM latency).
 // BZ planes per brick.
@@ -168,8 +266,10 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
                       uint32_t max_steps, uint64_t loop_ns, uint64_t barrier_ns,
-                      const volatile int *cancel, unsigned long long *trace) {
+                      const volatile int *cancel, unsigned long long *trace, BQueue Qb, int use_bitmap) {
     __shared__ uint32_t s_red[kWPB];
+    __shared__ uint32_t s_scan[kWPB];
+    __shared__ uint32_t s_off[2];
     const Geo &g = G.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpAppender ap{&S->err, 0u};
@@ -185,12 +285,20 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             uint32_t x, y, z;
             m2xyz(g, __ldcg(seeds + i), x, y, z);
             const bool want = lane < 27 && (IS3D || (lane / 9) == 1);
-            queue_neighbours(G, z / BZ, y / kBY, x / kBX, want, 1u, bstep, ap);
+            if (use_bitmap) {
+                uint32_t nb = 0;
+                if (want && neighbour_brick(G, z / BZ, y / kBY, x / kBX, lane, nb))
+                    atomicOr(Qb.q + (nb >> 5), 1u << (nb & 31u));
+            } else {
+                queue_neighbours(G, z / BZ, y / kBY, x / kBX, want, 1u, bstep, ap);
+            }
         }
-        ap.maybe_flush(B0, &S->sizes[0]);
+        if (!use_bitmap) ap.maybe_flush(B0, &S->sizes[0]);
     }
-    ap.flush(B0, &S->sizes[0]);
+    if (!use_bitmap) ap.flush(B0, &S->sizes[0]);
     bool ok = grid_sync(&S->bar, &S->err, barrier_ns);
+    // large volumes: step 0's list in brick order as well
+    if (use_bitmap && ok) ok = compact_queue(Qb, B0, &S->sizes[0], S, barrier_ns, s_red, s_scan, s_off);
 
     const uint64_t t_start = global_ns();
     uint32_t t = 0;
@@ -207,6 +315,9 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             tail = true;                      // uniform: nB was read after a barrier
             if (blockIdx.x != 0) break;       // CTA 0 finishes alone
         }
+        // many bricks on a large volume: the next list goes through the
+        // queue bitmap (brick order, two more barriers); otherwise appends
+        const bool bitmap = use_bitmap && !tail && nB >= kBitmapBricks;
         const uint32_t wstride = tail ? kWPB : gridDim.x * kWPB;
         const uint32_t wbase = tail ? 0 : blockIdx.x * kWPB;
         const bool box = (t & 1) == 0;
@@ -306,7 +417,10 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
             const bool pend = __any_sync(0xffffffffu, pl);
             if (lane == 0) Pf[idx] = pend ? 1u : 0u;
             // no unlabelled mask voxel left after this step: never queue it again
-            if (!__any_sync(0xffffffffu, remain) && lane == 0) atomicExch(bstep + b, 0xFFFFFFFFu);
+            if (!__any_sync(0xffffffffu, remain) && lane == 0) {
+                atomicExch(bstep + b, 0xFFFFFFFFu);
+                atomicOr(Qb.done + (b >> 5), 1u << (b & 31u));
+            }
         }
         const uint32_t bs = block_total(changed, s_red);
         if (threadIdx.x == 0 && bs) atomicAdd(&S->changes[t & 3], bs);
@@ -360,13 +474,20 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                         if (pend && dz == 0 && dyb == 0 && dxb == 0) want = true;
                     }
                 }
-                queue_neighbours(G, zb, yb, xb, want, tag, bstep, ap);
+                if (bitmap) {
+                    uint32_t nb = 0;
+                    if (want && lane < 27 && neighbour_brick(G, zb, yb, xb, lane, nb))
+                        atomicOr(Qb.q + (nb >> 5), 1u << (nb & 31u));
+                } else {
+                    queue_neighbours(G, zb, yb, xb, want, tag, bstep, ap);
+                }
             }
-            ap.maybe_flush(Fn, nsize);
+            if (!bitmap) ap.maybe_flush(Fn, nsize);
         }
-        ap.flush(Fn, nsize);
+        if (!bitmap) ap.flush(Fn, nsize);
         if (!tail) ok = grid_sync(&S->bar, &S->err, barrier_ns);
         else { __syncthreads(); ok = *(volatile int *)&S->err == 0; }
+        if (bitmap && ok) ok = compact_queue(Qb, Fn, nsize, S, barrier_ns, s_red, s_scan, s_off);
         if (trace && gtid == 0 && t < kTraceSteps) trace[4 * t + 3] = global_ns() - t_start;
         ++t;
     }
@@ -395,6 +516,9 @@ size_t voronoi_frontier_workspace_bytes(const Img &im) {
     a.take<uint32_t>(nb);        // per-brick step tags
     a.take<uint32_t>(nb * 32 * (size_t)brick_planes(im));   // per-voxel phase-A results
     a.take<uint32_t>(nb);        // per-entry pending flags
+    a.take<uint32_t>((nb + 31) / 32);   // queue bitmap
+    a.take<uint32_t>((nb + 31) / 32);   // finished-brick bitmap
+    a.take<uint32_t>(2048);             // per-CTA counts of the compaction
     return a.off;
 }
 
@@ -408,7 +532,14 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     uint32_t *bstep = ws.take<uint32_t>(nb);
     uint32_t *Mv = ws.take<uint32_t>(nb * 32 * (size_t)brick_planes(im));
     uint32_t *Pf = ws.take<uint32_t>(nb);
+    BQueue Qb;
+    Qb.nwords = (uint32_t)((nb + 31) / 32);
+    Qb.q = ws.take<uint32_t>(Qb.nwords);
+    Qb.done = ws.take<uint32_t>(Qb.nwords);
+    Qb.ccount = ws.take<uint32_t>(2048);
     if (!ws.ok()) { set_error("masked_voronoi_labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
+    CLE_CUDA(cudaMemsetAsync(Qb.q, 0, sizeof(uint32_t) * (size_t)Qb.nwords, st));
+    CLE_CUDA(cudaMemsetAsync(Qb.done, 0, sizeof(uint32_t) * (size_t)Qb.nwords, st));
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(BState), st));
     CLE_CUDA(cudaMemsetAsync(bstep, 0, sizeof(uint32_t) * nb, st));
     BGeo G;
@@ -430,6 +561,9 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
         {(const void *)voronoi_bricks_kernel<false, 1, 1>, (const void *)voronoi_bricks_kernel<false, 1, 2>},
         {(const void *)voronoi_bricks_kernel<true, kBZ3, 1>, (const void *)voronoi_bricks_kernel<true, kBZ3, 1>}};
     const void *kern = kerns[G.is3d][wide];
+    // the sorted bitmap queue pays off where labels do not stay in L2 (on the
+    // 33.5M-voxel nuclei volume the append queue is faster: 0.56 vs 0.69 ms)
+    int use_bitmap = im.n() > kWideVoxels ? 1 : 0;
     // set on every call: the attribute belongs to the current device's context
     CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBBufBytes));
     int dev = 0;
@@ -438,11 +572,12 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBT, kBBufBytes));
     if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
-    const int grid = (int)std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev, lim));
+    const int grid = (int)std::min<int64_t>(std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev, lim)), 2048);
     unsigned long long *trace =
         (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv, &Pf,
-                    &bstep, &S, &d_status, &max_steps, &loop_ns, &barrier_ns, (void *)&cancel, &trace};
+                    &bstep, &S, &d_status, &max_steps, &loop_ns, &barrier_ns, (void *)&cancel, &trace, &Qb,
+                    &use_bitmap};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
     count_launches(1);
     return CLE_OK;
