@@ -97,11 +97,18 @@ maxima_kernel(const Ts *__restrict__ src, Td *__restrict__ dst, int D, int H, in
 // (x-major pixel index + 1) in the label buffer and the seeds listed -- the
 // spots image is never written or re-read.  Every voxel's seg and label entry
 // is written.
+// ROWS output rows per thread (the window holds ROWS + 2), so rows are read
+// (ROWS + 2) / ROWS times.  Row offsets inside a plane and their validity are
+// computed once; per plane only the plane's base moves.  Every owned voxel's
+// seg and label entry is written.
+template <int ROWS>
 __global__ void __launch_bounds__(32 * kGroups)
 maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr32, Geo g, int zchunk,
                     uint8_t *__restrict__ seg, uint32_t *__restrict__ lab, uint32_t *__restrict__ seeds,
                     uint32_t *__restrict__ d_count) {
+    constexpr int kRows = ROWS, kWin = ROWS + 2;
     const int D = (int)g.D, H = (int)g.H, W = (int)g.W;
+    const uint32_t HW = g.H * g.W;
     const int lane = threadIdx.x;
     const int x = (int)blockIdx.x * kOutX + lane - 1;
     const int y0 = ((int)blockIdx.y * kGroups + threadIdx.y) * kRows;
@@ -112,35 +119,40 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
     const bool own = lane >= 1 && lane <= kOutX && xin;
     const float NEG = -INFINITY;
     const float t = *d_thr32;
-
-    auto load = [&](int z, int j) -> float {
-        int y = y0 - 1 + j;
-        if (!xin || z < 0 || z >= D || y < 0 || y >= H) return NEG;
-        return T[((int64_t)z * H + y) * W + x];
+    uint32_t roff[kWin];
+    bool rok[kWin];
+#pragma unroll
+    for (int j = 0; j < kWin; ++j) {
+        const int y = y0 - 1 + j;
+        rok[j] = xin && y >= 0 && y < H;
+        roff[j] = rok[j] ? (uint32_t)y * g.W + (uint32_t)x : 0u;
+    }
+    auto load_plane = [&](int z, float *v) {
+        const bool zok = z >= 0 && z < D;
+        const float *P = T + (size_t)(zok ? z : 0) * HW;
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) v[j] = (zok && rok[j]) ? P[roff[j]] : NEG;
     };
 
     float vm[kWin], vc[kWin], vp[kWin];
-#pragma unroll
-    for (int j = 0; j < kWin; ++j) {
-        vm[j] = load(z0 - 1, j);
-        vc[j] = load(z0, j);
-    }
+    load_plane(z0 - 1, vm);
+    load_plane(z0, vc);
     for (int z = z0; z < z1; ++z) {
-#pragma unroll
-        for (int j = 0; j < kWin; ++j) vp[j] = load(z + 1, j);
+        load_plane(z + 1, vp);
         float Tm[kWin];
 #pragma unroll
         for (int j = 0; j < kWin; ++j) Tm[j] = fmaxf(fmaxf(vm[j], vc[j]), vp[j]);
         float S[kRows];
 #pragma unroll
         for (int j = 0; j < kRows; ++j) S[j] = fmaxf(fmaxf(Tm[j], Tm[j + 1]), Tm[j + 2]);
+        const uint32_t zoff = (uint32_t)z * HW;
 #pragma unroll
         for (int j = 0; j < kRows; ++j) {
             const float sl = __shfl_up_sync(0xffffffffu, S[j], 1);
             const float sr = __shfl_down_sync(0xffffffffu, S[j], 1);
-            const int y = y0 + j;
-            const bool mine = own && y < H;
+            const bool mine = own && rok[j + 1];
             bool seed = false;
+            const uint32_t m = zoff + roff[j + 1];
             if (mine) {
                 const float v = vc[j + 1];
                 const float A = fmaxf(fmaxf(sl, Tm[j]), vm[j + 1]);
@@ -155,9 +167,8 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
                 }
                 const bool sg = v > t;
                 seed = sg && win;
-                const int64_t m = ((int64_t)z * H + y) * W + x;
                 seg[m] = sg ? 1 : 0;
-                lab[m] = seed ? xyz2k(g, (uint32_t)x, (uint32_t)y, (uint32_t)z) + 1u : 0u;
+                lab[m] = seed ? xyz2k(g, (uint32_t)x, (uint32_t)(y0 + j), (uint32_t)z) + 1u : 0u;
             }
             const unsigned b = __ballot_sync(0xffffffffu, seed);
             if (b) {
@@ -165,7 +176,7 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
                 const int leader = __ffs(b) - 1;
                 if (lane == leader) base = atomicAdd(d_count, (uint32_t)__popc(b));
                 base = __shfl_sync(0xffffffffu, base, leader);
-                if (seed) seeds[base + __popc(b & ((1u << lane) - 1u))] = (uint32_t)(((int64_t)z * H + y) * W + x);
+                if (seed) seeds[base + __popc(b & ((1u << lane) - 1u))] = m;
             }
         }
 #pragma unroll
@@ -178,10 +189,10 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
 
 // Grid of the z-marching kernels: 30 columns per warp, kGroups x kRows rows
 // per block, z chunks so that about 12 blocks per SM are launched.
-int maxima_grid(const Img &src, dim3 &grid, int &zchunk) {
+int maxima_grid(const Img &src, dim3 &grid, int &zchunk, int rows = kRows) {
     const int D = (int)src.D, H = (int)src.H, W = (int)src.W;
     const int gx = (W + kOutX - 1) / kOutX;
-    const int gy = (H + kRows * kGroups - 1) / (kRows * kGroups);
+    const int gy = (H + rows * kGroups - 1) / (rows * kGroups);
     int dev = 0;
     cudaGetDevice(&dev);
     const int64_t target = (int64_t)num_sms(dev) * 12;   // blocks
@@ -223,11 +234,12 @@ int maxima_dst(const Img &src, const Img &dst, cudaStream_t st) {
 int maxima_seeds(const Img &T, const float *d_thr32, uint8_t *seg, uint32_t *lab, uint32_t *seeds,
                  uint32_t *d_count, cudaStream_t st) {
     if (T.dtype != CLE_F32) { set_error("internal: maxima_seeds needs a float32 image"); return CLE_ERR_DTYPE; }
+    constexpr int kSeedRows = 8;
     dim3 grid;
     int zchunk = 1;
-    CLE_TRY(maxima_grid(T, grid, zchunk));
-    maxima_seeds_kernel<<<grid, dim3(32, kGroups), 0, st>>>((const float *)T.data, d_thr32, make_geo(T), zchunk,
-                                                           seg, lab, seeds, d_count);
+    CLE_TRY(maxima_grid(T, grid, zchunk, kSeedRows));
+    maxima_seeds_kernel<kSeedRows><<<grid, dim3(32, kGroups), 0, st>>>((const float *)T.data, d_thr32, make_geo(T),
+                                                                     zchunk, seg, lab, seeds, d_count);
     CLE_LAUNCH_CHECK("detect_maxima + seeds");
     return CLE_OK;
 }

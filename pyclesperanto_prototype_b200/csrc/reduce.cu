@@ -148,6 +148,43 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
     const int64_t z1 = min(D, z0 + zchunk);
     uint32_t *mine = sh + (priv ? (threadIdx.x >> 5) * bins : 0);
     const unsigned lane = threadIdx.x & 31;
+    auto count = [&](int b) {
+        // warp-aggregated increment: one shared atomic per distinct bin
+        unsigned peers = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && (__ffs(peers) - 1) == (int)lane) atomicAdd(&mine[b], (uint32_t)__popc(peers));
+    };
+    auto bin_of = [&](float x) {
+        return fast ? hist_bin_fast(x, mn, range, rr, bm1, bins) : hist_bin(x, mn, range, bm1, bins);
+    };
+    if constexpr (std::is_same<T, float>::value) {
+        if ((W & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+            // float rows of a multiple of 4: 128-bit loads, 2 per thread per
+            // round, all issued before the binning
+            const uint32_t W4 = (uint32_t)(W >> 2);
+            const uint32_t span4 = (uint32_t)((z1 - z0) * W4);
+            for (uint32_t base = 0; base < span4; base += 2 * kHistThreads) {
+                float4 q[2];
+                bool ok[2];
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const uint32_t j = base + k * kHistThreads + threadIdx.x;
+                    ok[k] = j < span4;
+                    const uint32_t zz = j / W4, x4 = j - zz * W4;
+                    q[k] = ok[k] ? __ldg(reinterpret_cast<const float4 *>(src + ((z0 + zz) * H + y) * W) + x4)
+                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    count(ok[k] ? bin_of(q[k].x) : -1);
+                    count(ok[k] ? bin_of(q[k].y) : -1);
+                    count(ok[k] ? bin_of(q[k].z) : -1);
+                    count(ok[k] ? bin_of(q[k].w) : -1);
+                }
+            }
+            goto merge;
+        }
+    }
+    {
     // the block's voxels, (z0..z1) x W, visited 4 per thread per round with
     // all loads issued before the binning
     const uint32_t span = (uint32_t)((z1 - z0) * W);
@@ -162,14 +199,10 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
             v[k] = ok[k] ? to_f32(src[((z0 + zz) * H + y) * W + xx]) : 0.0f;
         }
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            int b = !ok[k] ? -1 : (fast ? hist_bin_fast(v[k], mn, range, rr, bm1, bins)
-                                         : hist_bin(v[k], mn, range, bm1, bins));
-            // warp-aggregated increment: one shared atomic per distinct bin
-            unsigned peers = __match_any_sync(0xffffffffu, b);
-            if (b >= 0 && (__ffs(peers) - 1) == (int)lane) atomicAdd(&mine[b], (uint32_t)__popc(peers));
-        }
+        for (int k = 0; k < 4; ++k) count(!ok[k] ? -1 : bin_of(v[k]));
     }
+    }
+merge:
     __syncthreads();
     for (int b = threadIdx.x; b < bins; b += kHistThreads) {
         uint32_t c = 0;
