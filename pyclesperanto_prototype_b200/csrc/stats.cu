@@ -2,16 +2,18 @@
 // (_tier9/_statistics_of_labelled_pixels.py:7-293, kernels
 // _tier9/statistics_per_label_x.cl:1-146, _tier9/standard_deviation_per_label_x.cl:1-96).
 //
-// Two passes over (labels, intensity), as in the reference (the second needs
-// the per-label centroid, mass centre and mean).  A warp covers 32
-// consecutive voxels of one x-row, so y and z are warp-uniform; each run of
-// equal labels along x contributes count, x-sum and bbox in closed form and
-// the intensity fields through a segmented shuffle scan; the run's last lane
-// adds them to per-label accumulators (exact integers for coordinates,
-// float64 for intensity products, order-preserving int atomics for min/max).
-// The finalise kernels apply the reference's float32 column arithmetic and
-// its sentinels for labels absent from the image (min FLT_MAX, max -FLT_MAX,
-// sums 0, 0/0 = NaN).
+// Sorted-segment reductions: the labelled voxels are first put in label order
+// (a count per label, an exclusive scan into offsets, a scatter of voxel
+// indices), then warps sweep the sorted index array, each keeping per-lane
+// accumulators of the label at hand and adding them to the per-label
+// accumulators once the label changes -- a few atomics per label instead of
+// one set per row run.  Two sweeps, as in the reference (the second needs the
+// per-label centroid, mass centre and mean).  Coordinates and 8/16-bit
+// intensities are summed in exact 64-bit integers, other intensities in
+// float64; min / max through order-preserving integer atomics.  The finalise
+// kernels apply the reference's float32 column arithmetic and its sentinels
+// for labels absent from the image (min FLT_MAX, max -FLT_MAX, sums 0,
+// 0/0 = NaN).
 #include <cfloat>
 
 #include "common.cuh"
@@ -22,7 +24,8 @@ namespace cle {
 namespace {
 
 constexpr int kST = 256;
-constexpr int kBatch = 4;   // row segments per warp round
+constexpr int kChunk = 4096;   // sorted positions per warp in a sweep
+constexpr int kScanTile = 4096;  // labels per block of the offset scan
 
 struct Acc1 {
     uint32_t *cnt;
@@ -100,160 +103,391 @@ __device__ __forceinline__ uint32_t lab_of(T v) {
     else return (uint32_t)v;
 }
 
-struct Seg {
-    int lane, hl;
-    bool tail;
-    __device__ __forceinline__ double scan_add(double v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            double t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v += t;
-        }
-        return v;
-    }
-    __device__ __forceinline__ float scan_min(float v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            float t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v = fminf(v, t);
-        }
-        return v;
-    }
-    __device__ __forceinline__ float scan_max(float v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            float t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v = fmaxf(v, t);
-        }
-        return v;
-    }
-    __device__ __forceinline__ uint32_t scan_addu(uint32_t v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v += t;
-        }
-        return v;
-    }
-    __device__ __forceinline__ uint32_t scan_minu(uint32_t v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v = min(v, t);
-        }
-        return v;
-    }
-    __device__ __forceinline__ uint32_t scan_maxu(uint32_t v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v = max(v, t);
-        }
-        return v;
-    }
-    __device__ __forceinline__ double scan_maxd(double v) const {
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            double t = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane - o >= hl) v = fmax(v, t);
-        }
-        return v;
-    }
+// Label-sorted voxel indices and the per-label counts / offsets / cursors.
+struct Sorted {
+    uint32_t *cnt, *off, *cursor, *tsum, *sorted;
 };
 
-__device__ __forceinline__ Seg make_seg(uint32_t l) {
-    Seg s;
-    s.lane = threadIdx.x & 31;
-    const uint32_t lp = __shfl_up_sync(0xffffffffu, l, 1);
-    const bool head = (s.lane == 0) || (l != lp);
-    const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const unsigned upto = (s.lane == 31) ? 0xffffffffu : ((2u << s.lane) - 1u);
-    s.hl = 31 - __clz(heads & upto);
-    s.tail = (s.lane == 31) || ((heads >> (s.lane + 1)) & 1u);
+Sorted take_sorted(Arena &a, const Img &labels, int64_t L) {
+    Sorted s;
+    s.cnt = a.take<uint32_t>(L);
+    s.off = a.take<uint32_t>(L + 1);
+    s.cursor = a.take<uint32_t>(L);
+    s.tsum = a.take<uint32_t>((L + kScanTile - 1) / kScanTile + 1);
+    s.sorted = a.take<uint32_t>(labels.n());
     return s;
 }
 
-// 4 CTAs per SM (64 registers): more loads in flight for the latency-bound scan
-template <typename TL, typename TI>
-__global__ void __launch_bounds__(kST, 4)
-stats_pass1(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t Lcap, Acc1 a, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
-    const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
+__device__ __forceinline__ void m2xyz_fd(const FastDiv &fW, const FastDiv &fH, uint32_t m, uint32_t &x,
+                                         uint32_t &y, uint32_t &z) {
+    const uint32_t r = fW.div(m);
+    x = m - r * fW.d;
+    z = fH.div(r);
+    y = r - z * fH.d;
+}
+
+// Run of equal labels along x inside a warp's 32 voxels: head lane, and
+// whether this lane ends its run.
+struct Run {
+    int head;
+    bool tail;
+};
+
+__device__ __forceinline__ Run make_run(uint32_t l) {
     const int lane = threadIdx.x & 31;
-    const uint32_t chunks = (uint32_t)((W + 31) / 32);
-    const uint32_t tasks = (uint32_t)(D * H) * chunks;
+    const uint32_t lp = __shfl_up_sync(0xffffffffu, l, 1);
+    const bool hd = (lane == 0) || (l != lp);
+    const unsigned heads = __ballot_sync(0xffffffffu, hd);
+    const unsigned upto = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+    Run r;
+    r.head = 31 - __clz(heads & upto);
+    r.tail = (lane == 31) || ((heads >> (lane + 1)) & 1u);
+    return r;
+}
+
+// Label of one voxel, 0 for background and for labels above the live count.
+template <typename TL>
+__device__ __forceinline__ uint32_t live_label(const TL *lab, int64_t m, int64_t L) {
+    const uint32_t l = lab_of(lab[m]);
+    return (l > (uint32_t)L) ? 0u : l;
+}
+
+constexpr int kBatch = 4;   // row segments per warp round (loads in flight)
+
+// Pass A: voxels per label (one atomic per row run).  A warp takes 32 voxels
+// of one row at a time, kBatch row segments per round with every load issued
+// before its use.
+template <typename TL>
+__global__ void __launch_bounds__(kST)
+count_kernel(const TL *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fc, int64_t Lcap,
+             const uint32_t *__restrict__ d_L, uint32_t *__restrict__ cnt) {
+    const int64_t L = live_labels(Lcap, d_L);
+    const int lane = threadIdx.x & 31;
+    const uint32_t chunks = fc.d;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    // kBatch row segments per round: every load is issued before its use
     for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
         uint32_t lb[kBatch];
-        float vb[kBatch];
 #pragma unroll
         for (int k = 0; k < kBatch; ++k) {
-            const uint32_t t = t0 + k * nwarps;
-            const uint32_t row = fc.div(t);
-            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
-            const uint32_t l = (t < tasks && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
-            lb[k] = (l > (uint32_t)L) ? 0u : l;
+            const uint32_t t = t0 + (uint32_t)k * nwarps;
+            const uint32_t row = fc.div(t), x = (t - row * chunks) * 32u + (uint32_t)lane;
+            lb[k] = (t < tasks && x < W) ? live_label(lab, (int64_t)row * W + x, L) : 0u;
         }
 #pragma unroll
         for (int k = 0; k < kBatch; ++k) {
-            const uint32_t t = t0 + k * nwarps;
-            const uint32_t row = fc.div(t);
-            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
-            vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
+            const uint32_t l = lb[k];
+            if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+            const Run r = make_run(l);
+            if (r.tail && l) atomicAdd(cnt + (l - 1), (uint32_t)(lane - r.head + 1));
+        }
+    }
+}
+
+// Offsets: exclusive scan of the counts (tiles of kScanTile labels: tile sums,
+// a one-CTA scan of the tile sums, then each tile's scan); cursor = offset;
+// off[L] = total.
+__global__ void __launch_bounds__(kST)
+tile_sum_kernel(const uint32_t *__restrict__ cnt, int64_t Lcap, const uint32_t *__restrict__ d_L,
+                uint32_t *__restrict__ tsum) {
+    __shared__ uint32_t red[kST / 32];
+    const int64_t L = live_labels(Lcap, d_L);
+    const int64_t b0 = (int64_t)blockIdx.x * kScanTile;
+    uint32_t s = 0;
+    for (int64_t i = b0 + threadIdx.x; i < min(b0 + kScanTile, L); i += kST) s += cnt[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < kST / 32; ++w) t += red[w];
+        tsum[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+tile_scan_kernel(uint32_t *__restrict__ tsum, int64_t ntiles) {
+    __shared__ uint32_t s_w[32];
+    __shared__ uint32_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t base = 0; base < ntiles; base += 1024) {
+        const int64_t i = base + threadIdx.x;
+        const uint32_t v = i < ntiles ? tsum[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_w[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = s_w[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            s_w[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t excl = s_carry + (warp ? s_w[warp - 1] : 0u) + x - v;
+        if (i < ntiles) tsum[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += s_w[31];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kST)
+offset_kernel(const uint32_t *__restrict__ cnt, int64_t Lcap, const uint32_t *__restrict__ d_L,
+              const uint32_t *__restrict__ tsum, uint32_t *__restrict__ off, uint32_t *__restrict__ cursor) {
+    __shared__ uint32_t s_w[kST / 32];
+    __shared__ uint32_t s_carry;
+    const int64_t L = live_labels(Lcap, d_L);
+    const int64_t b0 = (int64_t)blockIdx.x * kScanTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_carry = tsum[blockIdx.x];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && L == 0) off[0] = 0u;   // no live label: empty sweep
+    __syncthreads();
+    for (int64_t base = b0; base < min(b0 + kScanTile, L); base += kST) {
+        const int64_t i = base + threadIdx.x;
+        const uint32_t v = i < L ? cnt[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_w[warp] = x;
+        __syncthreads();
+        uint32_t before = s_carry;
+        for (int w = 0; w < warp; ++w) before += s_w[w];
+        const uint32_t excl = before + x - v;
+        if (i < L) {
+            off[i] = excl;
+            cursor[i] = excl;
+            if (i == L - 1) off[L] = excl + v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (int w = 0; w < kST / 32; ++w) t += s_w[w];
+            s_carry += t;
+        }
+        __syncthreads();
+    }
+}
+
+// Pass B: each run reserves its place in its label's range (one atomic per
+// run) and its lanes write their voxel indices there.
+template <typename TL>
+__global__ void __launch_bounds__(kST)
+scatter_kernel(const TL *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fc, int64_t Lcap,
+               const uint32_t *__restrict__ d_L, uint32_t *__restrict__ cursor, uint32_t *__restrict__ sorted) {
+    const int64_t L = live_labels(Lcap, d_L);
+    const int lane = threadIdx.x & 31;
+    const uint32_t chunks = fc.d;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch], mb[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + (uint32_t)k * nwarps;
+            const uint32_t row = fc.div(t), x = (t - row * chunks) * 32u + (uint32_t)lane;
+            mb[k] = row * W + x;
+            lb[k] = (t < tasks && x < W) ? live_label(lab, (int64_t)mb[k], L) : 0u;
         }
 #pragma unroll
         for (int k = 0; k < kBatch; ++k) {
-        const uint32_t l = lb[k];
-        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
-        const uint32_t t = t0 + k * nwarps;
-        const uint32_t row = fc.div(t);
-        const uint32_t c = t - row * chunks;
-        const int64_t x = (int64_t)c * 32 + lane;
-        const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
-        const float v = vb[k];
-        const Seg s = make_seg(l);
-        double ssum, ssx;
-        float smin, smax;
-        if constexpr (sizeof(TI) <= 2) {
-            // 8/16-bit intensities: exact uint32 scans of v and v * lane
-            // (at most 32 * 65535 * 31 < 2^32), x = 32 c + lane
-            const uint32_t iv = (uint32_t)v;
-            const uint32_t su = s.scan_addu(iv);
-            const uint32_t sl = s.scan_addu(iv * (uint32_t)lane);
-            ssum = (double)su;
-            ssx = (double)su * (double)(c * 32u) + (double)sl;
-            smin = (float)s.scan_minu(iv);
-            smax = (float)s.scan_maxu(iv);
+            const uint32_t l = lb[k];
+            if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+            const Run r = make_run(l);
+            uint32_t pos = 0;
+            if (r.tail && l) pos = atomicAdd(cursor + (l - 1), (uint32_t)(lane - r.head + 1));
+            // the run's tail lane holds its base: the first tail at or after this lane
+            const unsigned tails = __ballot_sync(0xffffffffu, r.tail);
+            const int tl = __ffs(tails >> lane) - 1 + lane;
+            const uint32_t base = __shfl_sync(0xffffffffu, pos, tl);
+            if (l) sorted[base + (uint32_t)(lane - r.head)] = mb[k];
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Per-lane accumulators of pass 1 for the label at hand.
+template <bool INT>
+struct Lane1 {
+    uint32_t cnt;
+    unsigned long long sx, sy, sz;
+    unsigned long long iv, ivx, ivy, ivz;   // 8/16-bit intensities: exact
+    double dv, dvx, dvy, dvz;               // others
+    int vmin, vmax;
+    uint32_t x0, x1, y0, y1, z0, z1;
+    __device__ __forceinline__ void reset() {
+        cnt = 0;
+        sx = sy = sz = 0ull;
+        iv = ivx = ivy = ivz = 0ull;
+        dv = dvx = dvy = dvz = 0.0;
+        vmin = 0x7FFFFFFF;
+        vmax = (int)0x80000000;
+        x0 = y0 = z0 = 0xFFFFFFFFu;
+        x1 = y1 = z1 = 0u;
+    }
+    __device__ __forceinline__ void add(uint32_t x, uint32_t y, uint32_t z, float v) {
+        ++cnt;
+        sx += x; sy += y; sz += z;
+        if constexpr (INT) {
+            const unsigned long long u = (unsigned long long)v;
+            iv += u; ivx += u * x; ivy += u * y; ivz += u * z;
         } else {
-            const double dv = (double)v;
-            ssum = s.scan_add(dv);
-            ssx = s.scan_add(dv * (double)x);
-            smin = s.scan_min(l ? v : INFINITY);
-            smax = s.scan_max(l ? v : -INFINITY);
+            const double d = (double)v;
+            dv += d; dvx += d * (double)x; dvy += d * (double)y; dvz += d * (double)z;
         }
-        if (s.tail && l) {
+        const int o = f2ord(v);
+        vmin = min(vmin, o); vmax = max(vmax, o);
+        x0 = min(x0, x); x1 = max(x1, x);
+        y0 = min(y0, y); y1 = max(y1, y);
+        z0 = min(z0, z); z1 = max(z1, z);
+    }
+    // warp-wide: the label's totals over the lanes, added by lane 0
+    __device__ __forceinline__ void flush(const Acc1 &a, uint32_t l) {
+        const uint32_t c = warp_sum(cnt);
+        const unsigned long long Sx = warp_sum(sx), Sy = warp_sum(sy), Sz = warp_sum(sz);
+        double Sv, Svx, Svy, Svz;
+        if constexpr (INT) {
+            // exact: per-label totals stay far below 2^53
+            Sv = (double)warp_sum(iv); Svx = (double)warp_sum(ivx);
+            Svy = (double)warp_sum(ivy); Svz = (double)warp_sum(ivz);
+        } else {
+            Sv = warp_sum(dv); Svx = warp_sum(dvx); Svy = warp_sum(dvy); Svz = warp_sum(dvz);
+        }
+        const int mn = warp_min(vmin), mx = warp_max(vmax);
+        const uint32_t X0 = warp_min(x0), X1 = warp_max(x1), Y0 = warp_min(y0), Y1 = warp_max(y1);
+        const uint32_t Z0 = warp_min(z0), Z1 = warp_max(z1);
+        if ((threadIdx.x & 31) == 0 && c) {
             const uint32_t i = l - 1;
-            const uint32_t cnt = (uint32_t)(s.lane - s.hl + 1);
-            const uint32_t xh = (uint32_t)(c * 32 + s.hl), xt = (uint32_t)x;
-            atomicAdd(a.cnt + i, cnt);
-            atomicAdd(a.sx + i, (unsigned long long)(xh + xt) * cnt / 2ull);
-            atomicAdd(a.sy + i, (unsigned long long)y * cnt);
-            atomicAdd(a.sz + i, (unsigned long long)z * cnt);
-            atomicAdd(a.sv + i, ssum);
-            atomicAdd(a.svx + i, ssx);
-            atomicAdd(a.svy + i, ssum * (double)y);
-            atomicAdd(a.svz + i, ssum * (double)z);
-            atomicMin(a.vmin + i, f2ord(smin));
-            atomicMax(a.vmax + i, f2ord(smax));
-            atomicMin(a.xmin + i, xh);
-            atomicMax(a.xmax + i, xt);
-            atomicMin(a.ymin + i, (uint32_t)y);
-            atomicMax(a.ymax + i, (uint32_t)y);
-            atomicMin(a.zmin + i, (uint32_t)z);
-            atomicMax(a.zmax + i, (uint32_t)z);
+            atomicAdd(a.cnt + i, c);
+            atomicAdd(a.sx + i, Sx); atomicAdd(a.sy + i, Sy); atomicAdd(a.sz + i, Sz);
+            atomicAdd(a.sv + i, Sv); atomicAdd(a.svx + i, Svx); atomicAdd(a.svy + i, Svy); atomicAdd(a.svz + i, Svz);
+            atomicMin(a.vmin + i, mn); atomicMax(a.vmax + i, mx);
+            atomicMin(a.xmin + i, X0); atomicMax(a.xmax + i, X1);
+            atomicMin(a.ymin + i, Y0); atomicMax(a.ymax + i, Y1);
+            atomicMin(a.zmin + i, Z0); atomicMax(a.zmax + i, Z1);
         }
+        reset();
+    }
+};
+
+// Per-lane accumulators of pass 2 for the label at hand.
+struct Lane2 {
+    double sdc, sdm, ssq;
+    float mdc, mdm;
+    __device__ __forceinline__ void reset() { sdc = sdm = ssq = 0.0; mdc = mdm = 0.0f; }
+    __device__ __forceinline__ void flush(const Acc2 &b, uint32_t l) {
+        const double Sdc = warp_sum(sdc), Sdm = warp_sum(sdm), Ssq = warp_sum(ssq);
+        const float Mdc = warp_max(mdc), Mdm = warp_max(mdm);
+        if ((threadIdx.x & 31) == 0) {
+            const uint32_t i = l - 1;
+            atomicAdd(b.sdc + i, Sdc);
+            atomicAdd(b.sdm + i, Sdm);
+            atomicAdd(b.ssq + i, Ssq);
+            atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong((double)Mdc));
+            atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong((double)Mdm));
+        }
+        reset();
+    }
+};
+
+// Sweeps: each warp takes kChunk consecutive positions of the sorted array
+// (labels in order), 32 per round; lanes add their voxels to the accumulators
+// of the warp's current label, which are flushed when the label changes.
+template <int PASS, typename TL, typename TI>
+__global__ void __launch_bounds__(kST)
+sweep_kernel(const TL *__restrict__ lab, const TI *__restrict__ inten, const uint32_t *__restrict__ sorted,
+             const uint32_t *__restrict__ off, int64_t Lcap, const uint32_t *__restrict__ d_L, FastDiv fW,
+             FastDiv fH, Acc1 a, Acc2 b) {
+    constexpr bool INT = sizeof(TI) <= 2 && !std::is_floating_point<TI>::value;
+    const int64_t L = live_labels(Lcap, d_L);
+    const uint32_t total = off[L];
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    Lane1<INT> A;
+    Lane2 B;
+    A.reset();
+    B.reset();
+    for (uint32_t c0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (uint32_t)kChunk; c0 < total;
+         c0 += nwarps * (uint32_t)kChunk) {
+        const uint32_t c1 = min(total, c0 + (uint32_t)kChunk);
+        uint32_t cur = 0;
+        float4 pc = make_float4(0.f, 0.f, 0.f, 0.f), pm = pc;
+        for (uint32_t p = c0 + lane; p - lane < c1; p += 32) {
+            const bool valid = p < c1;
+            const uint32_t m = valid ? sorted[p] : 0u;
+            const uint32_t l = valid ? lab_of(lab[m]) : 0xFFFFFFFFu;
+            const float v = valid ? to_f32(inten[m]) : 0.0f;
+            uint32_t x = 0, y = 0, z = 0;
+            if (valid) m2xyz_fd(fW, fH, m, x, y, z);
+            unsigned todo = __ballot_sync(0xffffffffu, valid);
+            while (todo) {
+                const uint32_t g = __shfl_sync(0xffffffffu, l, __ffs(todo) - 1);
+                if (g != cur) {
+                    if (cur) {
+                        if constexpr (PASS == 1) A.flush(a, cur);
+                        else B.flush(b, cur);
+                    }
+                    cur = g;
+                    if constexpr (PASS == 2) { pc = b.pc[cur - 1]; pm = b.pm[cur - 1]; }
+                }
+                const bool mine = valid && l == g;
+                if (mine) {
+                    if constexpr (PASS == 1) {
+                        A.add(x, y, z, v);
+                    } else {
+                        // distances in float32 (relative error a few 1e-7), their
+                        // sums and the squared deviations in float64; the squared
+                        // deviations are divided by the area once per label
+                        const float xf = (float)x, yf = (float)y, zf = (float)z;
+                        const float ex = xf - pc.x, ey = yf - pc.y, ez = zf - pc.z;
+                        const float fx = xf - pm.x, fy = yf - pm.y, fz = zf - pm.z;
+                        const float dc = sqrtf(ex * ex + ey * ey + ez * ez);
+                        const float dm = sqrtf(fx * fx + fy * fy + fz * fz);
+                        const double dv = (double)v - (double)pc.w;
+                        B.sdc += (double)dc;
+                        B.sdm += (double)dm;
+                        B.ssq += dv * dv;
+                        B.mdc = fmaxf(B.mdc, dc);
+                        B.mdm = fmaxf(B.mdm, dm);
+                    }
+                }
+                todo &= ~__ballot_sync(0xffffffffu, mine);
+            }
+        }
+        if (cur) {
+            if constexpr (PASS == 1) A.flush(a, cur);
+            else B.flush(b, cur);
         }
     }
 }
@@ -306,78 +540,6 @@ __global__ void stats_final1(Acc1 a, Acc2 b, int64_t L, float *__restrict__ T, c
     }
 }
 
-template <typename TL, typename TI>
-__global__ void __launch_bounds__(kST)
-stats_pass2(const TL *__restrict__ lab, const TI *__restrict__ inten, int64_t D, int64_t H,
-            int64_t W, int64_t Lcap, Acc2 b, FastDiv fc, FastDiv fh, const uint32_t *__restrict__ d_L) {
-    const int64_t L = d_L ? ((int64_t)*d_L < Lcap ? (int64_t)*d_L : Lcap) : Lcap;
-    const int lane = threadIdx.x & 31;
-    const uint32_t chunks = (uint32_t)((W + 31) / 32);
-    const uint32_t tasks = (uint32_t)(D * H) * chunks;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    // kBatch row segments per round: every load is issued before its use
-    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
-        uint32_t lb[kBatch];
-        float vb[kBatch];
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-            const uint32_t t = t0 + k * nwarps;
-            const uint32_t row = fc.div(t);
-            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
-            const uint32_t l = (t < tasks && x < W) ? lab_of(lab[(int64_t)row * W + x]) : 0u;
-            lb[k] = (l > (uint32_t)L) ? 0u : l;
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-            const uint32_t t = t0 + k * nwarps;
-            const uint32_t row = fc.div(t);
-            const int64_t x = (int64_t)(t - row * chunks) * 32 + lane;
-            vb[k] = lb[k] ? to_f32(inten[(int64_t)row * W + x]) : 0.0f;
-        }
-#pragma unroll
-        for (int k = 0; k < kBatch; ++k) {
-        const uint32_t l = lb[k];
-        if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
-        const uint32_t t = t0 + k * nwarps;
-        const uint32_t row = fc.div(t);
-        const uint32_t c = t - row * chunks;
-        const int64_t x = (int64_t)c * 32 + lane;
-        const uint32_t z = fh.div(row), y = row - z * (uint32_t)H;
-        // distances in float32 (relative error a few 1e-7), their sums and the
-        // squared deviations in float64; the squared deviations are divided
-        // by the area once per label
-        float dc = 0.0f, dm = 0.0f;
-        double sq = 0.0;
-        if (l) {
-            const uint32_t i = l - 1;
-            const float4 pc = b.pc[i], pm = b.pm[i];
-            const float xf = (float)x, yf = (float)y, zf = (float)z;
-            const float ex = xf - pc.x, ey = yf - pc.y, ez = zf - pc.z;
-            const float fx = xf - pm.x, fy = yf - pm.y, fz = zf - pm.z;
-            dc = sqrtf(ex * ex + ey * ey + ez * ez);
-            dm = sqrtf(fx * fx + fy * fy + fz * fz);
-            const double dv = (double)vb[k] - (double)pc.w;
-            sq = dv * dv;
-        }
-        const Seg s = make_seg(l);
-        const double sdc = s.scan_add((double)dc);
-        const double sdm = s.scan_add((double)dm);
-        const double ssq = s.scan_add(sq);
-        const float mdc = s.scan_max(dc);
-        const float mdm = s.scan_max(dm);
-        if (s.tail && l) {
-            const uint32_t i = l - 1;
-            atomicAdd(b.sdc + i, sdc);
-            atomicAdd(b.sdm + i, sdm);
-            atomicAdd(b.ssq + i, ssq);
-            atomicMax(b.mdc + i, (unsigned long long)__double_as_longlong((double)mdc));
-            atomicMax(b.mdm + i, (unsigned long long)__double_as_longlong((double)mdm));
-        }
-        }
-    }
-}
-
 __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T, const uint32_t *__restrict__ d_L) {
     const int64_t n = live_labels(L, d_L);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -399,44 +561,56 @@ __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T, const uin
 }
 
 template <typename TL, typename TI>
-int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a,
-                const Acc2 &b, cudaStream_t st, const uint32_t *d_L) {
-    const int64_t tasks = lab.D * lab.H * ((lab.W + 31) / 32);
+int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a, const Acc2 &b,
+                const Sorted &so, cudaStream_t st, const uint32_t *d_L) {
+    const int64_t rows = lab.D * lab.H;
+    const int64_t tasks = rows * ((lab.W + 31) / 32);
     const int blocks = launch_blocks(tasks * 32, kST, 8);
-    const FastDiv fc((uint32_t)((lab.W + 31) / 32)), fh((uint32_t)lab.H);
+    const int64_t ntiles = (L + kScanTile - 1) / kScanTile;
+    // sweeps: enough warps for every chunk of the worst case (all voxels labelled)
+    const int sweep_blocks = launch_blocks((lab.n() + kChunk - 1) / kChunk * 32, kST, 8);
+    const FastDiv fW((uint32_t)lab.W), fH((uint32_t)lab.H);
     stage_mark(8, st);
-    stats_pass1<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, a, fc, fh, d_L);
+    const FastDiv fc((uint32_t)((lab.W + 31) / 32));
+    count_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L, so.cnt);
+    tile_sum_kernel<<<(unsigned)ntiles, kST, 0, st>>>(so.cnt, L, d_L, so.tsum);
+    tile_scan_kernel<<<1, 1024, 0, st>>>(so.tsum, ntiles);
+    offset_kernel<<<(unsigned)ntiles, kST, 0, st>>>(so.cnt, L, d_L, so.tsum, so.off, so.cursor);
+    scatter_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L,
+                                               so.cursor, so.sorted);
+    sweep_kernel<1, TL, TI><<<sweep_blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, so.sorted,
+                                                          so.off, L, d_L, fW, fH, a, b);
     stage_mark(9, st);
     stats_final1<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, T, d_L);
     stage_mark(10, st);
-    stats_pass2<TL, TI><<<blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, lab.D,
-                                                lab.H, lab.W, L, b, fc, fh, d_L);
+    sweep_kernel<2, TL, TI><<<sweep_blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, so.sorted,
+                                                          so.off, L, d_L, fW, fH, a, b);
     stage_mark(11, st);
     stats_final2<<<launch_blocks(L, 256), 256, 0, st>>>(b, L, T, d_L);
     stage_mark(12, st);
-    CLE_LAUNCH_CHECK_N("statistics", 4);
+    CLE_LAUNCH_CHECK_N("statistics", 9);
     return CLE_OK;
 }
 
 template <typename TL>
 int stats_i(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a, const Acc2 &b,
-            cudaStream_t st, const uint32_t *d_L) {
+            const Sorted &so, cudaStream_t st, const uint32_t *d_L) {
     switch (inten.dtype) {
-        case CLE_F32: return stats_typed<TL, float>(inten, lab, L, T, a, b, st, d_L);
-        case CLE_U16: return stats_typed<TL, uint16_t>(inten, lab, L, T, a, b, st, d_L);
-        case CLE_U8: return stats_typed<TL, uint8_t>(inten, lab, L, T, a, b, st, d_L);
-        case CLE_U32: return stats_typed<TL, uint32_t>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_F32: return stats_typed<TL, float>(inten, lab, L, T, a, b, so, st, d_L);
+        case CLE_U16: return stats_typed<TL, uint16_t>(inten, lab, L, T, a, b, so, st, d_L);
+        case CLE_U8: return stats_typed<TL, uint8_t>(inten, lab, L, T, a, b, so, st, d_L);
+        case CLE_U32: return stats_typed<TL, uint32_t>(inten, lab, L, T, a, b, so, st, d_L);
         default: set_error("statistics: unsupported intensity dtype %d", inten.dtype); return CLE_ERR_DTYPE;
     }
 }
 
 }  // namespace
 
-size_t stats_workspace_bytes(const Img &, int64_t L) {
+size_t stats_workspace_bytes(const Img &labels, int64_t L) {
     Arena a(nullptr, 0);
     take_acc1(a, L < 1 ? 1 : L);
     take_acc2(a, L < 1 ? 1 : L);
+    take_sorted(a, labels, L < 1 ? 1 : L);
     return a.off;
 }
 
@@ -447,14 +621,16 @@ int statistics(const Img &inten, const Img &lab, int64_t L, float *T, Arena &ws,
     if (L == 0) return CLE_OK;
     Acc1 a = take_acc1(ws, L);
     Acc2 b = take_acc2(ws, L);
+    Sorted so = take_sorted(ws, lab, L);
     if (!ws.ok()) { set_error("statistics: workspace too small"); return CLE_ERR_WORKSPACE; }
     stats_init<<<launch_blocks(L, 256), 256, 0, st>>>(a, b, L, d_L);
     CLE_LAUNCH_CHECK("statistics init");
+    CLE_CUDA(cudaMemsetAsync(so.cnt, 0, sizeof(uint32_t) * (size_t)L, st));
     switch (lab.dtype) {
-        case CLE_U32: return stats_i<uint32_t>(inten, lab, L, T, a, b, st, d_L);
-        case CLE_F32: return stats_i<float>(inten, lab, L, T, a, b, st, d_L);
-        case CLE_U16: return stats_i<uint16_t>(inten, lab, L, T, a, b, st, d_L);
-        case CLE_U8: return stats_i<uint8_t>(inten, lab, L, T, a, b, st, d_L);
+        case CLE_U32: return stats_i<uint32_t>(inten, lab, L, T, a, b, so, st, d_L);
+        case CLE_F32: return stats_i<float>(inten, lab, L, T, a, b, so, st, d_L);
+        case CLE_U16: return stats_i<uint16_t>(inten, lab, L, T, a, b, so, st, d_L);
+        case CLE_U8: return stats_i<uint8_t>(inten, lab, L, T, a, b, so, st, d_L);
         default: set_error("statistics: unsupported label dtype %d", lab.dtype); return CLE_ERR_DTYPE;
     }
 }
