@@ -121,7 +121,9 @@ int cle_profile_trace(void *host, size_t bytes);
  * replaces _tier1/_gaussian_blur.py:6-58 (+ _tier1/_execute_separable_kernel.py:7-76,
  * _tier0/_sigma_to_kernel_size.py:1-4).  src: u8/u16/f32; dst: f32.
  * Kernel size per axis int(8*sigma)|1; sigma <= 0 leaves that axis as is;
- * sigma_z is ignored for 2D images. */
+ * sigma_z is ignored for 2D images.  An isotropic blur of a volume stages
+ * its planes with TMA copies; a copy wait that ran out (2 s) is reported by
+ * cle_workspace_status on the same workspace as CLE_ERR_ITER_LIMIT. */
 size_t cle_gaussian_blur_workspace_bytes(const cle_tensor *src);
 int cle_gaussian_blur(const cle_tensor *src, const cle_tensor *dst, double sigma_x,
                       double sigma_y, double sigma_z, void *workspace, size_t workspace_bytes,

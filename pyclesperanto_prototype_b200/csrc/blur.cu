@@ -177,9 +177,9 @@ int separable_filter(const Img &src, float *dst, const Taps *tx, const Taps *ty,
 }
 
 int gaussian_blur(const Img &src, float *dst, double sx, double sy, double sz, Arena &ws,
-                  cudaStream_t st) {
+                  cudaStream_t st, int *status) {
     if (fused_blur_applies(src, sx, sy, sz))
-        return fused_blur(src, dst, sx, st);
+        return fused_blur(src, dst, sx, st, nullptr, status);
     Taps tx, ty, tz;
     const Taps *px = nullptr, *py = nullptr, *pz = nullptr;
     if (sx > 0) { CLE_TRY(make_gauss_taps(sx, tx)); px = &tx; }

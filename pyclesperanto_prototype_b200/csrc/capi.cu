@@ -56,8 +56,16 @@ int cle_gaussian_blur(const cle_tensor *src, const cle_tensor *dst, double sx, d
     if (b.dtype != CLE_F32) { set_error("gaussian_blur: destination must be float32"); return CLE_ERR_DTYPE; }
     CLE_TRY(ws_check(ws, ws_bytes, separable_workspace_bytes(a), "gaussian_blur"));
     CLE_TRY(set_device_of(a, src));
+    // the fused path of a volume reports a staging wait that ran out in the
+    // workspace's first word (cle_workspace_status); the three-pass path
+    // uses the workspace for its intermediates instead
+    int *status = nullptr;
+    if (a.ndim == 3 && fused_blur_applies(a, sx, sy, sz) && ws && ws_bytes >= sizeof(int)) {
+        status = static_cast<int *>(ws);
+        CLE_CUDA(cudaMemsetAsync(status, 0, sizeof(int), S(stream)));
+    }
     Arena ar(ws, ws_bytes);
-    return gaussian_blur(a, (float *)b.data, sx, sy, sz, ar, S(stream));
+    return gaussian_blur(a, (float *)b.data, sx, sy, sz, ar, S(stream), status);
 }
 
 // ---- min / max -------------------------------------------------------------

@@ -9,18 +9,23 @@ namespace cle {
 size_t separable_workspace_bytes(const Img &im);
 int separable_filter(const Img &src, float *dst, const Taps *tx, const Taps *ty, const Taps *tz,
                      Arena &ws, cudaStream_t st);
+// status (optional): a device status word; given it, the fused path of a
+// volume may stage planes with TMA copies and reports a stage wait that ran
+// out there (CLE_ERR_ITER_LIMIT)
 int gaussian_blur(const Img &src, float *dst, double sx, double sy, double sz, Arena &ws,
-                  cudaStream_t st);
+                  cudaStream_t st, int *status = nullptr);
 
 // blur_fused.cu (isotropic sigma, radius <= kMaxFusedR, one launch)
 constexpr int kMaxFusedR = 14;
 bool fused_blur_applies(const Img &src, double sx, double sy, double sz);
 // mm (optional): 2 floats per CTA, the CTA's min / max of the result
-int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st, float *mm = nullptr);
+int fused_blur(const Img &src, float *dst, double sigma, cudaStream_t st, float *mm = nullptr,
+               int *status = nullptr);
 // Isotropic blur whose {min, max} lands in d_minmax (device): the fused
 // launch's CTA partials and a one-CTA finish, or blur + minmax otherwise.
 size_t blur_minmax_workspace_bytes(const Img &src);
-int blur_minmax(const Img &src, float *dst, double sigma, float *d_minmax, Arena &ws, cudaStream_t st);
+int blur_minmax(const Img &src, float *dst, double sigma, float *d_minmax, Arena &ws, cudaStream_t st,
+                int *status = nullptr);
 
 // reduce.cu
 size_t minmax_workspace_bytes(const Img &im);

@@ -391,8 +391,8 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     // threshold, as the reference's second blur would have recomputed it.
     const bool same_blur = (float)spot_sigma == (float)outline_sigma &&
                            sigma_to_kernel_size(spot_sigma) == sigma_to_kernel_size(outline_sigma);
-    if (same_blur) CLE_TRY(blur_minmax(src, l.T, spot_sigma, l.sc->minmax, ws, st));
-    else CLE_TRY(gaussian_blur(src, l.T, spot_sigma, spot_sigma, spot_sigma, ws, st));
+    if (same_blur) CLE_TRY(blur_minmax(src, l.T, spot_sigma, l.sc->minmax, ws, st, &l.sc->status));
+    else CLE_TRY(gaussian_blur(src, l.T, spot_sigma, spot_sigma, spot_sigma, ws, st, &l.sc->status));
     stage_mark(1, st);
     ws.off = tail_off;
     Img Ti = src;
@@ -406,7 +406,7 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     if (!same_blur) CLE_TRY(detect_maxima(Ti, Si, st));
     stage_mark(2, st);
     // the outline blur also reduces the blurred image's min / max (step 4)
-    if (!same_blur) CLE_TRY(blur_minmax(src, l.T, outline_sigma, l.sc->minmax, ws, st));
+    if (!same_blur) CLE_TRY(blur_minmax(src, l.T, outline_sigma, l.sc->minmax, ws, st, &l.sc->status));
     ws.off = tail_off;
     stage_mark(3, st);
 

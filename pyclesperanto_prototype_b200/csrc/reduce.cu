@@ -159,7 +159,10 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
     if constexpr (std::is_same<T, float>::value) {
         if ((W & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
             // float rows of a multiple of 4: 128-bit loads, 2 per thread per
-            // round, all issued before the binning
+            // round (8 voxels), all issued before the binning.  A lane whose 8
+            // voxels share one bin (most of a blurred image's background)
+            // joins one warp-aggregated add of 8 per lane; the other lanes
+            // add each run of equal bins with one shared atomic.
             const uint32_t W4 = (uint32_t)(W >> 2);
             const uint32_t span4 = (uint32_t)((z1 - z0) * W4);
             for (uint32_t base = 0; base < span4; base += 2 * kHistThreads) {
@@ -173,12 +176,36 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
                     q[k] = ok[k] ? __ldg(reinterpret_cast<const float4 *>(src + ((z0 + zz) * H + y) * W) + x4)
                                  : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
+                int b[8];
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
-                    count(ok[k] ? bin_of(q[k].x) : -1);
-                    count(ok[k] ? bin_of(q[k].y) : -1);
-                    count(ok[k] ? bin_of(q[k].z) : -1);
-                    count(ok[k] ? bin_of(q[k].w) : -1);
+                    b[4 * k + 0] = ok[k] ? bin_of(q[k].x) : -1;
+                    b[4 * k + 1] = ok[k] ? bin_of(q[k].y) : -1;
+                    b[4 * k + 2] = ok[k] ? bin_of(q[k].z) : -1;
+                    b[4 * k + 3] = ok[k] ? bin_of(q[k].w) : -1;
+                }
+                bool uni = b[0] >= 0;
+#pragma unroll
+                for (int k = 1; k < 8; ++k) uni = uni && b[k] == b[0];
+                {
+                    const int key = uni ? b[0] : -1;
+                    const unsigned peers = __match_any_sync(0xffffffffu, key);
+                    if (key >= 0 && (__ffs(peers) - 1) == (int)lane) atomicAdd(&mine[key], 8u * (uint32_t)__popc(peers));
+                }
+                if (!uni) {
+                    int cur = b[0];
+                    uint32_t n = 1;
+#pragma unroll
+                    for (int k = 1; k < 8; ++k) {
+                        if (b[k] == cur) {
+                            ++n;
+                        } else {
+                            if (cur >= 0) atomicAdd(&mine[cur], n);
+                            cur = b[k];
+                            n = 1;
+                        }
+                    }
+                    if (cur >= 0) atomicAdd(&mine[cur], n);
                 }
             }
             goto merge;

@@ -495,7 +495,8 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
         S->steps = t + 1;
         S->done = done ? 1 : 0;
         const int e = *(volatile int *)&S->err;
-        *d_status = done ? CLE_OK : (e ? e : (int)CLE_ERR_ITER_LIMIT);
+        // the caller cleared the word; an earlier stage's error stays
+        if (!done) *d_status = e ? e : (int)CLE_ERR_ITER_LIMIT;
     }
 }
 

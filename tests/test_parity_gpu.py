@@ -53,6 +53,34 @@ def test_gaussian_blur_narrow_input(cle, oracle, dtype):
     assert np.array_equal(got, oracle.gaussian_blur(a.astype(np.float32), 2, 2, 2))
 
 
+# rows of a multiple of 16 bytes: the fused volume blur stages its planes
+# with TMA copies (boxes starting left of / above the image, partial tiles at
+# the right and bottom edges, fewer planes than the z window)
+TMA_CASES = [(np.uint8, (5, 45, 80)), (np.uint8, (40, 70, 160)), (np.uint16, (5, 45, 72)),
+             (np.uint16, (40, 70, 136)), (np.uint16, (3, 33, 8)), (np.float32, (5, 45, 68)),
+             (np.float32, (40, 70, 132))]
+
+
+@pytest.mark.parametrize("dtype,shape", TMA_CASES)
+@pytest.mark.parametrize("sigma", [0.3, 0.8, 1.0, 1.7, 2.0, 3.5])
+def test_gaussian_blur_tma_staging_bit_exact(cle, oracle, dtype, shape, sigma):
+    import torch
+    from pyclesperanto_prototype_b200 import _lib
+    r = rng(23)
+    a = (r.integers(0, np.iinfo(dtype).max, size=shape) if dtype != np.float32
+         else r.uniform(0, 5000, size=shape)).astype(dtype)
+    src = torch.from_numpy(a).cuda()
+    dst = torch.empty(shape, dtype=torch.float32, device="cuda")
+    lib = _lib.load()
+    s, d = _lib.tensor_desc(src), _lib.tensor_desc(dst)
+    ws = torch.empty(lib.cle_gaussian_blur_workspace_bytes(_lib.ref(s)), dtype=torch.uint8, device="cuda")
+    stream = _lib.stream_ptr()
+    _lib.check(lib.cle_gaussian_blur(_lib.ref(s), _lib.ref(d), sigma, sigma, sigma, ws.data_ptr(), ws.numel(),
+                                     stream), "gaussian_blur")
+    assert lib.cle_workspace_status(ws.data_ptr(), ws.numel(), stream) == 0
+    assert np.array_equal(dst.cpu().numpy(), oracle.gaussian_blur(a.astype(np.float32), sigma, sigma, sigma))
+
+
 def test_gaussian_blur_reference_test(cle):
     # tests/test_gaussian_blur.py:4-22 of the reference
     t = np.zeros((5, 5))
@@ -96,6 +124,22 @@ def test_min_max_histogram_exact(cle, oracle, shape):
     assert cle.maximum_of_all_pixels(a) == a.max()
     h = cle.pull(cle.histogram(a, num_bins=256))
     assert np.array_equal(h, oracle.histogram(a, 256))
+
+
+@pytest.mark.parametrize("shape", [(64, 100), (9, 50, 64), (3, 128, 256), (5, 7, 1028)])
+@pytest.mark.parametrize("bins", [256, 7, 600])
+def test_histogram_smooth_image_exact(cle, oracle, shape, bins):
+    # rows of a multiple of 4 floats: lanes whose 8 voxels share a bin add
+    # them at once, the others add runs of equal bins; plateaus, ramps,
+    # noisy patches and values on bin edges exercise both
+    r = rng(25)
+    a = np.full(shape, 100.0, np.float32)
+    ramp = np.linspace(0.0, 1000.0, shape[-1], dtype=np.float32)
+    a[..., : shape[-1] // 3] += ramp[: shape[-1] // 3]
+    a += (r.uniform(size=shape) < 0.02) * r.normal(0, 300, size=shape).astype(np.float32)
+    a.reshape(-1)[:: 97] = 100.0 + 1000.0 * r.integers(0, 8, size=a.size)[:: 97].astype(np.float32) / 7.0
+    h = cle.pull(cle.histogram(a, num_bins=bins))
+    assert np.array_equal(h, oracle.histogram(a, bins))
 
 
 @pytest.mark.parametrize("img", [
