@@ -105,6 +105,21 @@ STAGES = ["blur_spot", "detect_maxima", "blur_outline", "minmax_hist_otsu", "thr
 ALGO_BYTES = {"blur_spot": 2 + 4, "detect_maxima": 4 + 1, "blur_outline": 2 + 4,
               "minmax_hist_otsu": 4 + 4, "threshold_seeds": 4 + 1 + 1 + 4,
               "voronoi_growth": 1 + 1 + 4, "stats_pass1": 4 + 2, "stats_pass2": 4 + 2}
+
+
+def algo_bytes(w, labelled_fraction=None):
+    """ALGO_BYTES for a workload: with equal spot and outline sigmas the blur
+    runs once (its stage carries the min / max) and the maxima are found in
+    the seed pass (read T, write the mask and the labels; no spots image, no
+    second blur).  The second statistics pass reads the label and intensity
+    of labelled voxels only."""
+    b = dict(ALGO_BYTES)
+    if w.get("spot") is not None and w.get("spot") == w.get("outline"):
+        b["threshold_seeds"] = 4 + 1 + 4
+        del b["detect_maxima"], b["blur_outline"]
+    if labelled_fraction is not None:
+        b["stats_pass2"] = (4 + 2) * labelled_fraction
+    return b
 # The pipeline's compulsory traffic per voxel (the minimal pass structure the
 # two global reductions force): read src + write blur 8, read blur for the
 # histogram 4, read src + blur and write mask + seeds 10, read mask + seeds
@@ -585,14 +600,19 @@ def run_b200(args):
     # roofline: the dominant kernel stage
     sm = np.array([s + [0.0] * (12 - len(s)) for s in stage_ms])[:, :12]
     mean_stage = sm.mean(axis=0)
-    cands = [(mean_stage[i], STAGES[i]) for i in range(12) if STAGES[i] in ALGO_BYTES]
+    frac_lab = None
+    if not dense and L:
+        from pyclesperanto_prototype_b200._ops import STAT_KEYS
+        frac_lab = float(table[STAT_KEYS.index("area")][:int(L)].double().sum()) / nvox
+    abytes = algo_bytes(w, frac_lab)
+    cands = [(mean_stage[i], STAGES[i]) for i in range(12) if STAGES[i] in abytes]
     peak, peak_kind = load_peaks()
     if dense:
         # no stage events on this composition: the whole step against the peak
         dom, t_dom, bpv = "gauss_otsu_labeling + statistics (whole step)", ms_per_step, DENSE_BYTES_PER_VOXEL
     else:
         t_dom, dom = max(cands)
-        bpv = ALGO_BYTES[dom]
+        bpv = abytes[dom]
     achieved = bpv * nvox / (t_dom / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
@@ -602,8 +622,8 @@ def run_b200(args):
         roofline["traffic"] = tr[0]
         roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/" + tr[1]
     stages = {STAGES[i]: round(float(mean_stage[i]), 4) for i in range(12) if STAGES[i]}
-    stage_roofline = {name: round(ALGO_BYTES[name] * nvox / (stages[name] / 1e3) / 1e9 / peak, 4)
-                      for name in ALGO_BYTES if stages.get(name)}
+    stage_roofline = {name: round(abytes[name] * nvox / (stages[name] / 1e3) / 1e9 / peak, 4)
+                      for name in abytes if stages.get(name)}
     # the whole pipeline against the same peak at the compulsory bytes per voxel
     bpv_pipe = DENSE_BYTES_PER_VOXEL if dense else PIPELINE_BYTES_PER_VOXEL
     pipe_bytes = bpv_pipe * nvox

@@ -7,8 +7,9 @@
 //   * a CTA owns a kTX x kTY output tile in (x, y) and marches along z over a
 //     chunk of planes (plus R halo planes at each end, clamped);
 //   * per input plane it stages the clamped (kTY+2R) x (kTX+2R) tile in
-//     shared memory as float32.  On 3D volumes whose rows are a multiple of
-//     16 bytes (and when the caller gives a status word) one thread fetches
+//     shared memory as float32.  On volumes whose rows are a multiple of 16
+//     bytes and whose grid fills two waves of resident CTAs (and when the
+//     caller gives a status word) one thread fetches
 //     each plane's raw tile with a TMA copy (cp.async.bulk.tensor) into a ring
 //     of kStages shared-memory stages, kStages-1 planes ahead, completion
 //     counted by an mbarrier per stage; the CTA converts the landed tile to
@@ -482,7 +483,15 @@ int launch_fused_r(const Img &src, float *dst, const Taps &t, float *mm, int *st
     alignas(64) CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
     if constexpr (Z) {
-        if (status != nullptr && encode_source_map<Tin, R>(src, map)) {
+        // TMA staging once the grid fills two waves of resident CTAs: with
+        // fewer CTAs (one wave, one or two per SM) the register-staged path
+        // measured faster (128 x 512 x 512 at R = 8: 0.265 vs 0.305 ms;
+        // 512 x 1024 x 1024: 3.19 vs 3.12 ms the other way)
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const int64_t ctas = (int64_t)grid.x * grid.y * grid.z;
+        const bool waves2 = ctas >= 2 * (int64_t)num_sms(dev) * min_ctas<R>();
+        if (status != nullptr && waves2 && encode_source_map<Tin, R>(src, map)) {
             auto kern = blur_fused_kernel<Tin, R, true, true>;
             const size_t smem = TmaGeom<Tin, R>::SMEM;
             // set on every call: the attribute belongs to the current device's context

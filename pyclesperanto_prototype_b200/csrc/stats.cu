@@ -184,6 +184,126 @@ count_kernel(const TL *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fc,
     }
 }
 
+// Runs over 128 voxels of a row, 4 per lane (uint32 labels, rows of a multiple
+// of 4, 16-byte aligned): position p = 4 lane + k.  Per lane the 4-bit masks
+// of run heads and run tails, and for each position the position of its run's
+// head (the last head at or before it, in this lane or, through the nearest
+// earlier lane that holds a head, before it; position 0 is always a head).
+struct Run4 {
+    uint32_t hmask, tmask;
+    int hpos[4];
+};
+
+__device__ __forceinline__ Run4 make_run4(const uint32_t (&l)[4]) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, l[3], 1);
+    const uint32_t next = __shfl_down_sync(0xffffffffu, l[0], 1);
+    Run4 r;
+    r.hmask = ((lane == 0 || l[0] != prev) ? 1u : 0u) | (l[1] != l[0] ? 2u : 0u) | (l[2] != l[1] ? 4u : 0u) |
+              (l[3] != l[2] ? 8u : 0u);
+    r.tmask = (r.hmask >> 1) | ((lane == 31 || l[3] != next) ? 8u : 0u);
+    const unsigned has = __ballot_sync(0xffffffffu, r.hmask != 0u);
+    const int last = r.hmask ? 4 * lane + 31 - __clz(r.hmask) : 0;
+    const int j = lane ? 31 - __clz(has & ((1u << lane) - 1u)) : 0;
+    const int before = __shfl_sync(0xffffffffu, last, j);   // lane 0: unused (its bit 0 is a head)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t upto = r.hmask & ((2u << k) - 1u);
+        r.hpos[k] = upto ? 4 * lane + 31 - __clz(upto) : before;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void live4(const uint32_t *lab, int64_t m, int64_t L, uint32_t (&l)[4]) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(lab + m));
+    l[0] = v.x > (uint32_t)L ? 0u : v.x;
+    l[1] = v.y > (uint32_t)L ? 0u : v.y;
+    l[2] = v.z > (uint32_t)L ? 0u : v.z;
+    l[3] = v.w > (uint32_t)L ? 0u : v.w;
+}
+
+// Pass A, uint32 labels in 128-voxel row segments: one atomic per run.
+__global__ void __launch_bounds__(kST)
+count4_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fs, int64_t Lcap,
+              const uint32_t *__restrict__ d_L, uint32_t *__restrict__ cnt) {
+    const int64_t L = live_labels(Lcap, d_L);
+    const int lane = threadIdx.x & 31;
+    const uint32_t segs = fs.d;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch][4];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const uint32_t t = t0 + (uint32_t)b * nwarps;
+            const uint32_t row = fs.div(t), x = (t - row * segs) * 128u + 4u * (uint32_t)lane;
+            if (t < tasks && x < W) live4(lab, (int64_t)row * W + x, L, lb[b]);
+            else lb[b][0] = lb[b][1] = lb[b][2] = lb[b][3] = 0u;
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const uint32_t(&l)[4] = lb[b];
+            if (__ballot_sync(0xffffffffu, (l[0] | l[1] | l[2] | l[3]) != 0u) == 0u) continue;
+            const Run4 r = make_run4(l);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (((r.tmask >> k) & 1u) && l[k]) atomicAdd(cnt + (l[k] - 1), (uint32_t)(4 * lane + k - r.hpos[k] + 1));
+        }
+    }
+}
+
+// Pass B, the same segments: each run reserves its place with one atomic (at
+// its tail) and every voxel writes its index at the run's base + its offset
+// from the head; the base of a run whose tail lies in a later lane comes from
+// the nearest later lane holding a tail (its first tail).
+__global__ void __launch_bounds__(kST)
+scatter4_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fs, int64_t Lcap,
+                const uint32_t *__restrict__ d_L, uint32_t *__restrict__ cursor, uint32_t *__restrict__ sorted) {
+    const int64_t L = live_labels(Lcap, d_L);
+    const int lane = threadIdx.x & 31;
+    const uint32_t segs = fs.d;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch][4], mb[kBatch];
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const uint32_t t = t0 + (uint32_t)b * nwarps;
+            const uint32_t row = fs.div(t), x = (t - row * segs) * 128u + 4u * (uint32_t)lane;
+            mb[b] = row * W + x;
+            if (t < tasks && x < W) live4(lab, (int64_t)mb[b], L, lb[b]);
+            else lb[b][0] = lb[b][1] = lb[b][2] = lb[b][3] = 0u;
+        }
+#pragma unroll
+        for (int b = 0; b < kBatch; ++b) {
+            const uint32_t(&l)[4] = lb[b];
+            if (__ballot_sync(0xffffffffu, (l[0] | l[1] | l[2] | l[3]) != 0u) == 0u) continue;
+            const Run4 r = make_run4(l);
+            uint32_t pos[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                pos[k] = 0u;
+                if (((r.tmask >> k) & 1u) && l[k])
+                    pos[k] = atomicAdd(cursor + (l[k] - 1), (uint32_t)(4 * lane + k - r.hpos[k] + 1));
+            }
+            // base of the run holding this lane's first voxel when its tail is later
+            const uint32_t first = r.tmask & (0u - r.tmask);   // lowest tail bit
+            const uint32_t pfirst = first == 1u ? pos[0] : first == 2u ? pos[1] : first == 4u ? pos[2] : pos[3];
+            const unsigned hasT = __ballot_sync(0xffffffffu, r.tmask != 0u);
+            const unsigned later = hasT & ~((2u << lane) - 1u);   // lane 31 always holds a tail
+            const int j = later ? __ffs(later) - 1 : lane;
+            const uint32_t after = __shfl_sync(0xffffffffu, pfirst, j);
+            // walk the lane's voxels from the last: the base of the run ending at or after k
+            uint32_t base = after;
+#pragma unroll
+            for (int k = 3; k >= 0; --k) {
+                if ((r.tmask >> k) & 1u) base = pos[k];
+                if (l[k]) sorted[base + (uint32_t)(4 * lane + k - r.hpos[k])] = mb[b] + (uint32_t)k;
+            }
+        }
+    }
+}
+
 // Offsets: exclusive scan of the counts (tiles of kScanTile labels: tile sums,
 // a one-CTA scan of the tile sums, then each tile's scan); cursor = offset;
 // off[L] = total.
@@ -572,12 +692,22 @@ int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc
     const FastDiv fW((uint32_t)lab.W), fH((uint32_t)lab.H);
     stage_mark(8, st);
     const FastDiv fc((uint32_t)((lab.W + 31) / 32));
-    count_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L, so.cnt);
+    // uint32 rows of a multiple of 4 voxels on a 16-byte boundary: 128-voxel
+    // segments with 128-bit loads
+    const bool seg4 = std::is_same<TL, uint32_t>::value && lab.W % 4 == 0 &&
+                      (reinterpret_cast<uintptr_t>(lab.data) & 15) == 0;
+    const int64_t tasks4 = rows * ((lab.W + 127) / 128);
+    const FastDiv fs((uint32_t)((lab.W + 127) / 128));
+    const int blocks4 = launch_blocks(tasks4 * 32, kST, 8);
+    if (seg4) count4_kernel<<<blocks4, kST, 0, st>>>((const uint32_t *)lab.data, (uint32_t)lab.W, (uint32_t)tasks4, fs, L, d_L, so.cnt);
+    else count_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L, so.cnt);
     tile_sum_kernel<<<(unsigned)ntiles, kST, 0, st>>>(so.cnt, L, d_L, so.tsum);
     tile_scan_kernel<<<1, 1024, 0, st>>>(so.tsum, ntiles);
     offset_kernel<<<(unsigned)ntiles, kST, 0, st>>>(so.cnt, L, d_L, so.tsum, so.off, so.cursor);
-    scatter_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L,
-                                               so.cursor, so.sorted);
+    if (seg4) scatter4_kernel<<<blocks4, kST, 0, st>>>((const uint32_t *)lab.data, (uint32_t)lab.W, (uint32_t)tasks4, fs, L, d_L,
+                                                        so.cursor, so.sorted);
+    else scatter_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L,
+                                                    so.cursor, so.sorted);
     sweep_kernel<1, TL, TI><<<sweep_blocks, kST, 0, st>>>((const TL *)lab.data, (const TI *)inten.data, so.sorted,
                                                           so.off, L, d_L, fW, fH, a, b);
     stage_mark(9, st);

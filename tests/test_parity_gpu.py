@@ -53,16 +53,17 @@ def test_gaussian_blur_narrow_input(cle, oracle, dtype):
     assert np.array_equal(got, oracle.gaussian_blur(a.astype(np.float32), 2, 2, 2))
 
 
-# rows of a multiple of 16 bytes: the fused volume blur stages its planes
-# with TMA copies (boxes starting left of / above the image, partial tiles at
-# the right and bottom edges, fewer planes than the z window)
-TMA_CASES = [(np.uint8, (5, 45, 80)), (np.uint8, (40, 70, 160)), (np.uint16, (5, 45, 72)),
-             (np.uint16, (40, 70, 136)), (np.uint16, (3, 33, 8)), (np.float32, (5, 45, 68)),
-             (np.float32, (40, 70, 132))]
+# rows of a multiple of 16 bytes and grids of at least two waves of CTAs: the
+# fused volume blur stages its planes with TMA copies (boxes starting left of /
+# above the image, partial tiles at the right and bottom edges, volumes with
+# fewer planes than the z window inside each chunk's halo)
+TMA_CASES = [(np.uint16, (96, 700, 1000), 0.8), (np.uint16, (96, 700, 1000), 2.0),
+             (np.uint16, (60, 700, 1000), 3.5), (np.uint16, (9, 1030, 4104), 1.7),
+             (np.uint8, (80, 700, 1008), 1.0), (np.uint8, (80, 700, 1008), 2.0),
+             (np.float32, (64, 700, 1004), 1.0), (np.float32, (64, 700, 1004), 0.3)]
 
 
-@pytest.mark.parametrize("dtype,shape", TMA_CASES)
-@pytest.mark.parametrize("sigma", [0.3, 0.8, 1.0, 1.7, 2.0, 3.5])
+@pytest.mark.parametrize("dtype,shape,sigma", TMA_CASES)
 def test_gaussian_blur_tma_staging_bit_exact(cle, oracle, dtype, shape, sigma):
     import torch
     from pyclesperanto_prototype_b200 import _lib
@@ -322,6 +323,30 @@ def test_statistics_random(cle, oracle, shape):
     lab[lab == 5] = 0           # label 5 absent: reference sentinels
     inten = r.uniform(0, 1000, size=shape).astype(np.float32)
     _assert_stats(cle.statistics_of_labelled_pixels(inten, lab), oracle.statistics_of_labelled_pixels(inten, lab))
+
+
+@pytest.mark.parametrize("shape", [(3, 5, 8), (40, 260), (6, 33, 132), (2, 9, 1024)])
+@pytest.mark.parametrize("pattern", ["runs", "random", "stripes"])
+def test_statistics_row_segments(cle, oracle, shape, pattern):
+    # uint32 rows of a multiple of 4 voxels take the 4-per-lane run passes:
+    # runs that cross lanes and 128-voxel segments, single voxels, rows that
+    # end inside a segment
+    r = rng(27)
+    if pattern == "runs":
+        lab = np.repeat(r.integers(0, 9, size=shape[:-1] + (shape[-1] // 4 + 1,)), 4 + shape[-1] % 3, axis=-1)
+        lab = lab[..., : shape[-1]]
+        lab = np.ascontiguousarray(np.broadcast_to(lab, shape) if lab.shape != shape else lab)
+    elif pattern == "random":
+        lab = r.integers(0, 7, size=shape)
+    else:
+        lab = (np.arange(shape[-1]) // 37 % 5) * np.ones(shape, np.int64)
+    lab = lab.astype(np.uint32)
+    inten = r.integers(0, 4000, size=shape).astype(np.uint16)
+    import torch
+    # uint32 labels on the device (a numpy label image is pushed as float32)
+    dlab = cle.B200Array(torch.from_numpy(lab).cuda())
+    _assert_stats(cle.statistics_of_labelled_pixels(inten, dlab),
+                  oracle.statistics_of_labelled_pixels(inten.astype(np.float32), lab))
 
 
 def test_statistics_reference_tables(cle, oracle):
