@@ -563,10 +563,21 @@ sweep_kernel(const TL *__restrict__ lab, const TI *__restrict__ inten, const uin
         const uint32_t c1 = min(total, c0 + (uint32_t)kChunk);
         uint32_t cur = 0;
         float4 pc = make_float4(0.f, 0.f, 0.f, 0.f), pm = pc;
+        // label of the entries seen last and the end of its range: a block of
+        // 32 entries inside that range takes the label without reading it
+        uint32_t lc = 0, lend = 0;
         for (uint32_t p = c0 + lane; p - lane < c1; p += 32) {
             const bool valid = p < c1;
             const uint32_t m = valid ? sorted[p] : 0u;
-            const uint32_t l = valid ? lab_of(lab[m]) : 0xFFFFFFFFu;
+            const uint32_t pb = p - lane, plast = min(pb + 31u, c1 - 1u);
+            uint32_t l;
+            if (plast < lend) {
+                l = valid ? lc : 0xFFFFFFFFu;
+            } else {
+                l = valid ? lab_of(lab[m]) : 0xFFFFFFFFu;
+                lc = __shfl_sync(0xffffffffu, l, (int)(plast - pb));
+                lend = off[lc];
+            }
             const float v = valid ? to_f32(inten[m]) : 0.0f;
             uint32_t x = 0, y = 0, z = 0;
             if (valid) m2xyz_fd(fW, fH, m, x, y, z);
