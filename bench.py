@@ -127,16 +127,23 @@ def algo_bytes(w, labelled_fraction=None):
 PIPELINE_BYTES_PER_VOXEL = 8 + 4 + 10 + 6 + 8
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
-# one ncu --set full capture per kernel; the captures are summarised in
-# profiles/<kernel>_<workload>.md.
+# DRAM bytes per launch from one ncu capture per kernel (dram__bytes_read.sum +
+# dram__bytes_write.sum, or the DRAM bandwidth x the duration of the same
+# launch); the captures are summarised in profiles/<kernel>_<workload>.md.
 MEASURED_TRAFFIC = {
     "nuclei": {"voronoi_growth": (360.142e6 + 89.806e6, "voronoi_bricks_kernel_nuclei_128x512x512.md"),
                "blur_spot": (67.164e6 + 81.208e6, "blur_fused_kernel_nuclei_128x512x512.md"),
                "blur_outline": (67.155e6 + 81.081e6, "blur_fused_kernel_nuclei_128x512x512.md"),
                "detect_maxima": (135.090e6 + 19.932e6, "maxima_kernel_nuclei_128x512x512.md"),
-               "stats_pass1": (165.217e6 + 3.589e6, "stats_pass1_nuclei_128x512x512.md"),
-               "stats_pass2": (165.196e6 + 4.073e6, "stats_pass2_nuclei_128x512x512.md")},
+               },
+    # slab captures (128x1024x1024) scaled by 4 to the 512x1024x1024 volume:
+    # the same recipe and cell density, traffic in proportion to the voxels
+    "lightsheet": {"voronoi_growth": (4 * 3.668e9, "voronoi_bricks_kernel_lightsheet_slab_128x1024x1024.md"),
+                   "blur_spot": (4 * 0.792e9, "blur_fused_kernel_lightsheet_slab_128x1024x1024.md"),
+                   "threshold_seeds": (4 * 1.165e9, "maxima_seeds_kernel_lightsheet_slab_128x1024x1024.md")},
+    "lightsheet_slab": {"voronoi_growth": (3.668e9, "voronoi_bricks_kernel_lightsheet_slab_128x1024x1024.md"),
+                        "blur_spot": (0.792e9, "blur_fused_kernel_lightsheet_slab_128x1024x1024.md"),
+                        "threshold_seeds": (1.165e9, "maxima_seeds_kernel_lightsheet_slab_128x1024x1024.md")},
 }
 
 # Algorithmic bytes per voxel of a whole gauss_otsu_labeling + statistics step
@@ -620,7 +627,8 @@ def run_b200(args):
     tr = MEASURED_TRAFFIC.get(args.workload, {}).get(dom)
     if tr:
         roofline["traffic"] = tr[0]
-        roofline["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/" + tr[1]
+        roofline["traffic_source"] = ("ncu DRAM bytes of one launch, profiles/" + tr[1]
+                                      + (" (128x1024x1024 capture x 4)" if args.workload == "lightsheet" else ""))
     stages = {STAGES[i]: round(float(mean_stage[i]), 4) for i in range(12) if STAGES[i]}
     stage_roofline = {name: round(abytes[name] * nvox / (stages[name] / 1e3) / 1e9 / peak, 4)
                       for name in abytes if stages.get(name)}
