@@ -102,7 +102,7 @@ maxima_kernel(const Ts *__restrict__ src, Td *__restrict__ dst, int D, int H, in
 // computed once; per plane only the plane's base moves.  Every owned voxel's
 // seg and label entry is written.
 template <int ROWS>
-__global__ void __launch_bounds__(32 * kGroups)
+__global__ void __launch_bounds__(32 * kGroups, 5)
 maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr32, Geo g, int zchunk,
                     uint8_t *__restrict__ seg, uint32_t *__restrict__ lab, uint32_t *__restrict__ seeds,
                     uint32_t *__restrict__ d_count) {
@@ -134,11 +134,13 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
         for (int j = 0; j < kWin; ++j) v[j] = (zok && rok[j]) ? P[roff[j]] : NEG;
     };
 
-    float vm[kWin], vc[kWin], vp[kWin];
+    // planes z-1, z, z+1 held; plane z+2 loads while plane z is computed
+    float vm[kWin], vc[kWin], vp[kWin], vn[kWin];
     load_plane(z0 - 1, vm);
     load_plane(z0, vc);
+    load_plane(z0 + 1, vp);
     for (int z = z0; z < z1; ++z) {
-        load_plane(z + 1, vp);
+        if (z + 1 < z1) load_plane(z + 2, vn);
         float Tm[kWin];
 #pragma unroll
         for (int j = 0; j < kWin; ++j) Tm[j] = fmaxf(fmaxf(vm[j], vc[j]), vp[j]);
@@ -183,6 +185,7 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
         for (int j = 0; j < kWin; ++j) {
             vm[j] = vc[j];
             vc[j] = vp[j];
+            vp[j] = vn[j];
         }
     }
 }
