@@ -153,6 +153,7 @@ __device__ __forceinline__ uint32_t live_label(const TL *lab, int64_t m, int64_t
 }
 
 constexpr int kBatch = 4;   // row segments per warp round (loads in flight)
+constexpr int kSweepBlocks = 4;   // 32-entry blocks per sweep round (loads in flight)
 
 // Pass A: voxels per label (one atomic per row run).  A warp takes 32 voxels
 // of one row at a time, kBatch row segments per round with every load issued
@@ -550,6 +551,8 @@ sweep_kernel(const TL *__restrict__ lab, const TI *__restrict__ inten, const uin
              const uint32_t *__restrict__ off, int64_t Lcap, const uint32_t *__restrict__ d_L, FastDiv fW,
              FastDiv fH, Acc1 a, Acc2 b) {
     constexpr bool INT = sizeof(TI) <= 2 && !std::is_floating_point<TI>::value;
+    // float64 accumulators (pass 1 of 32-bit intensities) leave room for 2 blocks
+    constexpr int NB = (PASS == 1 && !INT) ? 2 : kSweepBlocks;
     const int64_t L = live_labels(Lcap, d_L);
     const uint32_t total = off[L];
     const int lane = threadIdx.x & 31;
@@ -566,10 +569,29 @@ sweep_kernel(const TL *__restrict__ lab, const TI *__restrict__ inten, const uin
         // label of the entries seen last and the end of its range: a block of
         // 32 entries inside that range takes the label without reading it
         uint32_t lc = 0, lend = 0;
-        for (uint32_t p = c0 + lane; p - lane < c1; p += 32) {
+        // NB blocks of 32 entries per round: their index loads, then
+        // their intensity gathers, are all in flight before any is used
+        for (uint32_t q = c0; q < c1; q += 32u * NB) {
+            uint32_t mk[NB];
+            TI ik[NB];
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                const uint32_t p = q + 32u * k + lane;
+                mk[k] = p < c1 ? sorted[p] : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+                const uint32_t p = q + 32u * k + lane;
+                ik[k] = p < c1 ? inten[mk[k]] : TI(0);
+            }
+#pragma unroll
+            for (int k = 0; k < NB; ++k) {
+            const uint32_t pb = q + 32u * k;
+            if (pb >= c1) break;   // warp-uniform
+            const uint32_t p = pb + lane;
             const bool valid = p < c1;
-            const uint32_t m = valid ? sorted[p] : 0u;
-            const uint32_t pb = p - lane, plast = min(pb + 31u, c1 - 1u);
+            const uint32_t m = mk[k];
+            const uint32_t plast = min(pb + 31u, c1 - 1u);
             uint32_t l;
             if (plast < lend) {
                 l = valid ? lc : 0xFFFFFFFFu;
@@ -578,7 +600,7 @@ sweep_kernel(const TL *__restrict__ lab, const TI *__restrict__ inten, const uin
                 lc = __shfl_sync(0xffffffffu, l, (int)(plast - pb));
                 lend = off[lc];
             }
-            const float v = valid ? to_f32(inten[m]) : 0.0f;
+            const float v = valid ? to_f32(ik[k]) : 0.0f;
             uint32_t x = 0, y = 0, z = 0;
             if (valid) m2xyz_fd(fW, fH, m, x, y, z);
             unsigned todo = __ballot_sync(0xffffffffu, valid);
@@ -614,6 +636,7 @@ sweep_kernel(const TL *__restrict__ lab, const TI *__restrict__ inten, const uin
                     }
                 }
                 todo &= ~__ballot_sync(0xffffffffu, mine);
+            }
             }
         }
         if (cur) {

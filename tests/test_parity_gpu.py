@@ -143,6 +143,25 @@ def test_histogram_smooth_image_exact(cle, oracle, shape, bins):
     assert np.array_equal(h, oracle.histogram(a, bins))
 
 
+@pytest.mark.parametrize("bins", [256, 9])
+def test_histogram_nan_inf_given_range(cle, oracle, bins):
+    # NaN / +-inf voxels inside otherwise uniform 8-voxel groups, with the
+    # range given: those groups bin every voxel (NaN and -inf land in bin 0,
+    # +inf and values above the range in none)
+    r = rng(26)
+    a = np.full((6, 40, 128), 250.0, np.float32)
+    a[:, :, 64:] = 700.0
+    flat = a.reshape(-1)
+    idx = r.choice(flat.size, 300, replace=False)
+    flat[idx[:100]] = np.nan
+    flat[idx[100:200]] = np.inf
+    flat[idx[200:]] = -np.inf
+    a[2, 5, :] = 5000.0   # above the range
+    h = cle.pull(cle.histogram(a, num_bins=bins, minimum_intensity=100.0, maximum_intensity=1000.0,
+                               determine_min_max=False))
+    assert np.array_equal(h, oracle.histogram(a, bins, 100.0, 1000.0))
+
+
 @pytest.mark.parametrize("img", [
     [[1, 2, 4, 4, 2, 3], [3, 3, 4, 4, 5, 5]],
     [[[1, 2, 4, 4, 2, 3]], [[3, 3, 4, 4, 5, 5]]],
