@@ -114,15 +114,21 @@ __device__ __forceinline__ int hist_bin(float v, float mn, float range, float bm
 // wherever q + 0.5 lies at least 2^-8 from an integer the truncation gives
 // the same bin; everything else (near a bin edge, NaN, inf, an empty range)
 // takes the exact division.
-__device__ __forceinline__ int hist_bin_fast(float v, float mn, float range, float rr, float bm1, int bins) {
-    const float a = __fmul_rn(__fsub_rn(v, mn), bm1);
-    const float q = __fadd_rn(__fmul_rn(a, rr), 0.5f);
+// The bin from q = (v - min) * (bins-1) * (1/range) + 0.5 (each step rounded),
+// or the exact division near a bin edge.
+__device__ __forceinline__ int hist_bin_from_q(float q, float v, float mn, float range, float bm1, int bins) {
     const float d = fabsf(__fsub_rn(q, rintf(q)));
     if (d >= 0.00390625f && q >= 0.0f && q < 65536.0f) {
         const uint32_t b = (uint32_t)q;
         return b < (uint32_t)bins ? (int)b : -1;
     }
     return hist_bin(v, mn, range, bm1, bins);
+}
+
+__device__ __forceinline__ int hist_bin_fast(float v, float mn, float range, float rr, float bm1, int bins) {
+    const float a = __fmul_rn(__fsub_rn(v, mn), bm1);
+    const float q = __fadd_rn(__fmul_rn(a, rr), 0.5f);
+    return hist_bin_from_q(q, v, mn, range, bm1, bins);
 }
 
 constexpr int kHistThreads = 256;
@@ -177,12 +183,28 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
                                  : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
                 int b[8];
+                if (fast) {
+                    // the fast bins two at a time: (v + (-min)) * (bins-1) * (1/range)
+                    // + 0.5 in packed round-to-nearest pairs, the same roundings
+                    // as hist_bin_fast's scalar operations
+                    const float2 nmn = make_float2(-mn, -mn), s2 = make_float2(bm1, bm1);
+                    const float2 r2 = make_float2(rr, rr), h2 = make_float2(0.5f, 0.5f);
+                    const float v[8] = {q[0].x, q[0].y, q[0].z, q[0].w, q[1].x, q[1].y, q[1].z, q[1].w};
 #pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    b[4 * k + 0] = ok[k] ? bin_of(q[k].x) : -1;
-                    b[4 * k + 1] = ok[k] ? bin_of(q[k].y) : -1;
-                    b[4 * k + 2] = ok[k] ? bin_of(q[k].z) : -1;
-                    b[4 * k + 3] = ok[k] ? bin_of(q[k].w) : -1;
+                    for (int k = 0; k < 8; k += 2) {
+                        const float2 a = __fmul2_rn(__fadd2_rn(make_float2(v[k], v[k + 1]), nmn), s2);
+                        const float2 t = __fadd2_rn(__fmul2_rn(a, r2), h2);
+                        b[k] = ok[k / 4] ? hist_bin_from_q(t.x, v[k], mn, range, bm1, bins) : -1;
+                        b[k + 1] = ok[k / 4] ? hist_bin_from_q(t.y, v[k + 1], mn, range, bm1, bins) : -1;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        b[4 * k + 0] = ok[k] ? bin_of(q[k].x) : -1;
+                        b[4 * k + 1] = ok[k] ? bin_of(q[k].y) : -1;
+                        b[4 * k + 2] = ok[k] ? bin_of(q[k].z) : -1;
+                        b[4 * k + 3] = ok[k] ? bin_of(q[k].w) : -1;
+                    }
                 }
                 bool uni = b[0] >= 0;
 #pragma unroll
