@@ -190,11 +190,116 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
     }
 }
 
+// The same pass with two adjacent columns per lane (rows of an even length,
+// 8-byte aligned T and labels): 64-bit loads of T, a 16-bit store of the two
+// mask bytes and a 64-bit store of the two labels; the x neighbours of a
+// column come from the lane's other column or, across lanes, by shuffles.
+// A warp covers 60 output columns (lanes 1..30; lanes 0 and 31 load the halo
+// pairs).
+constexpr int kOutX2 = 60;
+
+template <int ROWS>
+__global__ void __launch_bounds__(32 * kGroups)
+maxima_seeds2_kernel(const float *__restrict__ T, const float *__restrict__ d_thr32, Geo g, int zchunk,
+                     uint8_t *__restrict__ seg, uint32_t *__restrict__ lab, uint32_t *__restrict__ seeds,
+                     uint32_t *__restrict__ d_count) {
+    constexpr int kRows = ROWS, kWin = ROWS + 2;
+    const int D = (int)g.D, H = (int)g.H, W = (int)g.W;
+    const uint32_t HW = g.H * g.W;
+    const int lane = threadIdx.x;
+    const int xa = (int)blockIdx.x * kOutX2 + 2 * lane - 2;   // columns xa, xa + 1
+    const int y0 = ((int)blockIdx.y * kGroups + threadIdx.y) * kRows;
+    const int z0 = (int)blockIdx.z * zchunk;
+    const int z1 = min(D, z0 + zchunk);
+    if (y0 >= H) return;   // whole warp leaves together (y0 is warp-uniform)
+    const bool xin = xa >= 0 && xa < W;   // W even: xa + 1 < W as well
+    const bool own = lane >= 1 && lane <= kOutX2 / 2 && xin;
+    const float NEG = -INFINITY;
+    const float t = *d_thr32;
+    uint32_t roff[kWin];
+    bool rok[kWin];
+#pragma unroll
+    for (int j = 0; j < kWin; ++j) {
+        const int y = y0 - 1 + j;
+        rok[j] = xin && y >= 0 && y < H;
+        roff[j] = rok[j] ? (uint32_t)y * g.W + (uint32_t)xa : 0u;
+    }
+    auto load_plane = [&](int z, float2 *v) {
+        const bool zok = z >= 0 && z < D;
+        const float *P = T + (size_t)(zok ? z : 0) * HW;
+#pragma unroll
+        for (int j = 0; j < kWin; ++j)
+            v[j] = (zok && rok[j]) ? *reinterpret_cast<const float2 *>(P + roff[j]) : make_float2(NEG, NEG);
+    };
+    auto winner = [](float v, float A, float B) {
+        if (v != v) return true;
+        if (__fsub_rn(v, 1.0f) < v) return (v > A) && (v >= B);
+        return (v >= A) && (v >= B);
+    };
+
+    // planes z-1, z, z+1 held; plane z+2 loads while plane z is computed
+    float2 vm[kWin], vc[kWin], vp[kWin], vn[kWin];
+    load_plane(z0 - 1, vm);
+    load_plane(z0, vc);
+    load_plane(z0 + 1, vp);
+    for (int z = z0; z < z1; ++z) {
+        if (z + 1 < z1) load_plane(z + 2, vn);
+        float2 Tm[kWin];
+#pragma unroll
+        for (int j = 0; j < kWin; ++j)
+            Tm[j] = make_float2(fmaxf(fmaxf(vm[j].x, vc[j].x), vp[j].x), fmaxf(fmaxf(vm[j].y, vc[j].y), vp[j].y));
+        const uint32_t zoff = (uint32_t)z * HW;
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) {
+            const float Sa = fmaxf(fmaxf(Tm[j].x, Tm[j + 1].x), Tm[j + 2].x);
+            const float Sb = fmaxf(fmaxf(Tm[j].y, Tm[j + 1].y), Tm[j + 2].y);
+            const float sl = __shfl_up_sync(0xffffffffu, Sb, 1);     // column xa - 1
+            const float sr = __shfl_down_sync(0xffffffffu, Sa, 1);   // column xa + 2
+            const bool mine = own && rok[j + 1];
+            bool seed_a = false, seed_b = false;
+            const uint32_t m = zoff + roff[j + 1];
+            if (mine) {
+                const float va = vc[j + 1].x, vb = vc[j + 1].y;
+                const bool wa = winner(va, fmaxf(fmaxf(sl, Tm[j].x), vm[j + 1].x), fmaxf(fmaxf(Sb, Tm[j + 2].x), vp[j + 1].x));
+                const bool wb = winner(vb, fmaxf(fmaxf(Sa, Tm[j].y), vm[j + 1].y), fmaxf(fmaxf(sr, Tm[j + 2].y), vp[j + 1].y));
+                const bool ga = va > t, gb = vb > t;
+                seed_a = ga && wa;
+                seed_b = gb && wb;
+                *reinterpret_cast<uint16_t *>(seg + m) = (uint16_t)((ga ? 1u : 0u) | (gb ? 0x100u : 0u));
+                uint2 lv = make_uint2(0u, 0u);
+                if (seed_a | seed_b) {
+                    const uint32_t k = xyz2k(g, (uint32_t)xa, (uint32_t)(y0 + j), (uint32_t)z) + 1u;
+                    lv.x = seed_a ? k : 0u;
+                    lv.y = seed_b ? k + g.H * g.D : 0u;   // key of column xa + 1
+                }
+                *reinterpret_cast<uint2 *>(lab + m) = lv;
+            }
+            const unsigned ba = __ballot_sync(0xffffffffu, seed_a), bb = __ballot_sync(0xffffffffu, seed_b);
+            if (ba | bb) {
+                uint32_t base = 0;
+                const int leader = __ffs(ba | bb) - 1;
+                if (lane == leader) base = atomicAdd(d_count, (uint32_t)(__popc(ba) + __popc(bb)));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                const unsigned below = (1u << lane) - 1u;
+                const uint32_t at = base + __popc(ba & below) + __popc(bb & below);
+                if (seed_a) seeds[at] = m;
+                if (seed_b) seeds[at + (seed_a ? 1u : 0u)] = m + 1u;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kWin; ++j) {
+            vm[j] = vc[j];
+            vc[j] = vp[j];
+            vp[j] = vn[j];
+        }
+    }
+}
+
 // Grid of the z-marching kernels: 30 columns per warp, kGroups x kRows rows
 // per block, z chunks so that about 12 blocks per SM are launched.
-int maxima_grid(const Img &src, dim3 &grid, int &zchunk, int rows = kRows) {
+int maxima_grid(const Img &src, dim3 &grid, int &zchunk, int rows = kRows, int cols = kOutX) {
     const int D = (int)src.D, H = (int)src.H, W = (int)src.W;
-    const int gx = (W + kOutX - 1) / kOutX;
+    const int gx = (W + cols - 1) / cols;
     const int gy = (H + rows * kGroups - 1) / (rows * kGroups);
     int dev = 0;
     cudaGetDevice(&dev);
@@ -240,6 +345,16 @@ int maxima_seeds(const Img &T, const float *d_thr32, uint8_t *seg, uint32_t *lab
     constexpr int kSeedRows = 8;
     dim3 grid;
     int zchunk = 1;
+    const bool pairs = T.W % 2 == 0 && (reinterpret_cast<uintptr_t>(T.data) & 7) == 0 &&
+                       (reinterpret_cast<uintptr_t>(lab) & 7) == 0 && (reinterpret_cast<uintptr_t>(seg) & 1) == 0;
+    if (pairs) {
+        constexpr int kPairRows = 4;
+        CLE_TRY(maxima_grid(T, grid, zchunk, kPairRows, kOutX2));
+        maxima_seeds2_kernel<kPairRows><<<grid, dim3(32, kGroups), 0, st>>>(
+            (const float *)T.data, d_thr32, make_geo(T), zchunk, seg, lab, seeds, d_count);
+        CLE_LAUNCH_CHECK("detect_maxima + seeds (column pairs)");
+        return CLE_OK;
+    }
     CLE_TRY(maxima_grid(T, grid, zchunk, kSeedRows));
     maxima_seeds_kernel<kSeedRows><<<grid, dim3(32, kGroups), 0, st>>>((const float *)T.data, d_thr32, make_geo(T),
                                                                      zchunk, seg, lab, seeds, d_count);

@@ -306,6 +306,19 @@ def test_vol_nuclei_3d_exact(cle, oracle, shape, n):
     assert np.array_equal(got32, ref)
 
 
+@pytest.mark.parametrize("shape,n", [((24, 96, 112), 40), ((9, 70, 62), 12), ((17, 65, 129), 30),
+                                     ((5, 33, 31), 6)])
+@pytest.mark.parametrize("sigma", [1.0, 2.0])
+def test_vol_equal_sigmas_3d_exact(cle, oracle, shape, n, sigma):
+    # equal spot and outline sigmas: one blur, maxima and seeds in one pass
+    # (even and odd row lengths, partial warps at the right edge)
+    from pyclesperanto_prototype_b200 import synthetic
+    vol = synthetic.nuclei_volume(shape, n, seed=5)
+    got = cle.pull(cle.voronoi_otsu_labeling(vol, spot_sigma=sigma, outline_sigma=sigma))
+    ref = oracle.voronoi_otsu_labeling(vol.astype(np.float32), sigma, sigma)
+    assert np.array_equal(got, ref) and ref.max() > 1
+
+
 def test_vol_edge_cases(cle):
     assert cle.pull(cle.voronoi_otsu_labeling(np.full((16, 16), 3.0, np.float32))).max() == 0
     assert cle.pull(cle.voronoi_otsu_labeling(np.zeros((1, 1), np.float32))).max() == 0
