@@ -357,7 +357,8 @@ def e2e_served(pinned_in, w, steps, world, ref_labels=None, slots=3):
     server = SegmentationServer(budget_bytes=60e9, slots=slots, spot_sigma=w["spot"],
                                 outline_sigma=w["outline"])
     outs = [torch.empty(tuple(pinned_in.shape), dtype=torch.uint32).pin_memory() for _ in range(slots)]
-    server.run([Request(-1, pinned_in, 0.0, labels_out=outs[0])], realtime=False)   # warm-up
+    # warm-up: every slot's device buffers allocated before the timed requests
+    server.run([Request(-1 - k, pinned_in, 0.0, labels_out=outs[k]) for k in range(slots)], realtime=False)
     torch.cuda.synchronize()
     reqs = [Request(i, pinned_in, 0.0, labels_out=outs[i % slots]) for i in range(steps)]
     barrier(world)
@@ -474,8 +475,10 @@ def served_vs_per_call(rate, duration, lanes, pool_per_class=3, closed_requests=
 
     server = SegmentationServer(budget_bytes=60e9, slots=lanes, compute_streams=compute_streams,
                                 express_voxels=express_voxels, spot_sigma=spot, outline_sigma=outline)
-    warm = [Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(SERVED_CLASSES)]
-    server.run(warm, realtime=False)
+    # warm-up: one untimed saturating burst, so the buffer pool holds what the
+    # busiest moments need (a device allocation inside a timed run synchronises
+    # the GPU)
+    server.run(make(closed), realtime=False)
     per_call_loop([Request(i, pool[c][0], arrival=0.0) for i, c in enumerate(SERVED_CLASSES)], spot, outline,
                   realtime=False)
     torch.cuda.synchronize()

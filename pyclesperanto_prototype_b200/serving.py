@@ -129,6 +129,10 @@ class SegmentationServer:
         self.spot, self.outline = float(spot_sigma), float(outline_sigma)
         self.copy_in = torch.cuda.Stream(device=self.device)
         self.copy_out = torch.cuda.Stream(device=self.device)
+        # the statistics tables on a stream of their own: behind the label
+        # images of other requests on copy_out, a finished request's table
+        # would hold its slot until those downloads end
+        self.copy_table = torch.cuda.Stream(device=self.device)
         self.computes = [torch.cuda.Stream(device=self.device) for _ in range(max(1, int(compute_streams)))]
         self._next = 0
         self.pool = collections.defaultdict(list)    # (shape, dtype) -> [_Buffers] free
@@ -222,10 +226,13 @@ class SegmentationServer:
             b.host_count.copy_(status_count, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(s)
+        b.labels_done = None
         if req.labels_out is not None:
             self.copy_out.wait_event(computed)
             with torch.cuda.stream(self.copy_out):
                 req.labels_out.copy_(b.labels, non_blocking=True)
+                b.labels_done = torch.cuda.Event()
+                b.labels_done.record(self.copy_out)
         req.admitted = time.perf_counter() - t_ref
         return ev
 
@@ -234,8 +241,10 @@ class SegmentationServer:
         statistics of the request's labels only; returns the event to poll
         (recorded after every copy that reads the request's buffers)."""
         status, count = int(b.host_count[0]), int(b.host_count[1])
-        s = self.copy_out
+        s = self.copy_table
         s.wait_event(done_compute)
+        if b.labels_done is not None:
+            s.wait_event(b.labels_done)   # the buffers stay busy until the labels are out
         if status == _lib.CLE_ERR_CANCELLED or (status == 0 and self._cancel_requested(req.rid)):
             req.cancelled = True
         elif status:
