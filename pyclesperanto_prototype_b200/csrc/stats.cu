@@ -215,17 +215,25 @@ __device__ __forceinline__ Run4 make_run4(const uint32_t (&l)[4]) {
     return r;
 }
 
-__device__ __forceinline__ void live4(const uint32_t *lab, int64_t m, int64_t L, uint32_t (&l)[4]) {
+// Four labels (uint32 or float32) of one 16-byte aligned group, 0 above L.
+template <typename TL>
+__device__ __forceinline__ void live4(const TL *lab, int64_t m, int64_t L, uint32_t (&l)[4]) {
+    static_assert(sizeof(TL) == 4, "4-byte labels");
     const uint4 v = __ldg(reinterpret_cast<const uint4 *>(lab + m));
-    l[0] = v.x > (uint32_t)L ? 0u : v.x;
-    l[1] = v.y > (uint32_t)L ? 0u : v.y;
-    l[2] = v.z > (uint32_t)L ? 0u : v.z;
-    l[3] = v.w > (uint32_t)L ? 0u : v.w;
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint32_t x;
+        if constexpr (std::is_same<TL, float>::value) x = lab_of(__uint_as_float(w[k]));
+        else x = w[k];
+        l[k] = x > (uint32_t)L ? 0u : x;
+    }
 }
 
 // Pass A, uint32 labels in 128-voxel row segments: one atomic per run.
+template <typename TL>
 __global__ void __launch_bounds__(kST)
-count4_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fs, int64_t Lcap,
+count4_kernel(const TL *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fs, int64_t Lcap,
               const uint32_t *__restrict__ d_L, uint32_t *__restrict__ cnt) {
     const int64_t L = live_labels(Lcap, d_L);
     const int lane = threadIdx.x & 31;
@@ -257,8 +265,9 @@ count4_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t tasks, Fast
 // its tail) and every voxel writes its index at the run's base + its offset
 // from the head; the base of a run whose tail lies in a later lane comes from
 // the nearest later lane holding a tail (its first tail).
+template <typename TL>
 __global__ void __launch_bounds__(kST)
-scatter4_kernel(const uint32_t *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fs, int64_t Lcap,
+scatter4_kernel(const TL *__restrict__ lab, uint32_t W, uint32_t tasks, FastDiv fs, int64_t Lcap,
                 const uint32_t *__restrict__ d_L, uint32_t *__restrict__ cursor, uint32_t *__restrict__ sorted) {
     const int64_t L = live_labels(Lcap, d_L);
     const int lane = threadIdx.x & 31;
@@ -714,6 +723,11 @@ __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T, const uin
     }
 }
 
+// The label type of the 128-voxel row-segment passes: the type itself for
+// 4-byte labels (uint32, float32); others take the 32-voxel passes.
+template <typename TL>
+using TL4 = typename std::conditional<sizeof(TL) == 4, TL, uint32_t>::type;
+
 template <typename TL, typename TI>
 int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a, const Acc2 &b,
                 const Sorted &so, cudaStream_t st, const uint32_t *d_L) {
@@ -728,17 +742,16 @@ int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc
     const FastDiv fc((uint32_t)((lab.W + 31) / 32));
     // uint32 rows of a multiple of 4 voxels on a 16-byte boundary: 128-voxel
     // segments with 128-bit loads
-    const bool seg4 = std::is_same<TL, uint32_t>::value && lab.W % 4 == 0 &&
-                      (reinterpret_cast<uintptr_t>(lab.data) & 15) == 0;
+    const bool seg4 = sizeof(TL) == 4 && lab.W % 4 == 0 && (reinterpret_cast<uintptr_t>(lab.data) & 15) == 0;
     const int64_t tasks4 = rows * ((lab.W + 127) / 128);
     const FastDiv fs((uint32_t)((lab.W + 127) / 128));
     const int blocks4 = launch_blocks(tasks4 * 32, kST, 8);
-    if (seg4) count4_kernel<<<blocks4, kST, 0, st>>>((const uint32_t *)lab.data, (uint32_t)lab.W, (uint32_t)tasks4, fs, L, d_L, so.cnt);
+    if (seg4) count4_kernel<TL4<TL>><<<blocks4, kST, 0, st>>>((const TL4<TL> *)lab.data, (uint32_t)lab.W, (uint32_t)tasks4, fs, L, d_L, so.cnt);
     else count_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L, so.cnt);
     tile_sum_kernel<<<(unsigned)ntiles, kST, 0, st>>>(so.cnt, L, d_L, so.tsum);
     tile_scan_kernel<<<1, 1024, 0, st>>>(so.tsum, ntiles);
     offset_kernel<<<(unsigned)ntiles, kST, 0, st>>>(so.cnt, L, d_L, so.tsum, so.off, so.cursor);
-    if (seg4) scatter4_kernel<<<blocks4, kST, 0, st>>>((const uint32_t *)lab.data, (uint32_t)lab.W, (uint32_t)tasks4, fs, L, d_L,
+    if (seg4) scatter4_kernel<TL4<TL>><<<blocks4, kST, 0, st>>>((const TL4<TL> *)lab.data, (uint32_t)lab.W, (uint32_t)tasks4, fs, L, d_L,
                                                         so.cursor, so.sorted);
     else scatter_kernel<TL><<<blocks, kST, 0, st>>>((const TL *)lab.data, (uint32_t)lab.W, (uint32_t)tasks, fc, L, d_L,
                                                     so.cursor, so.sorted);

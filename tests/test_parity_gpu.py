@@ -145,9 +145,8 @@ def test_histogram_smooth_image_exact(cle, oracle, shape, bins):
 
 @pytest.mark.parametrize("bins", [256, 9])
 def test_histogram_nan_inf_given_range(cle, oracle, bins):
-    # NaN / +-inf voxels inside otherwise uniform 8-voxel groups, with the
-    # range given: those groups bin every voxel (NaN and -inf land in bin 0,
-    # +inf and values above the range in none)
+    # NaN / +-inf voxels among plateaus of equal values, with the range given
+    # (NaN and -inf land in bin 0, +inf and values above the range in none)
     r = rng(26)
     a = np.full((6, 40, 128), 250.0, np.float32)
     a[:, :, 64:] = 700.0
@@ -359,7 +358,8 @@ def test_statistics_random(cle, oracle, shape):
 
 @pytest.mark.parametrize("shape", [(3, 5, 8), (40, 260), (6, 33, 132), (2, 9, 1024)])
 @pytest.mark.parametrize("pattern", ["runs", "random", "stripes"])
-def test_statistics_row_segments(cle, oracle, shape, pattern):
+@pytest.mark.parametrize("on_device", [True, False])
+def test_statistics_row_segments(cle, oracle, shape, pattern, on_device):
     # uint32 rows of a multiple of 4 voxels take the 4-per-lane run passes:
     # runs that cross lanes and 128-voxel segments, single voxels, rows that
     # end inside a segment
@@ -375,8 +375,8 @@ def test_statistics_row_segments(cle, oracle, shape, pattern):
     lab = lab.astype(np.uint32)
     inten = r.integers(0, 4000, size=shape).astype(np.uint16)
     import torch
-    # uint32 labels on the device (a numpy label image is pushed as float32)
-    dlab = cle.B200Array(torch.from_numpy(lab).cuda())
+    # uint32 labels on the device, or a numpy label image (pushed as float32)
+    dlab = cle.B200Array(torch.from_numpy(lab).cuda()) if on_device else lab
     _assert_stats(cle.statistics_of_labelled_pixels(inten, dlab),
                   oracle.statistics_of_labelled_pixels(inten.astype(np.float32), lab))
 
