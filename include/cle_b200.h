@@ -379,6 +379,18 @@ int cle_statistics_of_labelled_pixels_device_count(const cle_tensor *intensity,
                                                    float *d_table, void *workspace,
                                                    size_t workspace_bytes, void *stream);
 
+/* ---- centroids of labels -------------------------------------------------
+ * replaces the centroid rows of _tier9/_statistics_of_labelled_pixels.py as
+ * used by _tier9/_centroids_of_labels.py: for labels 1..num_labels of a u32 /
+ * f32 label image, writes the float32 point list d_points[dim][num_labels]
+ * (dim = x, y (, z)): float32(exact coordinate sum) / float32(voxel count),
+ * the same values as the statistics table's centroid rows (NaN for a label
+ * with no voxel).  One pass over the labels; labels above num_labels and 0
+ * are ignored. */
+size_t cle_label_centroids_workspace_bytes(const cle_tensor *labels, int64_t num_labels);
+int cle_label_centroids(const cle_tensor *labels, int64_t num_labels, float *d_points,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -140,6 +140,8 @@ _SIGS = {
     "cle_vol_batch_launch": (ctypes.c_int, [_P, _T, _T, _P, _SZ, _P, _P]),
     "cle_vol_batch_free": (None, [_P]),
     "cle_workspace_status": (ctypes.c_int, [_P, _SZ, _P]),
+    "cle_label_centroids_workspace_bytes": (_SZ, [_T, ctypes.c_int64]),
+    "cle_label_centroids": (ctypes.c_int, [_T, ctypes.c_int64, _P, _P, _SZ, _P]),
     "cle_workspace_label_count": (_P, [_P]),
     "cle_statistics_of_labelled_pixels_device_count": (ctypes.c_int, [_T, _T, _P, ctypes.c_int64, _P, _P, _SZ, _P]),
     "cle_label_maximum_workspace_bytes": (_SZ, [_T]),

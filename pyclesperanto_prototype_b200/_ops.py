@@ -511,15 +511,19 @@ def centroids_of_labels(labels: Image, pointlist_destination: Image = None,
     (row 2 z in 3D), column = label (from label 0 with include_background,
     else from label 1); labels absent from the image get NaN
     (_tier9/_centroids_of_labels.py).  The coordinate sums are the statistics'
-    exact integer sums, divided by the voxel count in float32."""
+    exact integer sums, divided by the voxel count in float32, from one pass
+    over the labels (cle_label_centroids)."""
     from ._tier0 import push as _push
     labels = _push(labels)
     temp = add_image_and_scalar(labels, scalar=1)
     n = _label_max(temp)                                # labels 0 .. n-1
-    table = statistics_table(temp, temp, n)             # column j = original label j
     dims = 3 if len(labels.shape) == 3 else 2
-    rows = [table[STAT_KEYS.index(k)] for k in ("centroid_x", "centroid_y", "centroid_z")[:dims]]
-    pts = torch.stack(rows)
+    pts = torch.empty((dims, max(n, 0)), dtype=torch.float32, device=labels.tensor.device)
+    if n > 0:
+        t = _T(temp)
+        ws = _ws("cle_label_centroids_workspace_bytes", _lib.ref(t), int(n), device=labels.tensor.device)
+        _call("cle_label_centroids", _lib.ref(t), int(n), pts.data_ptr(), _ptr(ws), ws.numel(),
+              _lib.stream_ptr())                        # column j = original label j
     if not include_background:
         pts = pts[:, 1:]
     pts = pts.contiguous()

@@ -501,6 +501,21 @@ int cle_statistics_of_labelled_pixels(const cle_tensor *inten, const cle_tensor 
     return statistics(a, b, L, d_table, ar, S(stream));
 }
 
+size_t cle_label_centroids_workspace_bytes(const cle_tensor *, int64_t num_labels) {
+    return num_labels > 0 ? centroids_workspace_bytes(num_labels) : 0;
+}
+
+int cle_label_centroids(const cle_tensor *labels, int64_t num_labels, float *d_points, void *ws,
+                        size_t ws_bytes, void *stream) {
+    Img b;
+    CLE_TRY(to_img(labels, b, "label_image"));
+    if (num_labels > 0 && !d_points) { set_error("centroids: null point list"); return CLE_ERR_ARG; }
+    CLE_TRY(ws_check(ws, ws_bytes, num_labels > 0 ? centroids_workspace_bytes(num_labels) : 0, "centroids_of_labels"));
+    CLE_TRY(set_device_of(b, labels));
+    Arena ar(ws, ws_bytes);
+    return label_centroids(b, num_labels, d_points, ar, S(stream));
+}
+
 int cle_statistics_of_labelled_pixels_device_count(const cle_tensor *inten, const cle_tensor *labels,
                                                    const uint32_t *d_num_labels, int64_t capacity,
                                                    float *d_table, void *ws, size_t ws_bytes,

@@ -100,6 +100,9 @@ int masked_voronoi_dense(const Img &binary, const Img &mask, const Img &dst, int
 size_t stats_workspace_bytes(const Img &labels, int64_t L);
 int statistics(const Img &inten, const Img &labels, int64_t L, float *d_table, Arena &ws,
                cudaStream_t st, const uint32_t *d_L = nullptr);
+// centroid_x/y(/z) of labels 1..n as a float32 [dims][n] point list (pass 1 sums only)
+size_t centroids_workspace_bytes(int64_t n);
+int label_centroids(const Img &labels, int64_t n, float *pts, Arena &ws, cudaStream_t st);
 
 // pipeline.cu
 size_t vol_workspace_bytes(const Img &im);

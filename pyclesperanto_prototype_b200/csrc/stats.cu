@@ -728,6 +728,56 @@ __global__ void stats_final2(Acc2 b, int64_t L, float *__restrict__ T, const uin
 template <typename TL>
 using TL4 = typename std::conditional<sizeof(TL) == 4, TL, uint32_t>::type;
 
+// ---- centroids of labels (the point list, no second pass) ------------------
+// Per row run of label l (1..n): the voxel count and the exact 64-bit sums of
+// its x, y and z (x from the run's first voxel in closed form), added once per
+// run; then centroid = float32(sum) / float32(count), the division the
+// statistics table uses for centroid_x/y/z.
+template <typename TL>
+__global__ void __launch_bounds__(kST)
+centroid_sums_kernel(const TL *__restrict__ lab, uint32_t W, uint32_t H, uint32_t tasks, FastDiv fc,
+                     int64_t n, uint32_t *__restrict__ cnt, unsigned long long *__restrict__ sums) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t chunks = fc.d;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t0 = warp; t0 < tasks; t0 += kBatch * nwarps) {
+        uint32_t lb[kBatch], rb[kBatch], xb[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t t = t0 + (uint32_t)k * nwarps;
+            const uint32_t row = fc.div(t), x = (t - row * chunks) * 32u + (uint32_t)lane;
+            rb[k] = row;
+            xb[k] = x;
+            lb[k] = (t < tasks && x < W) ? live_label(lab, (int64_t)row * W + x, n) : 0u;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint32_t l = lb[k];
+            if (__ballot_sync(0xffffffffu, l != 0u) == 0u) continue;
+            const Run r = make_run(l);
+            if (r.tail && l) {
+                const unsigned long long len = (unsigned long long)(lane - r.head + 1);
+                const unsigned long long x0 = xb[k] - (uint32_t)(lane - r.head);
+                const uint32_t y = rb[k] % H, z = rb[k] / H;
+                const int64_t i = (int64_t)l - 1;
+                atomicAdd(cnt + i, (uint32_t)len);
+                atomicAdd(sums + 3 * i, len * x0 + len * (len - 1) / 2);
+                atomicAdd(sums + 3 * i + 1, len * y);
+                atomicAdd(sums + 3 * i + 2, len * z);
+            }
+        }
+    }
+}
+
+__global__ void centroid_final_kernel(const uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ sums,
+                                      int64_t n, int dims, float *__restrict__ pts) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float area = (float)cnt[i];
+        for (int d = 0; d < dims; ++d) pts[d * n + i] = __fdiv_rn((float)sums[3 * i + d], area);
+    }
+}
+
 template <typename TL, typename TI>
 int stats_typed(const Img &inten, const Img &lab, int64_t L, float *T, const Acc1 &a, const Acc2 &b,
                 const Sorted &so, cudaStream_t st, const uint32_t *d_L) {
@@ -810,6 +860,42 @@ int statistics(const Img &inten, const Img &lab, int64_t L, float *T, Arena &ws,
         case CLE_U8: return stats_i<uint8_t>(inten, lab, L, T, a, b, so, st, d_L);
         default: set_error("statistics: unsupported label dtype %d", lab.dtype); return CLE_ERR_DTYPE;
     }
+}
+
+size_t centroids_workspace_bytes(int64_t n) {
+    Arena a(nullptr, 0);
+    a.take<uint32_t>(n);
+    a.take<unsigned long long>(3 * n);
+    return a.off;
+}
+
+int label_centroids(const Img &lab, int64_t n, float *pts, Arena &ws, cudaStream_t st) {
+    if (n < 0 || n > 0x7FFFFFFF) { set_error("centroids: bad label count %lld", (long long)n); return CLE_ERR_ARG; }
+    if (n == 0) return CLE_OK;
+    uint32_t *cnt = ws.take<uint32_t>(n);
+    unsigned long long *sums = ws.take<unsigned long long>(3 * n);
+    if (!ws.ok()) { set_error("centroids: workspace too small"); return CLE_ERR_WORKSPACE; }
+    CLE_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * n, st));
+    CLE_CUDA(cudaMemsetAsync(sums, 0, sizeof(unsigned long long) * 3 * n, st));
+    const int64_t rows = lab.D * lab.H;
+    const int64_t tasks = rows * ((lab.W + 31) / 32);
+    if (tasks > 0xFFFFFFFFll) { set_error("centroids: image too large"); return CLE_ERR_TOO_LARGE; }
+    const int blocks = launch_blocks(tasks * 32, kST, 8);
+    const FastDiv fc((uint32_t)((lab.W + 31) / 32));
+    switch (lab.dtype) {
+        case CLE_U32:
+            centroid_sums_kernel<uint32_t><<<blocks, kST, 0, st>>>((const uint32_t *)lab.data, (uint32_t)lab.W,
+                                                                 (uint32_t)lab.H, (uint32_t)tasks, fc, n, cnt, sums);
+            break;
+        case CLE_F32:
+            centroid_sums_kernel<float><<<blocks, kST, 0, st>>>((const float *)lab.data, (uint32_t)lab.W,
+                                                              (uint32_t)lab.H, (uint32_t)tasks, fc, n, cnt, sums);
+            break;
+        default: set_error("centroids: unsupported label dtype %d", lab.dtype); return CLE_ERR_DTYPE;
+    }
+    centroid_final_kernel<<<launch_blocks(n, 256), 256, 0, st>>>(cnt, sums, n, lab.ndim == 3 ? 3 : 2, pts);
+    CLE_LAUNCH_CHECK_N("centroids", 2);
+    return CLE_OK;
 }
 
 }  // namespace cle

@@ -176,3 +176,21 @@ def test_centroids_of_labels_point_lists(cle, oracle):
     assert _close(with_bg[:, 1:], ref, RTOL)
     bg = np.argwhere(lab == 0)
     assert np.allclose(with_bg[:, 0], bg[:, ::-1].mean(axis=0), rtol=RTOL)
+
+
+@pytest.mark.parametrize("shape", [(40, 100), (6, 33, 70)])
+def test_centroids_of_labels_device_runs(cle, oracle, shape):
+    # uint32 labels on the device with runs longer than a warp's 32 voxels and
+    # an absent label (NaN column): one pass of per-run coordinate sums
+    import torch
+    rng = np.random.default_rng(6)
+    lab = np.repeat(rng.integers(0, 7, size=shape[:-1] + (shape[-1] // 9 + 1,)), 9, axis=-1)[..., :shape[-1]]
+    lab = np.ascontiguousarray(lab).astype(np.uint32)
+    lab[lab == 3] = 0
+    st = oracle.statistics_of_labelled_pixels(np.zeros(lab.shape, np.float32), lab)
+    keys = ["centroid_x", "centroid_y", "centroid_z"][:len(shape)]
+    ref = np.stack([st[k] for k in keys])
+    got = cle.pull(cle.centroids_of_labels(cle.B200Array(torch.from_numpy(lab).cuda())))
+    assert got.shape == ref.shape
+    assert _close(got, ref, RTOL)
+    assert np.all(np.isnan(got[:, 2]))   # label 3 is absent
