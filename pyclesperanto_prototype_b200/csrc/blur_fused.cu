@@ -32,6 +32,7 @@
 // saves threshold_otsu's separate pass over the blurred image.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <atomic>
 #include <cstring>
 
 #include "common.cuh"
@@ -443,22 +444,36 @@ dim3 fused_grid(const Img &src, int R, int &zchunk) {
 // The source as a 3D tiled tensor map (x = W innermost) with the box of
 // TmaGeom<Tin, R>; false when the layout does not allow one (row pitch or base
 // address not a multiple of 16 bytes) or the driver lacks the encoder.
+// The driver's tensor-map encoder, looked up once outside any stream capture
+// (an immutable function pointer; until then, and if the driver lacks it,
+// the register-staged path runs).
+void *tensor_map_encoder(cudaStream_t st) {
+    static std::atomic<void *> fn{nullptr};
+    static std::atomic<bool> looked{false};
+    if (looked.load(std::memory_order_acquire)) return fn.load(std::memory_order_acquire);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        (void)cudaGetLastError();
+        return nullptr;
+    }
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+        (void)cudaGetLastError();
+        f = nullptr;
+    }
+    fn.store(f, std::memory_order_release);
+    looked.store(true, std::memory_order_release);
+    return f;
+}
+
 template <typename Tin, int R>
-bool encode_source_map(const Img &src, CUtensorMap &map) {
+bool encode_source_map(const Img &src, CUtensorMap &map, cudaStream_t st) {
     using TG = TmaGeom<Tin, R>;
     const uint64_t pitch = (uint64_t)src.W * sizeof(Tin);
     if (pitch % 16 != 0 || (reinterpret_cast<uintptr_t>(src.data) & 15) != 0) return false;
-    // the driver's encoder, resolved once (an immutable function pointer)
-    static void *const fn = [] {
-        void *f = nullptr;
-        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess) {
-            (void)cudaGetLastError();
-            f = nullptr;
-        }
-        return f;
-    }();
+    void *const fn = tensor_map_encoder(st);
     if (fn == nullptr) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)src.W, (cuuint64_t)src.H, (cuuint64_t)src.D};
     const cuuint64_t strides[2] = {(cuuint64_t)pitch, (cuuint64_t)(pitch * (uint64_t)src.H)};
@@ -491,7 +506,7 @@ int launch_fused_r(const Img &src, float *dst, const Taps &t, float *mm, int *st
         cudaGetDevice(&dev);
         const int64_t ctas = (int64_t)grid.x * grid.y * grid.z;
         const bool waves2 = ctas >= 2 * (int64_t)num_sms(dev) * min_ctas<R>();
-        if (status != nullptr && waves2 && encode_source_map<Tin, R>(src, map)) {
+        if (status != nullptr && waves2 && encode_source_map<Tin, R>(src, map, st)) {
             auto kern = blur_fused_kernel<Tin, R, true, true>;
             const size_t smem = TmaGeom<Tin, R>::SMEM;
             // set on every call: the attribute belongs to the current device's context

@@ -92,3 +92,21 @@ def test_batch_plan_tuned_lanes_and_shape_check(cle):
     st = lib.cle_vol_batch_launch(b._plan, wrong, b._out, b.ws.data_ptr(), b.ws.numel(), b.status.data_ptr(),
                                   torch.cuda.current_stream().cuda_stream)
     assert st == 2 and b"planned" in lib.cle_last_error_message()
+
+
+def test_batch_graph_with_tma_staged_blur(cle):
+    # a uint16 volume whose blur grid fills two waves takes the TMA-staged blur;
+    # captured in the batch's CUDA graph it gives the per-call labels
+    from pyclesperanto_prototype_b200 import synthetic
+    from pyclesperanto_prototype_b200.batch import VolBatch
+    vol = torch.from_numpy(synthetic.nuclei_volume((64, 704, 1000), 400, seed=9)).cuda()
+    small = torch.from_numpy(synthetic.nuclei_volume((24, 96, 112), 40, seed=3)).cuda()
+    b = VolBatch([vol, small], spot_sigma=2.0, outline_sigma=2.0, lanes=2, use_graph=True)
+    b.run()
+    b.run()
+    torch.cuda.synchronize()
+    b.check()
+    for t, out in zip([vol, small], b.outputs):
+        ref = cle.voronoi_otsu_labeling(cle.B200Array(t), spot_sigma=2.0, outline_sigma=2.0)
+        assert torch.equal(out, ref.tensor)
+        assert int(ref.tensor.to(torch.int64).max()) > 0
