@@ -47,16 +47,31 @@ __global__ void replace_kernel(const Ts *__restrict__ src, const float *__restri
 
 // pts: row r (x, y, z) of the point list at pts[r * m + label]; label index
 // read like replace_kernel's (clamped to the list)
+// (x, y, z) of voxel i: 32-bit multiply-shift divisions while the image has
+// under 2^32 voxels, 64-bit division otherwise
 template <typename Ts, typename Td>
 __global__ void centroid_distance_kernel(const Ts *__restrict__ src, const float *__restrict__ pts, int64_t m,
-                                         int dims, int64_t W, int64_t H, Td *__restrict__ dst, int64_t n) {
+                                         int dims, int64_t W, int64_t H, FastDiv fW, FastDiv fH,
+                                         Td *__restrict__ dst, int64_t n) {
+    const bool small = n <= 0xFFFFFFFFll;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float v = (float)src[i];
         int64_t k = (v != v) ? 0 : (int64_t)fmaxf(fminf(v, 2147483647.0f), -2147483648.0f);
         float d = 0.0f;
         if (k != 0) {
             k = k < 0 ? 0 : (k >= m ? m - 1 : k);
-            const int64_t x = i % W, r = i / W, y = r % H, z = r / H;
+            int64_t x, y, z;
+            if (small) {
+                const uint32_t r = fW.div((uint32_t)i), q = fH.div(r);
+                x = (uint32_t)i - r * fW.d;
+                y = r - q * fH.d;
+                z = q;
+            } else {
+                const int64_t r = i / W;
+                x = i % W;
+                y = r % H;
+                z = r / H;
+            }
             const float dx = __fsub_rn((float)x, pts[k]);
             const float dy = __fsub_rn((float)y, pts[m + k]);
             float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
@@ -74,11 +89,12 @@ template <typename Ts>
 int centroid_distance_dst(const Img &s, const float *pts, int64_t m, int dims, const Img &d, cudaStream_t st) {
     const int64_t n = s.n();
     const int b = launch_blocks(n, 256);
+    const FastDiv fW((uint32_t)std::min<int64_t>(s.W, 0xFFFFFFFFll)), fH((uint32_t)std::min<int64_t>(s.H, 0xFFFFFFFFll));
     switch (d.dtype) {
-        case CLE_F32: centroid_distance_kernel<Ts, float><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, (float *)d.data, n); break;
-        case CLE_U32: centroid_distance_kernel<Ts, uint32_t><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, (uint32_t *)d.data, n); break;
-        case CLE_U16: centroid_distance_kernel<Ts, uint16_t><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, (uint16_t *)d.data, n); break;
-        case CLE_U8: centroid_distance_kernel<Ts, uint8_t><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, (uint8_t *)d.data, n); break;
+        case CLE_F32: centroid_distance_kernel<Ts, float><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, fW, fH, (float *)d.data, n); break;
+        case CLE_U32: centroid_distance_kernel<Ts, uint32_t><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, fW, fH, (uint32_t *)d.data, n); break;
+        case CLE_U16: centroid_distance_kernel<Ts, uint16_t><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, fW, fH, (uint16_t *)d.data, n); break;
+        case CLE_U8: centroid_distance_kernel<Ts, uint8_t><<<b, 256, 0, st>>>((const Ts *)s.data, pts, m, dims, s.W, s.H, fW, fH, (uint8_t *)d.data, n); break;
         default: set_error("euclidean_distance_from_label_centroid_map: unsupported destination dtype %d", d.dtype); return CLE_ERR_DTYPE;
     }
     CLE_LAUNCH_CHECK("euclidean_distance_from_label_centroid_map");

@@ -137,7 +137,7 @@ template <typename T>
 __global__ void __launch_bounds__(kHistThreads)
 hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int bins,
                  int zchunk, const float *__restrict__ d_minmax, uint32_t *__restrict__ part,
-                 FastDiv fw) {
+                 FastDiv fw, FastDiv fw4) {
     extern __shared__ uint32_t sh[];   // (warps x bins) when private, else bins
     const int nwarps = kHistThreads / 32;
     const bool priv = bins <= 512;
@@ -178,7 +178,7 @@ hist_rows_kernel(const T *__restrict__ src, int64_t D, int64_t H, int64_t W, int
                 for (int k = 0; k < 2; ++k) {
                     const uint32_t j = base + k * kHistThreads + threadIdx.x;
                     ok[k] = j < span4;
-                    const uint32_t zz = j / W4, x4 = j - zz * W4;
+                    const uint32_t zz = fw4.div(j), x4 = j - zz * W4;
                     q[k] = ok[k] ? __ldg(reinterpret_cast<const float4 *>(src + ((z0 + zz) * H + y) * W) + x4)
                                  : make_float4(0.f, 0.f, 0.f, 0.f);
                 }
@@ -488,15 +488,15 @@ int histogram(const Img &im, int bins, const float *d_minmax, float *d_hist, Are
     switch (im.dtype) {
         case CLE_F32:
             if (smem > 48 * 1024) CLE_CUDA(cudaFuncSetAttribute(hist_rows_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            hist_rows_kernel<float><<<grid, kHistThreads, smem, st>>>((const float *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W));
+            hist_rows_kernel<float><<<grid, kHistThreads, smem, st>>>((const float *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W), FastDiv((uint32_t)std::max<int64_t>(1, im.W / 4)));
             break;
         case CLE_U16:
             if (smem > 48 * 1024) CLE_CUDA(cudaFuncSetAttribute(hist_rows_kernel<uint16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            hist_rows_kernel<uint16_t><<<grid, kHistThreads, smem, st>>>((const uint16_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W));
+            hist_rows_kernel<uint16_t><<<grid, kHistThreads, smem, st>>>((const uint16_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W), FastDiv((uint32_t)std::max<int64_t>(1, im.W / 4)));
             break;
         case CLE_U8:
             if (smem > 48 * 1024) CLE_CUDA(cudaFuncSetAttribute(hist_rows_kernel<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            hist_rows_kernel<uint8_t><<<grid, kHistThreads, smem, st>>>((const uint8_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W));
+            hist_rows_kernel<uint8_t><<<grid, kHistThreads, smem, st>>>((const uint8_t *)im.data, im.D, im.H, im.W, bins, zchunk, d_minmax, part, FastDiv((uint32_t)im.W), FastDiv((uint32_t)std::max<int64_t>(1, im.W / 4)));
             break;
         default: set_error("histogram: unsupported dtype %d", im.dtype); return CLE_ERR_DTYPE;
     }
