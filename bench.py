@@ -131,17 +131,17 @@ PIPELINE_BYTES_PER_VOXEL = 8 + 4 + 10 + 6 + 8
 # dram__bytes_write.sum, or the DRAM bandwidth x the duration of the same
 # launch); the captures are summarised in profiles/<kernel>_<workload>.md.
 MEASURED_TRAFFIC = {
-    "nuclei": {"voronoi_growth": (360.142e6 + 89.806e6, "voronoi_bricks_kernel_nuclei_128x512x512.md"),
+    "nuclei": {"voronoi_growth": (0.347e9, "voronoi_keys_kernel_nuclei_128x512x512.md"),
                "blur_spot": (67.164e6 + 81.208e6, "blur_fused_kernel_nuclei_128x512x512.md"),
                "blur_outline": (67.155e6 + 81.081e6, "blur_fused_kernel_nuclei_128x512x512.md"),
                "detect_maxima": (135.090e6 + 19.932e6, "maxima_kernel_nuclei_128x512x512.md"),
                },
     # slab captures (128x1024x1024) scaled by 4 to the 512x1024x1024 volume:
     # the same recipe and cell density, traffic in proportion to the voxels
-    "lightsheet": {"voronoi_growth": (4 * 3.668e9, "voronoi_bricks_kernel_lightsheet_slab_128x1024x1024.md"),
+    "lightsheet": {"voronoi_growth": (4 * 1.713e9, "voronoi_keys_kernel_lightsheet_slab_128x1024x1024.md"),
                    "blur_spot": (4 * 0.792e9, "blur_fused_kernel_lightsheet_slab_128x1024x1024.md"),
                    "threshold_seeds": (4 * 1.165e9, "maxima_seeds_kernel_lightsheet_slab_128x1024x1024.md")},
-    "lightsheet_slab": {"voronoi_growth": (3.668e9, "voronoi_bricks_kernel_lightsheet_slab_128x1024x1024.md"),
+    "lightsheet_slab": {"voronoi_growth": (1.713e9, "voronoi_keys_kernel_lightsheet_slab_128x1024x1024.md"),
                         "blur_spot": (0.792e9, "blur_fused_kernel_lightsheet_slab_128x1024x1024.md"),
                         "threshold_seeds": (1.165e9, "maxima_seeds_kernel_lightsheet_slab_128x1024x1024.md")},
 }

@@ -92,6 +92,10 @@ struct Arena {
 // Device helpers
 // ---------------------------------------------------------------------------
 static constexpr uint32_t kMarkBit = 0x80000000u;
+// Mask byte of a voxel inside the segmentation, as the seed passes write it
+// (0 outside).  The key growth keeps a voxel's arrival step in the low 7 bits
+// once the voxel is labelled; all ones there stands for "not yet known".
+static constexpr uint8_t kMaskByte = 0xFF;
 static constexpr int kMaxTaps = 1025;
 
 struct Taps {

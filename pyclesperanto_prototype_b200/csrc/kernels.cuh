@@ -51,6 +51,16 @@ int erode_box(const Img &src, const Img &dst, cudaStream_t st);
 int add_image_and_scalar(const Img &src, const Img &dst, float c, cudaStream_t st);
 int replace_intensities(const Img &src, const Img &map, const Img &dst, cudaStream_t st);
 int centroid_distance_map(const Img &labels, const Img &pts, const Img &dst, cudaStream_t st);
+// neighbors.cu: distance / touch matrices and the neighbour-distance vectors
+int generate_distance_matrix(const Img &list1, const Img &list2, const Img &dst, cudaStream_t st);
+int generate_touch_matrix(const Img &labels, const Img &dst, cudaStream_t st);
+int average_distance_of_n_distances(const Img &dm, int n, int exclude_self, const Img &dst, cudaStream_t st);
+int average_distance_of_touching_neighbors(const Img &dm, const Img &tm, const Img &dst, cudaStream_t st);
+int average_distance_of_n_points(const Img &list1, const Img &list2, int n, int exclude_self, const Img &dst,
+                                 cudaStream_t st);
+size_t touching_labels_workspace_bytes(int64_t num_labels);
+int average_distance_of_touching_labels(const Img &labels, const Img &pts, const Img &dst, Arena &ws,
+                                        cudaStream_t st);
 
 size_t box_filter_workspace_bytes(const Img &im);
 int box_filter(const Img &src, const Img &dst, double rx, double ry, double rz, bool is_max, Arena &ws,
@@ -89,9 +99,21 @@ size_t voronoi_frontier_workspace_bytes(const Img &im);
 // Frontier-queued Jacobi growth.  labels: u32 with seed labels, 0 elsewhere;
 // seg: u8 mask (0/1); seeds: device list of seed memory indices (count in
 // d_seed_count).  d_status receives 0 or an error.
+// gate: when set, the launch returns at once unless *gate != 0 on the device.
 int voronoi_frontier(const Img &shape, uint32_t *labels, const uint8_t *seg,
                      const uint32_t *seeds, const uint32_t *d_seed_count, int *d_status,
-                     Arena &ws, cudaStream_t st, const Limits &lim);
+                     Arena &ws, cudaStream_t st, const Limits &lim, const int *gate = nullptr);
+// The same growth by arrival keys (bricks relaxed to convergence per visit,
+// rounds instead of steps), for labels up to 2^24 - 1 (d_max_label: the
+// largest seed label on the device) and up to 120 steps; otherwise the labels
+// are left as given and the frontier kernel above grows them.  seg: mask
+// bytes as the seed passes write them (kMaskByte); the growth keeps each
+// labelled voxel's arrival step in them.  Workspace includes the frontier
+// kernel's.
+size_t voronoi_grow_workspace_bytes(const Img &im);
+int voronoi_grow(const Img &shape, uint32_t *labels, uint8_t *seg, const uint32_t *seeds,
+                 const uint32_t *d_seed_count, const uint32_t *d_max_label, int *d_status, Arena &ws,
+                 cudaStream_t st, const Limits &lim);
 size_t voronoi_dense_workspace_bytes(const Img &im);
 int masked_voronoi_dense(const Img &binary, const Img &mask, const Img &dst, int *d_status,
                          Arena &ws, cudaStream_t st, const Limits &lim);

@@ -169,7 +169,7 @@ maxima_seeds_kernel(const float *__restrict__ T, const float *__restrict__ d_thr
                 }
                 const bool sg = v > t;
                 seed = sg && win;
-                seg[m] = sg ? 1 : 0;
+                seg[m] = sg ? kMaskByte : 0;
                 lab[m] = seed ? xyz2k(g, (uint32_t)x, (uint32_t)(y0 + j), (uint32_t)z) + 1u : 0u;
             }
             const unsigned b = __ballot_sync(0xffffffffu, seed);
@@ -265,7 +265,7 @@ maxima_seeds2_kernel(const float *__restrict__ T, const float *__restrict__ d_th
                 const bool ga = va > t, gb = vb > t;
                 seed_a = ga && wa;
                 seed_b = gb && wb;
-                *reinterpret_cast<uint16_t *>(seg + m) = (uint16_t)((ga ? 1u : 0u) | (gb ? 0x100u : 0u));
+                *reinterpret_cast<uint16_t *>(seg + m) = (uint16_t)((ga ? (uint32_t)kMaskByte : 0u) | (gb ? (uint32_t)kMaskByte << 8 : 0u));
                 uint2 lv = make_uint2(0u, 0u);
                 if (seed_a | seed_b) {
                     const uint32_t k = xyz2k(g, (uint32_t)xa, (uint32_t)(y0 + j), (uint32_t)z) + 1u;

@@ -49,7 +49,7 @@ __global__ void seeds_kernel(const float *__restrict__ T, const uint8_t *__restr
                 m2xyz(g, (uint32_t)i, x, y, z);
                 key = xyz2k(g, x, y, z) + 1u;
             }
-            seg[i] = s ? 1 : 0;
+            seg[i] = s ? kMaskByte : 0;
             lab[i] = key;
         }
         const unsigned b = __ballot_sync(0xffffffffu, seed);
@@ -83,7 +83,7 @@ __global__ void mask_seeds_kernel(const Tb *__restrict__ bin, const Tm *__restri
                 m2xyz(g, (uint32_t)i, x, y, z);
                 key = xyz2k(g, x, y, z) + 1u;
             }
-            seg[i] = s ? 1 : 0;
+            seg[i] = s ? kMaskByte : 0;
             lab[i] = key;
         }
         const unsigned b = __ballot_sync(0xffffffffu, seed);
@@ -158,7 +158,7 @@ int launch_mask_seeds(const Img &bin, const Img &mask, const Geo &g, const BinLa
 size_t masked_voronoi_binary_workspace_bytes(const Img &im) {
     Arena a(nullptr, 0);
     take_bin_layout(a, im);
-    size_t tail = std::max(rank_workspace_bytes(fkey_bits_for(im.n())), voronoi_frontier_workspace_bytes(im));
+    size_t tail = std::max(rank_workspace_bytes(fkey_bits_for(im.n())), voronoi_grow_workspace_bytes(im));
     return a.off + tail;
 }
 
@@ -187,7 +187,8 @@ int masked_voronoi_binary(const Img &bin, const Img &mask, const Img &dst, Arena
     }
     CLE_TRY(ccl_list(g, bin.n(), lab, l.seeds, &l.sc->seed_count, bin.n(), ws, st, &l.sc->nlabels));
     ws.off = tail_off;
-    CLE_TRY(voronoi_frontier(bin, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st, lim));
+    CLE_TRY(voronoi_grow(bin, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->nlabels, &l.sc->status, ws, st,
+                         lim));
     if (dst.dtype == CLE_F32) {
         u32_to_f32<<<launch_blocks(dst.n(), 256), 256, 0, st>>>(lab, (float *)dst.data, dst.n());
         CLE_LAUNCH_CHECK("labels to f32");
@@ -362,7 +363,7 @@ size_t vol_workspace_bytes(const Img &im) {
     tail = std::max(tail, minmax_workspace_bytes(im) + histogram_workspace_bytes(im, 256));
     tail = std::max(tail, blur_minmax_workspace_bytes(im));
     tail = std::max(tail, rank_workspace_bytes(fkey_bits_for(im.n())));
-    tail = std::max(tail, voronoi_frontier_workspace_bytes(im));
+    tail = std::max(tail, voronoi_grow_workspace_bytes(im));
     return base + tail;
 }
 
@@ -441,7 +442,8 @@ int voronoi_otsu_labeling(const Img &src, const Img &dst, double spot_sigma, dou
     stage_mark(6, st);
 
     // 9: grow inside the segmentation
-    CLE_TRY(voronoi_frontier(src, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->status, ws, st, lim));
+    CLE_TRY(voronoi_grow(src, lab, l.seg, l.seeds, &l.sc->seed_count, &l.sc->nlabels, &l.sc->status, ws, st,
+                         lim));
     ws.off = tail_off;
     stage_mark(7, st);
 

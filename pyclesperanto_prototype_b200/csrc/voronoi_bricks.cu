@@ -150,9 +150,10 @@ __device__ __forceinline__ bool neighbour_brick(const BGeo &G, uint32_t zb, uint
     return true;
 }
 
-// Exclusive prefix of v over the CTA (kBT threads); total of the CTA in `total`.
+// Exclusive prefix of v over the CTA (up to 1024 threads); total of the CTA in `total`.
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *s_w, uint32_t &total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (int)(blockDim.x >> 5);
     uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -163,16 +164,16 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t *s_w, u
     if (lane == 31) s_w[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < kWPB ? s_w[lane] : 0u;
+        uint32_t w = lane < nw ? s_w[lane] : 0u;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += y;
         }
-        if (lane < kWPB) s_w[lane] = w;
+        if (lane < nw) s_w[lane] = w;
     }
     __syncthreads();
-    total = s_w[kWPB - 1];
+    total = s_w[nw - 1];
     return (warp ? s_w[warp - 1] : 0u) + x - v;
 }
 
@@ -184,7 +185,7 @@ __device__ __forceinline__ uint32_t block_total(uint32_t v, uint32_t *red) {
     __syncthreads();
     uint32_t s = 0;
     if (threadIdx.x == 0)
-        for (int i = 0; i < kWPB; ++i) s += red[i];
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
     return s;   // thread 0
 }
 
@@ -212,7 +213,8 @@ __device__ __forceinline__ void queue_neighbours(const BGeo &G, uint32_t zb, uin
 // Two-pass grid compaction of the queue bitmap (q & ~done) into the list F in
 // brick-index order, its length in *nsize; clears q.  Grid-wide: every CTA
 // calls it; returns false when a barrier gave up.
-__device__ bool compact_queue(const BQueue &Qb, uint32_t *F, uint32_t *nsize, BState *S, uint64_t barrier_ns,
+template <typename St>
+__device__ bool compact_queue(const BQueue &Qb, uint32_t *F, uint32_t *nsize, St *S, uint64_t barrier_ns,
                               uint32_t *s_red, uint32_t *s_scan, uint32_t *s_off) {
     // pass 1: each CTA counts the queued bricks of its contiguous range of
     // bitmap words
@@ -266,10 +268,14 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
                       const uint32_t *seeds, const uint32_t *d_seed_count, uint32_t *B0,
                       uint32_t *B1, uint32_t *Mv, uint32_t *Pf, uint32_t *bstep, BState *S, int *d_status,
                       uint32_t max_steps, uint64_t loop_ns, uint64_t barrier_ns,
-                      const volatile int *cancel, unsigned long long *trace, BQueue Qb, int use_bitmap) {
+                      const volatile int *cancel, unsigned long long *trace, BQueue Qb, int use_bitmap,
+                      const int *gate) {
     __shared__ uint32_t s_red[kWPB];
     __shared__ uint32_t s_scan[kWPB];
     __shared__ uint32_t s_off[2];
+    // after the key growth (below) this launch only runs when that kernel
+    // handed the growth back (every CTA reads the same word)
+    if (gate && *(const volatile int *)gate == 0) return;
     const Geo &g = G.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpAppender ap{&S->err, 0u};
@@ -500,6 +506,451 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
     }
 }
 
+// ---- growth by arrival keys ---------------------------------------------------
+// The same labels as the Jacobi steps above, without a grid barrier per step.
+// A voxel the growth labels has an arrival step A (the step that writes it)
+// and a label; with s = A + 1 (seeds: s = 0) the reference's steps give
+//   s(v) = min over labelled neighbours u of   s(u) + 1         for a face neighbour,
+//                                              (s(u) + 1) | 1   for an edge / corner
+//                                              neighbour (box steps only: odd s),
+//   label(v) = the largest label among the neighbours that reach v at s(v).
+// So v's key K = s << 24 | (0xFFFFFF - label) is the minimum over its
+// neighbours of their keys sent through those two maps (the second map is
+// applied to each neighbour before the minimum: it merges pairs of steps, so
+// it does not commute with the minimum).  Re-evaluating voxels in any order
+// reaches that fixpoint -- the s part only decreases, and the label part then
+// settles in order of s -- so a warp relaxes its brick against the brick's
+// halo until nothing changes within one visit, and a brick is visited again
+// only when a neighbouring brick changes a voxel next to it.  Rounds of
+// visits are separated by grid barriers; a round ends the growth when it
+// queues nothing.
+//
+// The reference's loop stops at the first step that labels nothing: with S
+// the smallest s >= 1 that no voxel holds, voxels of s > S stay unlabelled,
+// and a last pass turns the kept keys into labels.  Per-CTA counts of the
+// voxels per s (kept up to date at every write) give S.
+//
+// The label buffer holds, during the growth: 0 (unlabelled or outside the
+// mask), a seed's label L (s = 0), or s << 24 | L for a grown voxel; the key
+// of a stored value p != 0 is p ^ 0xFFFFFF.  Labels above 2^24 - 1 or an s
+// above kKeyMaxS do not fit: the kernel then leaves the labels as it found
+// them and raises the gate word, and the brick kernel grows them instead.
+
+constexpr uint32_t kKInf = 0xFFFFFFFFu;
+constexpr uint32_t kKS1 = 0x01000000u;
+constexpr uint32_t kKeyMaxS = 120;   // steps fit the mask byte's 7 bits (127 = not yet known)
+constexpr int kKeyIters = 32;     // local iterations per visit; a brick still changing re-queues itself
+#ifndef CLE_KEY_BT
+#define CLE_KEY_BT 1024
+#endif
+constexpr int kKeyBT = CLE_KEY_BT; // threads per CTA of the key kernel (1024: light-sheet 4.10 ms vs 4.63 at 768)
+
+struct KState {
+    GridBarrier bar;
+    int err;
+    int gate;          // 1: the brick kernel grows the labels after this launch
+    int overflow;      // an s above kKeyMaxS was reached
+    uint32_t sizes[4];
+    uint32_t rounds;
+    uint32_t stop_s;   // S
+    uint32_t visits;
+    int hist[256];     // grown voxels per s
+};
+
+// key of a voxel from its label p and mask byte sg (the arrival step in its
+// low 7 bits once labelled; labels fit 24 bits).  A label read together with
+// a step field still at 127 ("not yet known": the byte of a voxel another
+// warp is labelling right now) counts as unlabelled -- a value that is never
+// below the voxel's true key, and the writer queues this brick again.
+__device__ __forceinline__ uint32_t key_of(uint32_t p, uint32_t sg) {
+    return (p && (sg & 0x7Fu) != 0x7Fu) ? (((sg & 0x7Fu) << 24) | (p ^ 0x00FFFFFFu)) : kKInf;
+}
+__device__ __forceinline__ uint32_t key_face(uint32_t k) { return k == kKInf ? kKInf : k + kKS1; }
+__device__ __forceinline__ uint32_t key_diag(uint32_t k) { return k == kKInf ? kKInf : ((k + kKS1) | kKS1); }
+
+template <bool IS3D, int BZ, int KBT>
+__global__ void __launch_bounds__(KBT, 1)
+voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
+                    const uint32_t *d_seed_count, const uint32_t *d_max_label, uint32_t *B0, uint32_t *B1,
+                    uint32_t *bstep, uint32_t *touched, KState *S, int *d_status, uint32_t max_steps,
+                    uint64_t loop_ns, uint64_t barrier_ns, const volatile int *cancel,
+                    unsigned long long *trace, BQueue Qb, int use_bitmap) {
+    constexpr int NW = KBT / 32;
+    constexpr int ZR = IS3D ? 1 : 0;
+    constexpr int K = BZ + 2 * ZR;
+    __shared__ uint32_t s_red[NW];
+    __shared__ uint32_t s_scan[NW];
+    __shared__ uint32_t s_off[2];
+    __shared__ int s_hist[256];
+    const Geo &g = G.g;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    WarpAppender ap{&S->err, 0u};
+    const uint64_t t_entry = global_ns();
+    // labels that do not fit 24 bits: the brick kernel takes over (uniform)
+    if (__ldcg(d_max_label) > 0x00FFFFFFu) {
+        if (gtid == 0) S->gate = 1;
+        return;
+    }
+    for (int i = threadIdx.x; i < 256; i += KBT) s_hist[i] = 0;
+
+    // round 0: each seed's brick and the neighbouring bricks the seed touches
+    // (a seed on a brick's face, edge or corner); the growth reaches every
+    // other brick through a changed voxel next to it
+    const uint32_t ns = __ldcg(d_seed_count);
+    for (uint32_t base = blockIdx.x * NW; base < ns; base += gridDim.x * NW) {
+        const uint32_t i = base + warp;
+        if (i < ns) {
+            const uint32_t m = __ldcg(seeds + i);
+            if (lane == 0) seg[m] = 0x80u;   // in the mask, arrival step 0
+            uint32_t x, y, z;
+            m2xyz(g, m, x, y, z);
+            const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+            const uint32_t xr = x % kBX, yr = y % kBY, zr = z % BZ;
+            const bool touch = (dxb == 0 || (dxb < 0 ? xr == 0 : xr == kBX - 1)) &&
+                               (dyb == 0 || (dyb < 0 ? yr == 0 : yr == kBY - 1)) &&
+                               (dz == 0 || (dz < 0 ? zr == 0 : zr == (uint32_t)BZ - 1));
+            const bool want = lane < 27 && (IS3D || dz == 0) && touch;
+            if (use_bitmap) {
+                uint32_t nb = 0;
+                if (want && neighbour_brick(G, z / BZ, y / kBY, x / kBX, lane, nb))
+                    atomicOr(Qb.q + (nb >> 5), 1u << (nb & 31u));
+            } else {
+                queue_neighbours(G, z / BZ, y / kBY, x / kBX, want, 1u, bstep, ap);
+            }
+        }
+        if (!use_bitmap) ap.maybe_flush(B0, &S->sizes[0]);
+    }
+    if (!use_bitmap) ap.flush(B0, &S->sizes[0]);
+    bool ok = grid_sync(&S->bar, &S->err, barrier_ns);
+    if (use_bitmap && ok) ok = compact_queue(Qb, B0, &S->sizes[0], S, barrier_ns, s_red, s_scan, s_off);
+
+    // the lane's column and halo voxel (as in the brick kernel)
+    const int xl = lane & (kBX - 1), yl = lane / kBX;
+    const bool x0 = xl == 0, x1 = xl == kBX - 1, y0 = yl == 0, y1 = yl == kBY - 1;
+    const int src_h = yl == 0 ? xl : 8 + xl;
+    const int src_s = (xl == 0 ? 16 : 20) + (yl & 3);
+    const int src_q = 24 + (yl == kBY - 1 ? 2 : 0) + (xl == kBX - 1 ? 1 : 0);
+
+    const uint64_t t_start = global_ns();
+    // trace: the last two rows hold the set-up (round 0's queue) and the
+    // finish (counts, S, conversion) times
+    if (trace && gtid == 0) trace[4 * (kTraceSteps - 2)] = t_start - t_entry;
+    const uint32_t max_rounds = max_steps > 0x0FFFFFFFu ? 0xFFFFFFFFu : 4u * max_steps + 64u;
+    uint32_t r = 0, visits = 0;
+    bool done = false;
+    while (ok && r < max_rounds) {
+        uint32_t iters = 0;
+        if (gtid == 0) {
+            if (global_ns() - t_start > loop_ns) atomicExch(&S->err, (int)CLE_ERR_ITER_LIMIT);
+            else if (cancel && *cancel) atomicExch(&S->err, (int)CLE_ERR_CANCELLED);
+        }
+        const uint32_t *F = (r & 1) ? B1 : B0;
+        uint32_t *Fn = (r & 1) ? B0 : B1;
+        const uint32_t nB = __ldcg(&S->sizes[r & 3]);
+        if (nB == 0u) { done = true; break; }
+        if (*(volatile int *)&S->overflow) break;
+        if (trace && gtid == 0 && r < kTraceSteps) {
+            trace[4 * r] = global_ns() - t_start;
+            trace[4 * r + 1] = nB;
+        }
+        if (gtid == 0) S->sizes[(r + 2) & 3] = 0u;
+        uint32_t *nsize = &S->sizes[(r + 1) & 3];
+        const bool bitmap = use_bitmap && nB >= kBitmapBricks;
+        const uint32_t tag = r + 2;
+        const uint32_t wstride = gridDim.x * NW, wbase = blockIdx.x * NW;
+        uint32_t bnext = (wbase + warp < nB) ? __ldcg(F + wbase + warp) : 0u;
+        for (uint32_t base = wbase; base < nB; base += wstride) {
+            const uint32_t idx = base + warp;
+            const uint32_t b = bnext;
+            bnext = (idx + wstride < nB) ? __ldcg(F + idx + wstride) : 0u;
+            if (idx < nB) {
+                if (lane == 0) ++visits;
+                uint32_t zb, yb, xb;
+                brick_zyx(G, b, zb, yb, xb);
+                const int z0 = (int)(zb * BZ);
+                const int x0b = (int)(xb * kBX), y0b = (int)(yb * kBY);
+                const int x = x0b + xl, y = y0b + yl;
+                const bool xyin = x < (int)g.W && y < (int)g.H;
+                int hx_ = x0b, hy_ = y0b;
+                if (lane < 8) { hx_ = x0b + lane; hy_ = y0b - 1; }
+                else if (lane < 16) { hx_ = x0b + lane - 8; hy_ = y0b + kBY; }
+                else if (lane < 24) { hx_ = lane < 20 ? x0b - 1 : x0b + kBX; hy_ = y0b + (lane & 3); }
+                else { hx_ = (lane & 1) ? x0b + kBX : x0b - 1; hy_ = (lane & 2) ? y0b + kBY : y0b - 1; }
+                const bool hin = lane < 28 && hx_ >= 0 && hy_ >= 0 && hx_ < (int)g.W && hy_ < (int)g.H;
+                const uint32_t hoff = (uint32_t)clampi(hy_, 0, (int)g.H - 1) * g.W + (uint32_t)clampi(hx_, 0, (int)g.W - 1);
+                const uint32_t coff = (uint32_t)min(y, (int)g.H - 1) * g.W + (uint32_t)min(x, (int)g.W - 1);
+                // keys of planes z0 - 1 .. z0 + BZ; voxels outside the image are
+                // no neighbour (key infinity), as the reference skips them
+                uint32_t k[K], h[K];
+                bool cm[K], hm[K];   // mask voxels: the lane's column, its halo voxel
+#pragma unroll
+                for (int q = 0; q < K; ++q) {
+                    const int zq = z0 - ZR + q;
+                    const bool zin = zq >= 0 && zq < (int)g.D;
+                    const uint32_t zo = (uint32_t)clampi(zq, 0, (int)g.D - 1) * g.H * g.W;
+                    const uint32_t kp = ld_cg(lab + zo + coff);
+                    const uint32_t hp = lane < 28 ? ld_cg(lab + zo + hoff) : 0u;
+                    const uint32_t ks = __ldcg(seg + zo + coff);
+                    const uint32_t hs = lane < 28 ? (uint32_t)__ldcg(seg + zo + hoff) : 0u;
+                    cm[q] = zin && xyin && ks != 0u;
+                    hm[q] = zin && hin && hs != 0u;
+                    k[q] = (zin && xyin) ? key_of(kp, ks) : kKInf;
+                    h[q] = (zin && hin) ? key_of(hp, hs) : kKInf;
+                }
+                // candidates: mask voxels that are not seeds (seeds have s = 0)
+                bool cand[BZ];
+                bool anyc = false;
+#pragma unroll
+                for (int j = 0; j < BZ; ++j) {
+                    cand[j] = cm[j + ZR] && (k[j + ZR] >> 24) != 0u;
+                    anyc |= cand[j];
+                }
+                // lane d < 27: does neighbouring brick d hold a candidate next to
+                // this brick (in its halo)?  If not, nothing this brick writes can
+                // change that brick, and it is not queued for it
+                bool present = false;
+                {
+                    const int dzn = lane / 9 - 1, dyn = (lane / 3) % 3 - 1, dxn = lane % 3 - 1;
+                    const unsigned hsel = dyn == 0 ? (dxn < 0 ? 0x000F0000u : 0x00F00000u)
+                                        : dxn == 0 ? (dyn < 0 ? 0x000000FFu : 0x0000FF00u)
+                                        : (1u << (24 + (dyn > 0 ? 2 : 0) + (dxn > 0 ? 1 : 0)));
+                    unsigned pres = 0u;
+#pragma unroll
+                    for (int q = 0; q < K; ++q) {
+                        const unsigned cb = __ballot_sync(0xffffffffu, cm[q] && (k[q] >> 24) != 0u);
+                        const unsigned hb = __ballot_sync(0xffffffffu, hm[q] && (h[q] >> 24) != 0u);
+                        const bool inP = dzn < 0 ? q == 0 : (dzn > 0 ? q == K - 1 : (q >= ZR && q < ZR + BZ));
+                        if (inP) pres |= (dyn == 0 && dxn == 0) ? cb : (hb & hsel);
+                    }
+                    present = lane < 27 && pres != 0u;
+                }
+                if (!__any_sync(0xffffffffu, anyc)) {
+                    // nothing here can change: never queue it again
+                    if (lane == 0) {
+                        atomicExch(bstep + b, 0xFFFFFFFFu);
+                        atomicOr(Qb.done + (b >> 5), 1u << (b & 31u));
+                    }
+                    continue;
+                }
+                // halo terms, fixed during the visit: per plane the halo row's
+                // x-minimum (y edge) and the halo column's value (x edge) of the
+                // box term, and the face term's halo row / column voxels
+                uint32_t HX[BZ], SZ[BZ], HC[BZ], SC[BZ];
+                {
+                    uint32_t dh[K];
+#pragma unroll
+                    for (int q = 0; q < K; ++q) dh[q] = key_diag(h[q]);
+#pragma unroll
+                    for (int j = 0; j < BZ; ++j) {
+                        const int kc = j + ZR;
+                        uint32_t dhm = dh[kc];
+                        if (ZR) dhm = min(dhm, min(dh[kc - ZR], dh[kc + ZR]));
+                        const uint32_t hz = __shfl_sync(0xffffffffu, dhm, src_h);
+                        const uint32_t sz = __shfl_sync(0xffffffffu, dhm, src_s);
+                        const uint32_t qz = __shfl_sync(0xffffffffu, dhm, src_q);
+                        const uint32_t hl = __shfl_up_sync(0xffffffffu, hz, 1), hr = __shfl_down_sync(0xffffffffu, hz, 1);
+                        HX[j] = min(hz, min(x0 ? qz : hl, x1 ? qz : hr));
+                        SZ[j] = sz;
+                        HC[j] = __shfl_sync(0xffffffffu, h[kc], src_h);
+                        SC[j] = __shfl_sync(0xffffffffu, h[kc], src_s);
+                    }
+                }
+                uint32_t k0[BZ], dk[K];
+#pragma unroll
+                for (int j = 0; j < BZ; ++j) k0[j] = k[j + ZR];
+#pragma unroll
+                for (int q = 0; q < K; ++q) dk[q] = key_diag(k[q]);
+                // Gauss-Seidel over the planes (upward on even iterations,
+                // downward on odd ones); a plane is evaluated again only after
+                // it or a plane next to it changed
+                unsigned cmask = 0u;
+#pragma unroll
+                for (int j = 0; j < BZ; ++j)
+                    if (__any_sync(0xffffffffu, cand[j])) cmask |= 1u << j;
+                unsigned act = cmask, nxt = 0u;
+                auto relax = [&](auto J) {
+                    constexpr int j = decltype(J)::value;
+                    if constexpr (j < BZ) {
+                        constexpr int kc = j + ZR;
+                        if ((act >> j) & 1u) {
+                            // box term over the map-2 keys: planes, then x, then y
+                            uint32_t dz = dk[kc];
+                            if constexpr (ZR > 0) dz = min(dz, min(dk[kc - 1], dk[kc + 1]));
+                            const uint32_t cl = __shfl_up_sync(0xffffffffu, dz, 1), cr = __shfl_down_sync(0xffffffffu, dz, 1);
+                            const uint32_t rx = min(dz, min(x0 ? SZ[j] : cl, x1 ? SZ[j] : cr));
+                            const uint32_t ru = __shfl_up_sync(0xffffffffu, rx, kBX), rd = __shfl_down_sync(0xffffffffu, rx, kBX);
+                            const uint32_t bm = min(rx, min(y0 ? HX[j] : ru, y1 ? HX[j] : rd));
+                            // face term over the raw keys
+                            const uint32_t v = k[kc];
+                            const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1), fr = __shfl_down_sync(0xffffffffu, v, 1);
+                            const uint32_t fu = __shfl_up_sync(0xffffffffu, v, kBX), fd = __shfl_down_sync(0xffffffffu, v, kBX);
+                            uint32_t fm = min(min(x0 ? SC[j] : fl, x1 ? SC[j] : fr), min(y0 ? HC[j] : fu, y1 ? HC[j] : fd));
+                            if constexpr (ZR > 0) fm = min(fm, min(k[kc - 1], k[kc + 1]));
+                            const uint32_t nk = cand[j] ? min(key_face(fm), bm) : v;
+                            const bool c = nk != v;
+                            if (__any_sync(0xffffffffu, c)) {
+                                if (c) { k[kc] = nk; dk[kc] = key_diag(nk); }
+                                const unsigned nb3 = ((7u << j) >> 1) & cmask;   // planes j-1 .. j+1
+                                nxt |= nb3;
+                                act |= nb3;   // the plane the sweep reaches next sees it now
+                            }
+                        }
+                    }
+                };
+                using I0 = std::integral_constant<int, 0>;
+                using I1 = std::integral_constant<int, 1>;
+                using I2 = std::integral_constant<int, 2>;
+                using I3 = std::integral_constant<int, 3>;
+                static_assert(BZ <= 4, "the plane sweep is unrolled for up to 4 planes");
+                bool conv = false;
+                int it = 0;
+                for (; it < kKeyIters; ++it) {
+                    nxt = 0u;
+                    if (it & 1) { relax(I3{}); relax(I2{}); relax(I1{}); relax(I0{}); }
+                    else        { relax(I0{}); relax(I1{}); relax(I2{}); relax(I3{}); }
+                    act = nxt;
+                    if (!act) { conv = true; break; }
+                }
+                if (lane == 0) iters += (uint32_t)it + 1u;
+                // write the changed voxels, keep the per-s counts, queue the
+                // bricks next to changed voxels (and this one if still changing)
+                unsigned chb[BZ], chall = 0u;
+                bool over = false;
+#pragma unroll
+                for (int j = 0; j < BZ; ++j) {
+                    const uint32_t kn = k[j + ZR];
+                    const bool c = kn != k0[j];
+                    if (c) {
+                        const uint32_t m = ((uint32_t)(z0 + j) * g.H + (uint32_t)y) * g.W + (uint32_t)x;
+                        // steps above kKeyMaxS raise the overflow below; the
+                        // clamp keeps such a step from wrapping into a seed's 0
+                        __stcg(seg + m, (uint8_t)(0x80u | min(kn >> 24, 126u)));
+                        st_cg(lab + m, (kn & 0x00FFFFFFu) ^ 0x00FFFFFFu);
+                        if (k0[j] != kKInf) atomicSub(&s_hist[k0[j] >> 24], 1);
+                        atomicAdd(&s_hist[kn >> 24], 1);
+                        over |= (kn >> 24) > kKeyMaxS;
+                    }
+                    chb[j] = __ballot_sync(0xffffffffu, c);
+                    chall |= chb[j];
+                }
+                if (over) atomicExch(&S->overflow, 1);
+                if (chall && lane == 0) atomicOr(touched + (b >> 5), 1u << (b & 31u));
+                bool want = false;
+                if (lane < 27) {
+                    const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
+                    if (IS3D || dz == 0) {
+                        unsigned sel = dz < 0 ? chb[0] : (dz > 0 ? chb[BZ - 1] : chall);
+                        if (dyb < 0) sel &= 0x000000FFu;
+                        else if (dyb > 0) sel &= 0xFF000000u;
+                        if (dxb < 0) sel &= 0x01010101u;
+                        else if (dxb > 0) sel &= 0x80808080u;
+                        want = sel != 0u && present && !(dz == 0 && dyb == 0 && dxb == 0);
+                        if (!conv && dz == 0 && dyb == 0 && dxb == 0) want = true;
+                    }
+                }
+                if (bitmap) {
+                    uint32_t nb = 0;
+                    if (want && neighbour_brick(G, zb, yb, xb, lane, nb))
+                        atomicOr(Qb.q + (nb >> 5), 1u << (nb & 31u));
+                } else {
+                    queue_neighbours(G, zb, yb, xb, want, tag, bstep, ap);
+                }
+            }
+            if (!bitmap) ap.maybe_flush(Fn, nsize);
+        }
+        if (!bitmap) ap.flush(Fn, nsize);
+        if (trace) {
+            const uint32_t is = block_total(iters, s_red);
+            if (threadIdx.x == 0 && r < kTraceSteps && is) atomicAdd(trace + 4 * r + 2, (unsigned long long)is);
+        }
+        ok = grid_sync(&S->bar, &S->err, barrier_ns);
+        if (bitmap && ok) ok = compact_queue(Qb, Fn, nsize, S, barrier_ns, s_red, s_scan, s_off);
+        if (trace && gtid == 0 && r < kTraceSteps) trace[4 * r + 3] = global_ns() - t_start;
+        ++r;
+    }
+    // ---- finish: S from the counts, keys back to labels ----------------------
+    if (trace && gtid == 0) trace[4 * (kTraceSteps - 1)] = global_ns() - t_start;
+    const uint32_t vs = block_total(visits, s_red);
+    if (threadIdx.x == 0 && vs) atomicAdd(&S->visits, vs);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += KBT)
+        if (s_hist[i]) atomicAdd(&S->hist[i], s_hist[i]);
+    if (ok) ok = grid_sync(&S->bar, &S->err, barrier_ns);
+    const bool overflow = *(volatile int *)&S->overflow != 0;
+    if (ok && !done && !overflow) ok = false;   // round bound reached
+    if (!ok && !overflow) {
+        if (gtid == 0) {
+            const int e = *(volatile int *)&S->err;
+            *d_status = e ? e : (int)CLE_ERR_ITER_LIMIT;
+            S->rounds = r;
+        }
+        return;
+    }
+    // S = the smallest s >= 1 that no voxel holds, and whether any voxel holds
+    // a larger s (warp 0 of each CTA)
+    if (warp == 0) {
+        uint32_t stop = 128u;
+        for (int c = 0; c < 4 && stop == 128u; ++c) {
+            const int sidx = 32 * c + lane;
+            const unsigned empty = __ballot_sync(0xffffffffu, sidx >= 1 && __ldcg(&S->hist[sidx]) == 0);
+            if (empty) stop = (uint32_t)(32 * c + __ffs(empty) - 1);
+        }
+        bool beyond = false;
+        for (int c = 0; c < 4; ++c) {
+            const int sidx = 32 * c + lane;
+            beyond |= sidx > (int)stop && __ldcg(&S->hist[sidx]) != 0;
+        }
+        beyond = __any_sync(0xffffffffu, beyond);
+        if (lane == 0) {
+            s_off[0] = overflow ? 0u : stop;         // 0: keep no grown voxel
+            s_off[1] = (overflow || beyond) ? 1u : 0u;
+        }
+    }
+    __syncthreads();
+    const uint32_t stop = s_off[0];
+    const bool cut = s_off[1] != 0u;
+    if (cut) {
+        // labels of voxels that arrived after step S (or, after an overflow,
+        // of every grown voxel) go back to 0: the touched bricks in a list
+        // (the next-round bitmap q is clear and serves as the empty filter)
+        BQueue Tq = Qb;
+        Tq.q = touched;
+        Tq.done = Qb.q;
+        ok = compact_queue(Tq, B0, &S->sizes[0], S, barrier_ns, s_red, s_scan, s_off);
+        if (!ok) {
+            if (gtid == 0) *d_status = *(volatile int *)&S->err;
+            return;
+        }
+        const uint32_t nT = __ldcg(&S->sizes[0]);
+        for (uint32_t idx = blockIdx.x * NW + warp; idx < nT; idx += gridDim.x * NW) {
+            const uint32_t b = __ldcg(B0 + idx);
+            uint32_t zb, yb, xb;
+            brick_zyx(G, b, zb, yb, xb);
+            const uint32_t x = xb * kBX + (uint32_t)xl, y = yb * kBY + (uint32_t)yl;
+            if (x >= g.W || y >= g.H) continue;
+#pragma unroll
+            for (int j = 0; j < BZ; ++j) {
+                const uint32_t z = zb * BZ + (uint32_t)j;
+                if (z >= g.D) break;
+                const uint32_t m = (z * g.H + y) * g.W + x;
+                const uint32_t sv = (uint32_t)__ldcg(seg + m) & 0x7Fu;
+                if (sv > stop && ld_cg(lab + m) != 0u) st_cg(lab + m, 0u);
+            }
+        }
+    }
+    if (trace) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(trace + 4 * (kTraceSteps - 1) + 3, (unsigned long long)(global_ns() - t_start));
+    }
+    if (gtid == 0) {
+        S->rounds = r;
+        S->stop_s = stop;
+        if (overflow) S->gate = 1;                          // labels restored; the brick kernel grows them
+        else if (stop > max_steps) *d_status = (int)CLE_ERR_ITER_LIMIT;   // the reference needs S steps
+    }
+}
+
 int brick_planes(const Img &im) { return im.ndim == 3 ? kBZ3 : 1; }
 uint32_t bricks_x(const Img &im) { return (uint32_t)((im.W + kBX - 1) / kBX); }
 uint32_t bricks_y(const Img &im) { return (uint32_t)((im.H + kBY - 1) / kBY); }
@@ -525,7 +976,7 @@ size_t voronoi_frontier_workspace_bytes(const Img &im) {
 
 int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uint32_t *seeds,
                      const uint32_t *d_seed_count, int *d_status, Arena &ws, cudaStream_t st,
-                     const Limits &lim) {
+                     const Limits &lim, const int *gate) {
     const size_t nb = brick_count(im);
     BState *S = ws.take<BState>(1);
     uint32_t *B0 = ws.take<uint32_t>(nb);
@@ -574,14 +1025,95 @@ int voronoi_frontier(const Img &im, uint32_t *lab, const uint8_t *seg, const uin
     if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
     const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * kWPB - 1) / (4 * kWPB));
     const int grid = (int)std::min<int64_t>(std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev, lim)), 2048);
-    unsigned long long *trace =
-        (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
+    // behind the key kernel (gate set) the trace stays that kernel's
+    unsigned long long *trace = gate ? nullptr
+        : (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, &B0, &B1, &Mv, &Pf,
                     &bstep, &S, &d_status, &max_steps, &loop_ns, &barrier_ns, (void *)&cancel, &trace, &Qb,
-                    &use_bitmap};
+                    &use_bitmap, (void *)&gate};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kBT), args, kBBufBytes, st));
     count_launches(1);
     return CLE_OK;
+}
+
+namespace {
+
+size_t keys_part_bytes(const Img &im) {
+    const size_t nb = brick_count(im);
+    Arena a(nullptr, 0);
+    a.take<KState>(1);
+    a.take<uint32_t>(nb);               // list 0
+    a.take<uint32_t>(nb);               // list 1
+    a.take<uint32_t>(nb);               // per-brick round tags
+    a.take<uint32_t>((nb + 31) / 32);   // queue bitmap
+    a.take<uint32_t>((nb + 31) / 32);   // bricks without candidates
+    a.take<uint32_t>((nb + 31) / 32);   // bricks with grown voxels
+    a.take<uint32_t>(2048);             // per-CTA counts of the compaction
+    return a.off;
+}
+
+}  // namespace
+
+size_t voronoi_grow_workspace_bytes(const Img &im) {
+    return voronoi_frontier_workspace_bytes(im) + keys_part_bytes(im);
+}
+
+int voronoi_grow(const Img &im, uint32_t *lab, uint8_t *seg, const uint32_t *seeds,
+                 const uint32_t *d_seed_count, const uint32_t *d_max_label, int *d_status, Arena &ws,
+                 cudaStream_t st, const Limits &lim) {
+    // the key kernel's state sits behind the brick kernel's workspace, so the
+    // gate word survives that kernel's set-up
+    const size_t off0 = ws.off;
+    ws.off = off0 + voronoi_frontier_workspace_bytes(im);
+    const size_t nb = brick_count(im);
+    KState *S = ws.take<KState>(1);
+    uint32_t *B0 = ws.take<uint32_t>(nb);
+    uint32_t *B1 = ws.take<uint32_t>(nb);
+    uint32_t *bstep = ws.take<uint32_t>(nb);
+    BQueue Qb;
+    Qb.nwords = (uint32_t)((nb + 31) / 32);
+    Qb.q = ws.take<uint32_t>(Qb.nwords);
+    Qb.done = ws.take<uint32_t>(Qb.nwords);
+    uint32_t *touched = ws.take<uint32_t>(Qb.nwords);
+    Qb.ccount = ws.take<uint32_t>(2048);
+    if (!ws.ok()) { set_error("masked_voronoi_labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
+    CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(KState), st));
+    CLE_CUDA(cudaMemsetAsync(bstep, 0, sizeof(uint32_t) * nb, st));
+    // q, done and touched are adjacent: one clear
+    CLE_CUDA(cudaMemsetAsync(Qb.q, 0, (size_t)((char *)(touched + Qb.nwords) - (char *)Qb.q), st));
+    BGeo G;
+    G.g = make_geo(im);
+    G.WB = bricks_x(im);
+    G.HB = bricks_y(im);
+    G.DB = bricks_z(im);
+    G.fWB = FastDiv(G.WB);
+    G.fHB = FastDiv(G.HB);
+    G.is3d = im.ndim == 3 ? 1 : 0;
+    uint32_t max_steps = lim.steps_for(im.n());
+    uint64_t loop_ns = lim.loop_ns, barrier_ns = lim.barrier_ns;
+    const volatile int *cancel = lim.cancel;
+    const void *kern = G.is3d ? (const void *)voronoi_keys_kernel<true, kBZ3, kKeyBT>
+                              : (const void *)voronoi_keys_kernel<false, 1, kKeyBT>;
+    const size_t smem = sizeof(uint32_t) * kSlice * (kKeyBT / 32);
+    CLE_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0;
+    CLE_CUDA(cudaGetDevice(&dev));
+    int per_sm = 0;
+    CLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kKeyBT, smem));
+    if (per_sm < 1) { set_error("masked_voronoi_labeling: kernel does not fit on an SM"); return CLE_ERR_CUDA; }
+    const int64_t want = std::max<int64_t>(1, (int64_t)(nb + 4 * (kKeyBT / 32) - 1) / (4 * (kKeyBT / 32)));
+    const int grid = (int)std::min<int64_t>(std::min<int64_t>(want, (int64_t)per_sm * cooperative_ctas(dev, lim)), 2048);
+    unsigned long long *trace =
+        (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
+    int use_bitmap = im.n() > kWideVoxels ? 1 : 0;
+    void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, (void *)&d_max_label,
+                    &B0, &B1, &bstep, &touched, &S, &d_status, &max_steps, &loop_ns, &barrier_ns,
+                    (void *)&cancel, &trace, &Qb, &use_bitmap};
+    CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kKeyBT), args, smem, st));
+    count_launches(1);
+    // the brick kernel, which returns at once unless the gate was raised
+    ws.off = off0;
+    return voronoi_frontier(im, lab, seg, seeds, d_seed_count, d_status, ws, st, lim, &S->gate);
 }
 
 }  // namespace cle

@@ -433,6 +433,60 @@ def test_masked_voronoi_binary_diagonal_stop(cle, oracle):
     assert (ref > 0).sum() < mask.sum()      # growth stopped early, as in the reference
 
 
+def _snake(length, width=40):
+    """A one-voxel-wide serpentine path of `length` voxels in plane z = 1 of a
+    3-plane volume (rows y = 1, 3, 5, ... joined at alternating ends), seeded at
+    its start: the growth needs about `length` steps."""
+    rows = (length + width - 1) // width + 1
+    mask = np.zeros((3, 2 * rows + 2, width), np.uint8)
+    n, y, left = 0, 1, True
+    while n < length:
+        xs = range(width) if left else range(width - 1, -1, -1)
+        for x in xs:
+            if n == length:
+                break
+            mask[1, y, x] = 1
+            n += 1
+        if n < length:
+            mask[1, y + 1, width - 1 if left else 0] = 1
+            n += 1
+        y += 2
+        left = not left
+    seeds = np.zeros_like(mask)
+    seeds[1, 1, 0] = 1
+    return seeds, mask
+
+
+def _path_order(plane):
+    # the path's voxels from its start (y 1, x 0), by walking face neighbours
+    y, x = 1, 0
+    seen, out = {(y, x)}, [(y, x)]
+    while True:
+        nxt = [(y + dy, x + dx) for dy, dx in ((0, 1), (0, -1), (1, 0), (-1, 0))
+               if 0 <= y + dy < plane.shape[0] and 0 <= x + dx < plane.shape[1]
+               and plane[y + dy, x + dx] and (y + dy, x + dx) not in seen]
+        if not nxt:
+            return out
+        y, x = nxt[0]
+        seen.add((y, x))
+        out.append((y, x))
+
+
+@pytest.mark.parametrize("length", [60, 247, 249, 252, 254, 257, 600])
+def test_masked_voronoi_binary_long_path(cle, oracle, length):
+    # paths around the arrival-step limit of the key growth (120 steps, above
+    # which the step-by-step brick growth takes over), with a second seed a
+    # few voxels before the path's end so two labels meet on the path
+    seeds, mask = _snake(length)
+    path = _path_order(mask[1])
+    y, x = path[-6]
+    seeds[1, y, x] = 1
+    ref, steps = oracle.masked_voronoi_labeling(seeds, mask, return_steps=True)
+    got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
+    assert np.array_equal(got, ref)
+    assert (ref > 0).sum() == mask.sum()
+
+
 def test_masked_voronoi_binary_many_seeds_3d(cle, oracle):
     seeds, mask = _binary_case((24, 100, 70), 32, 0.6, 0.02)
     got = cle.pull(cle.masked_voronoi_labeling_binary(seeds, mask))
