@@ -208,6 +208,46 @@ int cle_replace_intensities(const cle_tensor *src, const cle_tensor *map, const 
 int cle_euclidean_distance_from_label_centroid_map(const cle_tensor *labels, const cle_tensor *centroids,
                                                    const cle_tensor *dst, void *stream);
 
+/* ---- distance / touch matrices and neighbour distances ------------------
+ * Point lists are float32 [d, n] (one row per dimension x, y(, z), as
+ * centroids_of_labels makes them).  Matrices are float32 [rows, columns] with
+ * row y = item y - 1 of the second list (or label y), column x = item x - 1 of
+ * the first (or label x), row and column 0 the background (zeros).
+ * cle_generate_distance_matrix replaces _tier1/_generate_distance_matrix.py
+ * (dst [m+1, n+1]: float32 Euclidean distances, squared differences summed x,
+ * y, z in order).  cle_generate_touch_matrix replaces
+ * _tier1/_generate_touch_matrix.py with generate_touch_matrix_{2,3}d_x.cl (dst
+ * [L+1, L+1], cleared, then 1 at (a, b) and (b, a) for labels a != b meeting
+ * across a face).  cle_average_distance_of_n_distances replaces
+ * _tier1/_average_distance_of_n_nearest_distances.py (exclude_self 0, with
+ * average_distance_of_n_nearest_distances_x.cl) and
+ * _tier1/_average_distance_of_n_shortest_distances.py (exclude_self 1: row ==
+ * column left out): per column the mean of the n smallest of rows 1.. (0 <= n
+ * <= 1000; NaN when no row counts).  cle_average_distance_of_touching_neighbors
+ * replaces _tier1/_average_distance_of_touching_neighbors.py: per column the
+ * mean distance over rows >= 1 whose touch entry is set (0 if none).
+ * cle_average_distance_of_n_nearest_points gives the n-distances vector of the
+ * distance matrix of two point lists without building it, and
+ * cle_average_distance_of_touching_labels the touching-neighbour vector of a
+ * label image and its centroids (workspace: a bitmap of touching label pairs,
+ * (L+1) x ceil((L+1)/32) words); these serve
+ * _tier9/_average_distance_of_n_nearest_neighbors_map.py,
+ * _tier9/_average_distance_to_n_nearest_other_labels_map.py and
+ * _tier9/_average_neighbor_distance_map.py with replace_intensities. */
+int cle_generate_distance_matrix(const cle_tensor *list1, const cle_tensor *list2, const cle_tensor *dst,
+                                 void *stream);
+int cle_generate_touch_matrix(const cle_tensor *labels, const cle_tensor *dst, void *stream);
+int cle_average_distance_of_n_distances(const cle_tensor *distance_matrix, int n, int exclude_self,
+                                        const cle_tensor *dst, void *stream);
+int cle_average_distance_of_touching_neighbors(const cle_tensor *distance_matrix, const cle_tensor *touch_matrix,
+                                               const cle_tensor *dst, void *stream);
+int cle_average_distance_of_n_nearest_points(const cle_tensor *list1, const cle_tensor *list2, int n,
+                                             int exclude_self, const cle_tensor *dst, void *stream);
+size_t cle_average_distance_of_touching_labels_workspace_bytes(int64_t num_labels);
+int cle_average_distance_of_touching_labels(const cle_tensor *labels, const cle_tensor *centroids,
+                                            const cle_tensor *dst, void *workspace, size_t workspace_bytes,
+                                            void *stream);
+
 /* ---- minimum_box / maximum_box / top_hat_box ----------------------------
  * minimum_box replaces _tier1/_minimum_box.py:6-55, maximum_box
  * _tier1/_maximum_box.py, top_hat_box _tier2/_top_hat_box.py:6-43 (source minus

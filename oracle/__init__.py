@@ -377,3 +377,155 @@ def euclidean_distance_from_label_centroid_map(labels) -> np.ndarray:
         d2 += (grid - c[col].astype(np.float64)) ** 2
     out = np.where(lab != 0, np.sqrt(d2), 0.0)
     return out.astype(np.float32)
+
+
+# ---- neighbour-distance maps ------------------------------------------------
+# _tier1/_generate_distance_matrix.py, _tier1/_generate_touch_matrix.py with
+# generate_touch_matrix_{2,3}d_x.cl, _tier1/_average_distance_of_n_nearest_distances.py
+# with average_distance_of_n_nearest_distances_x.cl,
+# _tier1/_average_distance_of_n_shortest_distances.py,
+# _tier1/_average_distance_of_touching_neighbors.py and the three maps of _tier9
+# built from them.  float32 throughout, as the reference's kernels compute.
+
+def centroids_of_labels(labels) -> np.ndarray:
+    """[d, L] float32 point list of labels 1..L (L = the largest label): per
+    dimension float32(coordinate sum) / float32(voxel count), NaN for a label
+    without voxels (_tier9/_centroids_of_labels.py)."""
+    lab = np.asarray(labels)
+    if lab.dtype.kind == "f":
+        lab = np.nan_to_num(lab, nan=0.0)
+    lab = np.clip(lab.astype(np.int64), 0, None)
+    L = int(lab.max()) if lab.size else 0
+    coords = np.indices(lab.shape)[::-1]          # x, y(, z)
+    flat = lab.ravel()
+    cnt = np.bincount(flat, minlength=L + 1)[1:L + 1]
+    out = np.empty((lab.ndim, L), np.float32)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for k, g in enumerate(coords):
+            s = np.bincount(flat, weights=g.ravel().astype(np.float64), minlength=L + 1)[1:L + 1]
+            out[k] = np.float32(s) / np.float32(cnt)
+    return out
+
+
+def generate_distance_matrix(p1, p2) -> np.ndarray:
+    """[m+1, n+1] float32: [j+1, i+1] = sqrt of the float32 sum, in the order
+    x, y(, z), of the squared float32 differences of point i of p1 and point j
+    of p2; row and column 0 zero."""
+    p1 = np.asarray(p1, np.float32)
+    p2 = np.asarray(p2, np.float32)
+    n, m = p1.shape[1], p2.shape[1]
+    out = np.zeros((m + 1, n + 1), np.float32)
+    s = np.zeros((m, n), np.float32)
+    with np.errstate(invalid="ignore"):
+        for k in range(p1.shape[0]):
+            t = (p1[k][None, :] - p2[k][:, None]).astype(np.float32)
+            s = (s + (t * t).astype(np.float32)).astype(np.float32)
+        out[1:, 1:] = np.sqrt(s)
+    return out
+
+
+def generate_touch_matrix(labels) -> np.ndarray:
+    """[L+1, L+1] float32: 1 at (a, b) and (b, a) where a voxel of label a has
+    its +x, +y (or +z) neighbour in label b != a."""
+    lab = np.asarray(labels)
+    lab = lab.astype(np.float32).astype(np.int64) if lab.dtype.kind == "f" else lab.astype(np.int64)
+    L = int(lab.max()) if lab.size else 0
+    T = np.zeros((L + 1, L + 1), np.float32)
+    for ax in range(lab.ndim):
+        a = np.moveaxis(lab, ax, 0)
+        x, y = a[:-1].ravel(), a[1:].ravel()
+        d = (x != y) & (x >= 0) & (y >= 0)
+        T[y[d], x[d]] = 1.0
+        T[x[d], y[d]] = 1.0
+    return T
+
+
+def _held_mean(values, n):
+    """average_distance_of_n_nearest_distances_x.cl's selection: values are
+    appended while fewer than n are held, then one insertion pass from the end
+    moves a smaller value down; the mean is the float32 sum in buffer order over
+    the count (NaN when none)."""
+    buf = []
+    for v in values:
+        v = np.float32(v)
+        if len(buf) < n:
+            buf.append(v)
+        for i in range(len(buf) - 1, -1, -1):
+            if v > buf[i]:
+                break
+            if v < buf[i] and (i == 0 or v >= buf[i - 1]):
+                for j in range(len(buf) - 1, i, -1):
+                    buf[j] = buf[j - 1]
+                buf[i] = v
+                break
+    s = np.float32(0.0)
+    for b in buf:
+        s = np.float32(s + b)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.float32(s / np.float32(len(buf)))
+
+
+def _n_distance_vector(D, n, exclude_self):
+    D = np.asarray(D, np.float32)
+    H, W = D.shape
+    out = np.zeros((1, W), np.float32)
+    for x in range(W):
+        rows = [y for y in range(1, H) if not (exclude_self and y == x)]
+        col = D[rows, x]
+        if not np.isnan(col).any():
+            # no NaN: the selection keeps the n smallest in ascending order
+            col = np.sort(col)[:n]
+        out[0, x] = _held_mean(col, n)
+    return out
+
+
+def average_distance_of_n_nearest_distances(D, n=1) -> np.ndarray:
+    """[1, columns]: per column the mean of the n smallest of rows 1.."""
+    return _n_distance_vector(D, int(n), False)
+
+
+def average_distance_of_n_shortest_distances(D, n=1) -> np.ndarray:
+    """[1, rows]: as above with the column's own row left out (the distance of a
+    label to itself)."""
+    return _n_distance_vector(D, int(n), True)
+
+
+def average_distance_of_touching_neighbors(D, T) -> np.ndarray:
+    """[1, rows]: per column the float32 mean (sum in row order) of the
+    distances in rows >= 1 whose touch entry is set; 0 when none."""
+    D = np.asarray(D, np.float32)
+    T = np.asarray(T, np.float32)
+    H, W = D.shape
+    out = np.zeros((1, W), np.float32)
+    for x in range(W):
+        s, c = np.float32(0.0), 0
+        for y in range(1, H):
+            if T[y, x] > 0:
+                s = np.float32(s + D[y, x])
+                c += 1
+        out[0, x] = np.float32(s / np.float32(c)) if c else np.float32(0.0)
+    return out
+
+
+def replace_intensities(labels, vec) -> np.ndarray:
+    lab = np.asarray(labels)
+    idx = lab.astype(np.float32).astype(np.int64) if lab.dtype.kind == "f" else lab.astype(np.int64)
+    v = np.asarray(vec, np.float32).ravel()
+    return v[np.clip(idx, 0, len(v) - 1)]
+
+
+def average_distance_of_n_nearest_neighbors_map(labels, n=1) -> np.ndarray:
+    c = centroids_of_labels(labels)
+    D = generate_distance_matrix(c, c)
+    return replace_intensities(labels, average_distance_of_n_shortest_distances(D, n))
+
+
+def average_distance_to_n_nearest_other_labels_map(labels, other_labels, n=1) -> np.ndarray:
+    D = generate_distance_matrix(centroids_of_labels(labels), centroids_of_labels(other_labels))
+    return replace_intensities(labels, average_distance_of_n_nearest_distances(D, n))
+
+
+def average_neighbor_distance_map(labels) -> np.ndarray:
+    c = centroids_of_labels(labels)
+    D = generate_distance_matrix(c, c)
+    return replace_intensities(labels, average_distance_of_touching_neighbors(D, generate_touch_matrix(labels)))

@@ -13,6 +13,10 @@ the library or a CUDA device the ops raise; there is no CPU fallback.
 from ._tier0 import (B200Array, B200Backend, Backend, Image, asarray, create, create_binary_like,
                      create_labels_like, create_like, create_none, create_zyx, is_image, nparray,
                      plugin_function, pull, pull_zyx, push, push_native, push_zyx)
+from ._ops import (average_distance_of_n_nearest_distances, average_distance_of_n_nearest_neighbors_map,
+                   average_distance_of_n_shortest_distances, average_distance_of_touching_neighbors,
+                   average_distance_to_n_nearest_other_labels_map, average_neighbor_distance_map,
+                   generate_distance_matrix, generate_touch_matrix)
 from ._ops import (STATISTICS_ENTRY, add_image_and_scalar, centroids_of_background_and_labels,
                    centroids_of_labels, euclidean_distance_from_label_centroid_map,
                    label_maximum_extension_map,

@@ -110,6 +110,13 @@ _SIGS = {
     "cle_add_image_and_scalar": (ctypes.c_int, [_T, _T, ctypes.c_float, _P]),
     "cle_replace_intensities": (ctypes.c_int, [_T, _T, _T, _P]),
     "cle_euclidean_distance_from_label_centroid_map": (ctypes.c_int, [_T, _T, _T, _P]),
+    "cle_generate_distance_matrix": (ctypes.c_int, [_T, _T, _T, _P]),
+    "cle_generate_touch_matrix": (ctypes.c_int, [_T, _T, _P]),
+    "cle_average_distance_of_n_distances": (ctypes.c_int, [_T, ctypes.c_int, ctypes.c_int, _T, _P]),
+    "cle_average_distance_of_touching_neighbors": (ctypes.c_int, [_T, _T, _T, _P]),
+    "cle_average_distance_of_n_nearest_points": (ctypes.c_int, [_T, _T, ctypes.c_int, ctypes.c_int, _T, _P]),
+    "cle_average_distance_of_touching_labels_workspace_bytes": (_SZ, [ctypes.c_int64]),
+    "cle_average_distance_of_touching_labels": (ctypes.c_int, [_T, _T, _T, _P, _SZ, _P]),
     "cle_box_filter_workspace_bytes": (_SZ, [_T]),
     "cle_minimum_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),
     "cle_maximum_box": (ctypes.c_int, [_T, _T, ctypes.c_double, ctypes.c_double, ctypes.c_double, _P, _SZ, _P]),

@@ -555,6 +555,125 @@ def euclidean_distance_from_label_centroid_map(labels: Image, centroids_pointlis
     return distance_map_destination
 
 
+# ---- distance / touch matrices and the neighbour-distance maps -------------
+def _create_matrix_from_pointlists(pointlist1, pointlist2):
+    """_tier0/_create.py create_matrix_from_pointlists: [m + 1, n + 1] float32."""
+    return create([pointlist2.shape[1] + 1, pointlist1.shape[1] + 1])
+
+
+def _create_square_matrix_from_labelmap(labelmap):
+    """_tier0/_create.py create_square_matrix_from_labelmap: [L + 1, L + 1]."""
+    n = _label_max(push(labelmap)) + 1
+    return create([n, n])
+
+
+def _create_vector_from_square_matrix(square_matrix, *args):
+    """_tier0/_create.py create_vector_from_square_matrix: [1, rows]."""
+    return create([1, square_matrix.shape[0]])
+
+
+@plugin_function(output_creator=_create_matrix_from_pointlists)
+def generate_distance_matrix(coordinate_list1: Image, coordinate_list2: Image,
+                             distance_matrix_destination: Image = None) -> Image:
+    """Distances between all points of two [d, n] point lists as an
+    [m + 1, n + 1] float32 matrix, row and column 0 zero
+    (_tier1/_generate_distance_matrix.py)."""
+    _call("cle_generate_distance_matrix", _lib.ref(_T(coordinate_list1)), _lib.ref(_T(coordinate_list2)),
+          _lib.ref(_T(distance_matrix_destination)), _lib.stream_ptr())
+    return distance_matrix_destination
+
+
+@plugin_function(output_creator=_create_square_matrix_from_labelmap)
+def generate_touch_matrix(label_map: Image, touch_matrix_destination: Image = None) -> Image:
+    """[L + 1, L + 1] matrix with 1 where two labels (the background 0
+    included) meet across a face, both (a, b) and (b, a)
+    (_tier1/_generate_touch_matrix.py, generate_touch_matrix_{2,3}d_x.cl)."""
+    _call("cle_generate_touch_matrix", _lib.ref(_T(label_map)), _lib.ref(_T(touch_matrix_destination)),
+          _lib.stream_ptr())
+    return touch_matrix_destination
+
+
+@plugin_function(output_creator=_create_vector_from_square_matrix)
+def average_distance_of_n_shortest_distances(distance_matrix: Image, distance_vector_destination: Image = None,
+                                             n: int = 1) -> Image:
+    """Per column the mean of the n smallest distances in rows 1.., the
+    column's own row left out (_tier1/_average_distance_of_n_shortest_distances.py)."""
+    _call("cle_average_distance_of_n_distances", _lib.ref(_T(distance_matrix)), int(n), 1,
+          _lib.ref(_T(distance_vector_destination)), _lib.stream_ptr())
+    return distance_vector_destination
+
+
+@plugin_function(output_creator=create_none)
+def average_distance_of_n_nearest_distances(distance_matrix: Image, distance_vector_destination: Image = None,
+                                            n: int = 1) -> Image:
+    """Per column the mean of the n smallest distances in rows 1.., the
+    column's own row included (_tier1/_average_distance_of_n_nearest_distances.py,
+    average_distance_of_n_nearest_distances_x.cl); a [1, columns] vector."""
+    if distance_vector_destination is None:
+        distance_vector_destination = create([1, distance_matrix.shape[1]])
+    _call("cle_average_distance_of_n_distances", _lib.ref(_T(distance_matrix)), int(n), 0,
+          _lib.ref(_T(distance_vector_destination)), _lib.stream_ptr())
+    return distance_vector_destination
+
+
+@plugin_function(output_creator=_create_vector_from_square_matrix)
+def average_distance_of_touching_neighbors(distance_matrix: Image, touch_matrix: Image,
+                                           average_distancelist_destination: Image = None) -> Image:
+    """Per label the mean distance to the labels it touches, the background
+    left out, 0 for a label touching none
+    (_tier1/_average_distance_of_touching_neighbors.py)."""
+    _call("cle_average_distance_of_touching_neighbors", _lib.ref(_T(distance_matrix)), _lib.ref(_T(touch_matrix)),
+          _lib.ref(_T(average_distancelist_destination)), _lib.stream_ptr())
+    return average_distancelist_destination
+
+
+def _n_nearest_vector(pts_a, pts_b, n, exclude_self):
+    vec = create([1, pts_a.shape[1] + 1])
+    _call("cle_average_distance_of_n_nearest_points", _lib.ref(_T(pts_a)), _lib.ref(_T(pts_b)), int(n),
+          1 if exclude_self else 0, _lib.ref(_T(vec)), _lib.stream_ptr())
+    return vec
+
+
+@plugin_function(categories=['label measurement', 'map', 'in assistant'])
+def average_distance_of_n_nearest_neighbors_map(labels: Image, distance_map: Image = None, n: int = 1) -> Image:
+    """Every label replaced by the mean centroid distance to its n nearest other
+    labels (_tier9/_average_distance_of_n_nearest_neighbors_map.py): the vector
+    of average_distance_of_n_shortest_distances on the centroids' distance
+    matrix, computed from the centroids without building the matrix, then
+    replace_intensities."""
+    centroids = centroids_of_labels(labels)
+    vec = _n_nearest_vector(centroids, centroids, n, True)
+    return replace_intensities(labels, vec, distance_map)
+
+
+@plugin_function(categories=['label measurement', 'map', 'in assistant'])
+def average_distance_to_n_nearest_other_labels_map(labels: Image, other_labels: Image, distance_map: Image = None,
+                                                   n: int = 1) -> Image:
+    """Every label replaced by the mean distance from its centroid to the n
+    nearest centroids of other_labels
+    (_tier9/_average_distance_to_n_nearest_other_labels_map.py; the vector of
+    average_distance_of_n_nearest_distances, without the matrix)."""
+    centroids_a = centroids_of_labels(labels)
+    centroids_b = centroids_of_labels(other_labels)
+    vec = _n_nearest_vector(centroids_a, centroids_b, n, False)
+    return replace_intensities(labels, vec, distance_map)
+
+
+@plugin_function(categories=['label measurement', 'in assistant'])
+def average_neighbor_distance_map(labels: Image, distance_map: Image = None) -> Image:
+    """Every label replaced by the mean centroid distance to the labels it
+    touches (_tier9/_average_neighbor_distance_map.py): the vector of
+    average_distance_of_touching_neighbors, from a bitmap of touching label
+    pairs and the centroids instead of the two [L + 1, L + 1] matrices."""
+    centroids = centroids_of_labels(labels)
+    L = centroids.shape[1]
+    vec = create([1, L + 1])
+    ws = _ws("cle_average_distance_of_touching_labels_workspace_bytes", int(L), device=labels.tensor.device)
+    _call("cle_average_distance_of_touching_labels", _lib.ref(_T(labels)), _lib.ref(_T(centroids)),
+          _lib.ref(_T(vec)), _ptr(ws), ws.numel(), _lib.stream_ptr())
+    return replace_intensities(labels, vec, distance_map)
+
+
 def _box_call(name, source, destination, rx, ry, rz):
     s, d = _T(source), _T(destination)
     ws = _ws("cle_box_filter_workspace_bytes", _lib.ref(s))

@@ -213,6 +213,69 @@ int cle_euclidean_distance_from_label_centroid_map(const cle_tensor *labels, con
     return centroid_distance_map(a, p, d, S(stream));
 }
 
+int cle_generate_distance_matrix(const cle_tensor *list1, const cle_tensor *list2, const cle_tensor *dst,
+                                 void *stream) {
+    Img a, b, d;
+    CLE_TRY(to_img(list1, a, "coordinate_list1"));
+    CLE_TRY(to_img(list2, b, "coordinate_list2"));
+    CLE_TRY(to_img(dst, d, "distance_matrix_destination"));
+    CLE_TRY(set_device_of(a, list1));
+    return generate_distance_matrix(a, b, d, S(stream));
+}
+
+int cle_generate_touch_matrix(const cle_tensor *labels, const cle_tensor *dst, void *stream) {
+    Img a, d;
+    CLE_TRY(to_img(labels, a, "label_map"));
+    CLE_TRY(to_img(dst, d, "touch_matrix_destination"));
+    CLE_TRY(set_device_of(a, labels));
+    return generate_touch_matrix(a, d, S(stream));
+}
+
+int cle_average_distance_of_n_distances(const cle_tensor *distance_matrix, int n, int exclude_self,
+                                        const cle_tensor *dst, void *stream) {
+    Img m, d;
+    CLE_TRY(to_img(distance_matrix, m, "distance_matrix"));
+    CLE_TRY(to_img(dst, d, "distance_vector_destination"));
+    CLE_TRY(set_device_of(m, distance_matrix));
+    return average_distance_of_n_distances(m, n, exclude_self, d, S(stream));
+}
+
+int cle_average_distance_of_touching_neighbors(const cle_tensor *distance_matrix, const cle_tensor *touch_matrix,
+                                               const cle_tensor *dst, void *stream) {
+    Img m, t, d;
+    CLE_TRY(to_img(distance_matrix, m, "distance_matrix"));
+    CLE_TRY(to_img(touch_matrix, t, "touch_matrix"));
+    CLE_TRY(to_img(dst, d, "average_distancelist_destination"));
+    CLE_TRY(set_device_of(m, distance_matrix));
+    return average_distance_of_touching_neighbors(m, t, d, S(stream));
+}
+
+int cle_average_distance_of_n_nearest_points(const cle_tensor *list1, const cle_tensor *list2, int n,
+                                             int exclude_self, const cle_tensor *dst, void *stream) {
+    Img a, b, d;
+    CLE_TRY(to_img(list1, a, "pointlist1"));
+    CLE_TRY(to_img(list2, b, "pointlist2"));
+    CLE_TRY(to_img(dst, d, "distance_vector_destination"));
+    CLE_TRY(set_device_of(a, list1));
+    return average_distance_of_n_points(a, b, n, exclude_self, d, S(stream));
+}
+
+size_t cle_average_distance_of_touching_labels_workspace_bytes(int64_t num_labels) {
+    return touching_labels_workspace_bytes(num_labels);
+}
+
+int cle_average_distance_of_touching_labels(const cle_tensor *labels, const cle_tensor *centroids,
+                                            const cle_tensor *dst, void *ws, size_t ws_bytes, void *stream) {
+    Img a, p, d;
+    CLE_TRY(to_img(labels, a, "labels"));
+    CLE_TRY(to_img(centroids, p, "centroids"));
+    CLE_TRY(to_img(dst, d, "distance_vector_destination"));
+    CLE_TRY(ws_check(ws, ws_bytes, touching_labels_workspace_bytes(p.W), "average_neighbor_distance_map"));
+    CLE_TRY(set_device_of(a, labels));
+    Arena ar(ws, ws_bytes);
+    return average_distance_of_touching_labels(a, p, d, ar, S(stream));
+}
+
 size_t cle_box_filter_workspace_bytes(const cle_tensor *src) {
     Img im;
     if (to_img(src, im, "source")) return 0;

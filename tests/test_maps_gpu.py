@@ -194,3 +194,113 @@ def test_centroids_of_labels_device_runs(cle, oracle, shape):
     assert got.shape == ref.shape
     assert _close(got, ref, RTOL)
     assert np.all(np.isnan(got[:, 2]))   # label 3 is absent
+
+
+# ---- neighbour-distance maps and their matrices ---------------------------
+QUAD = np.asarray([[1, 1, 1, 3, 3, 3], [1, 1, 1, 3, 3, 3], [1, 1, 1, 3, 3, 3],
+                   [0, 0, 0, 2, 2, 2], [0, 0, 0, 2, 2, 2], [0, 0, 0, 2, 2, 2]])
+SPA = np.asarray([[1, 0, 0, 0, 0, 3], [0] * 6, [0] * 6, [0] * 6, [0] * 6, [0, 0, 0, 0, 0, 2]])
+SPB = np.asarray([[0, 2, 0, 0, 0, 3], [1, 0, 0, 0, 0, 0], [0] * 6, [0] * 6, [0, 0, 0, 0, 0, 4],
+                  [0, 0, 0, 0, 5, 0]])
+
+
+def test_neighbor_maps_reference_tests(cle):
+    # tests/test_average_distance_of_n_nearest_neighbors.py,
+    # tests/test_average_neighbor_distance_map.py,
+    # tests/test_average_distance_to_n_nearest_other_labels_map.py (rtol 0.01)
+    got = cle.pull(cle.average_distance_of_n_nearest_neighbors_map(cle.push(QUAD), n=2))
+    assert np.allclose(got, [[3.62] * 3 + [3] * 3] * 3 + [[0] * 3 + [3.62] * 3] * 3, 0.01)
+    got = cle.pull(cle.average_neighbor_distance_map(cle.push(QUAD)))
+    assert np.allclose(got, [[3] * 6] * 3 + [[0] * 3 + [3] * 3] * 3, 0.01)
+    got = cle.pull(cle.average_distance_to_n_nearest_other_labels_map(cle.push(SPA), cle.push(SPB), n=1))
+    ref = np.zeros((6, 6))
+    ref[0, 0] = ref[5, 5] = 1
+    assert np.allclose(got, ref, 0.01)
+
+
+def test_neighbor_matrices_reference_tests(cle):
+    # tests/test_generate_touch_matrix.py, test_average_distance_of_n_shortest_distances.py,
+    # test_average_distance_of_touching_neighbors.py, test_average_distance_of_n_nearest_distances.py
+    lab = np.asarray([[1, 1, 0, 0, 0], [1, 1, 0, 3, 0], [0, 2, 2, 3, 0], [0, 2, 2, 0, 0], [0, 0, 0, 0, 4]])
+    ref = np.asarray([[0, 1, 1, 1, 1], [1, 0, 1, 0, 0], [1, 1, 0, 1, 0], [1, 0, 1, 0, 0], [1, 0, 0, 0, 0]]).T
+    assert np.array_equal(cle.pull(cle.generate_touch_matrix(cle.push(lab))), ref)
+    c = cle.centroids_of_labels(cle.push(QUAD))
+    D = cle.generate_distance_matrix(c, c)
+    assert np.allclose(cle.pull(cle.average_distance_of_n_shortest_distances(D, n=1)), [[0, 3, 3, 3]], 0.01)
+    T = cle.generate_touch_matrix(cle.push(QUAD))
+    assert np.allclose(cle.pull(cle.average_distance_of_touching_neighbors(D, T)), [[0, 3, 3, 3]], 0.01)
+    D2 = cle.generate_distance_matrix(cle.centroids_of_labels(cle.push(SPA)), cle.centroids_of_labels(cle.push(SPB)))
+    assert np.allclose(cle.pull(cle.average_distance_of_n_nearest_distances(D2, n=1)), [[0, 1, 1, 0]], 0.01)
+
+
+def _voronoi_labels(shape, n, seed, gaps=False):
+    # touching labels: every voxel to its nearest of n random points (1..n),
+    # optionally with some labels dropped (absent labels: NaN centroids)
+    r = np.random.default_rng(seed)
+    pts = np.stack([r.integers(0, s, n) for s in shape], 1)
+    grid = np.stack(np.indices(shape), -1).reshape(-1, len(shape))
+    d2 = ((grid[:, None, :] - pts[None, :, :]) ** 2).sum(-1)
+    lab = (np.argmin(d2, 1) + 1).reshape(shape).astype(np.uint32)
+    lab[r.uniform(size=shape) < 0.15] = 0
+    if gaps:
+        for k in r.choice(np.arange(1, n + 1), n // 5, replace=False):
+            lab[lab == k] = 0
+    return lab
+
+
+@pytest.mark.parametrize("shape,n,gaps", [((60, 70), 40, False), ((60, 70), 40, True),
+                                          ((12, 30, 34), 60, False), ((12, 30, 34), 60, True)])
+def test_neighbor_matrices_match_oracle(cle, oracle, shape, n, gaps):
+    lab = _voronoi_labels(shape, n, 21, gaps).astype(np.float32)
+    c = oracle.centroids_of_labels(lab)
+    got_c = cle.pull(cle.centroids_of_labels(cle.push(lab)))
+    assert _close(got_c, c, 1e-6)
+    D = oracle.generate_distance_matrix(c, c)
+    Dg = cle.generate_distance_matrix(cle.push(c), cle.push(c))
+    assert np.array_equal(np.isnan(cle.pull(Dg)), np.isnan(D))
+    assert np.array_equal(cle.pull(Dg)[~np.isnan(D)], D[~np.isnan(D)])       # bit for bit
+    T = oracle.generate_touch_matrix(lab)
+    Tg = cle.generate_touch_matrix(cle.push(lab))
+    assert np.array_equal(cle.pull(Tg), T)
+    for k in (1, 3, 7):
+        assert _close(cle.pull(cle.average_distance_of_n_shortest_distances(Dg, n=k)),
+                      oracle.average_distance_of_n_shortest_distances(D, k), 1e-6)
+        assert _close(cle.pull(cle.average_distance_of_n_nearest_distances(Dg, n=k)),
+                      oracle.average_distance_of_n_nearest_distances(D, k), 1e-6)
+    assert _close(cle.pull(cle.average_distance_of_touching_neighbors(Dg, Tg)),
+                  oracle.average_distance_of_touching_neighbors(D, T), 1e-6)
+
+
+@pytest.mark.parametrize("shape,n,gaps", [((60, 70), 40, False), ((60, 70), 40, True),
+                                          ((12, 30, 34), 60, False), ((12, 30, 34), 60, True)])
+@pytest.mark.parametrize("k", [1, 4])
+def test_neighbor_maps_match_oracle(cle, oracle, shape, n, gaps, k):
+    lab = _voronoi_labels(shape, n, 22, gaps)
+    other = _voronoi_labels(shape, n // 2, 23, False)
+    src = cle.push(lab.astype(np.float32))
+    assert _close(cle.pull(cle.average_distance_of_n_nearest_neighbors_map(src, n=k)),
+                  oracle.average_distance_of_n_nearest_neighbors_map(lab, k), 1e-6)
+    assert _close(cle.pull(cle.average_distance_to_n_nearest_other_labels_map(src, cle.push(other.astype(np.float32)), n=k)),
+                  oracle.average_distance_to_n_nearest_other_labels_map(lab, other, k), 1e-6)
+    assert _close(cle.pull(cle.average_neighbor_distance_map(src)),
+                  oracle.average_neighbor_distance_map(lab), 1e-6)
+
+
+def test_neighbor_maps_on_device_uint32_labels(cle, oracle):
+    # uint32 device labels (the output of voronoi_otsu_labeling): the map is
+    # replace_intensities' destination, made by create_like -- float32 whatever
+    # the labels' type, as _tier0/_create.py create_like makes it
+    lab = _voronoi_labels((40, 50), 30, 24)
+    t = cle.B200Array(torch.from_numpy(lab).cuda())
+    out = cle.average_neighbor_distance_map(t)
+    assert out.dtype == np.float32
+    assert _close(cle.pull(out), oracle.average_neighbor_distance_map(lab), 1e-6)
+    out = cle.average_distance_of_n_nearest_neighbors_map(t, n=3)
+    assert _close(cle.pull(out), oracle.average_distance_of_n_nearest_neighbors_map(lab, 3), 1e-6)
+
+
+def test_n_distances_rejects_large_n(cle):
+    c = cle.centroids_of_labels(cle.push(QUAD))
+    D = cle.generate_distance_matrix(c, c)
+    with pytest.raises(ValueError):
+        cle.average_distance_of_n_shortest_distances(D, n=1001)

@@ -282,3 +282,59 @@ def test_euclidean_distance_from_label_centroid_map_golden(oracle):
     # tests/test_euclidean_distance_from_label_centroid_map.py:4-34 (rtol 1e-3)
     got = oracle.euclidean_distance_from_label_centroid_map(CENTROID_DIST_LABELS)
     assert np.allclose(got, CENTROID_DIST_REF, 0.001)
+
+
+# ---- neighbour-distance maps: the reference's own fixtures ------------------
+QUADRANT_LABELS = np.asarray([[1, 1, 1, 3, 3, 3], [1, 1, 1, 3, 3, 3], [1, 1, 1, 3, 3, 3],
+                              [0, 0, 0, 2, 2, 2], [0, 0, 0, 2, 2, 2], [0, 0, 0, 2, 2, 2]])
+SPARSE_A = np.asarray([[1, 0, 0, 0, 0, 3], [0] * 6, [0] * 6, [0] * 6, [0] * 6, [0, 0, 0, 0, 0, 2]])
+SPARSE_B = np.asarray([[0, 2, 0, 0, 0, 3], [1, 0, 0, 0, 0, 0], [0] * 6, [0] * 6, [0, 0, 0, 0, 0, 4],
+                       [0, 0, 0, 0, 5, 0]])
+
+
+def test_average_distance_of_n_nearest_neighbors_map_golden(oracle):
+    # tests/test_average_distance_of_n_nearest_neighbors.py:4-35 (n = 2, rtol 0.01)
+    ref = np.asarray([[3.62] * 3 + [3] * 3] * 3 + [[0] * 3 + [3.62] * 3] * 3)
+    assert np.allclose(oracle.average_distance_of_n_nearest_neighbors_map(QUADRANT_LABELS, 2), ref, 0.01)
+
+
+def test_average_neighbor_distance_map_golden(oracle):
+    # tests/test_average_neighbor_distance_map.py:4-35
+    ref = np.asarray([[3] * 6] * 3 + [[0] * 3 + [3] * 3] * 3)
+    assert np.allclose(oracle.average_neighbor_distance_map(QUADRANT_LABELS), ref, 0.01)
+
+
+def test_average_distance_to_n_nearest_other_labels_map_golden(oracle):
+    # tests/test_average_distance_to_n_nearest_other_labels_map.py:4-45
+    ref = np.zeros((6, 6))
+    ref[0, 0] = ref[5, 5] = 1
+    got = oracle.average_distance_to_n_nearest_other_labels_map(SPARSE_A, SPARSE_B, 1)
+    assert np.allclose(got, ref, 0.01)
+
+
+def test_neighbor_vectors_golden(oracle):
+    # tests/test_average_distance_of_n_shortest_distances.py,
+    # tests/test_average_distance_of_touching_neighbors.py,
+    # tests/test_average_distance_of_n_nearest_distances.py
+    c = oracle.centroids_of_labels(QUADRANT_LABELS)
+    D = oracle.generate_distance_matrix(c, c)
+    assert np.allclose(oracle.average_distance_of_n_shortest_distances(D, 1), [[0, 3, 3, 3]], 0.01)
+    T = oracle.generate_touch_matrix(QUADRANT_LABELS)
+    assert np.allclose(oracle.average_distance_of_touching_neighbors(D, T), [[0, 3, 3, 3]], 0.01)
+    D2 = oracle.generate_distance_matrix(oracle.centroids_of_labels(SPARSE_A), oracle.centroids_of_labels(SPARSE_B))
+    assert np.allclose(oracle.average_distance_of_n_nearest_distances(D2, 1), [[0, 1, 1, 0]], 0.01)
+
+
+def test_generate_touch_matrix_golden(oracle):
+    # tests/test_generate_touch_matrix.py:4-35
+    lab = np.asarray([[1, 1, 0, 0, 0], [1, 1, 0, 3, 0], [0, 2, 2, 3, 0], [0, 2, 2, 0, 0], [0, 0, 0, 0, 4]])
+    ref = np.asarray([[0, 1, 1, 1, 1], [1, 0, 1, 0, 0], [1, 1, 0, 1, 0], [1, 0, 1, 0, 0], [1, 0, 0, 0, 0]]).T
+    assert np.array_equal(oracle.generate_touch_matrix(lab), ref)
+
+
+def test_n_nearest_selection_keeps_nan_in_place(oracle):
+    # the kernel's insertion pass never moves a NaN (absent label) and never
+    # lets a value pass it: with n = 2 the NaN held first stays in the mean
+    assert np.isnan(oracle._held_mean([np.nan, 3.0, 1.0], 2))
+    assert oracle._held_mean([4.0, 3.0, 1.0, 2.0], 2) == np.float32(1.5)
+    assert np.isnan(oracle._held_mean([], 3))
