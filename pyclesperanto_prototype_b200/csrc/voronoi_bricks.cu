@@ -659,11 +659,17 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
         const bool bitmap = use_bitmap && nB >= kBitmapBricks;
         const uint32_t tag = r + 2;
         const uint32_t wstride = gridDim.x * NW, wbase = blockIdx.x * NW;
-        uint32_t bnext = (wbase + warp < nB) ? __ldcg(F + wbase + warp) : 0u;
+        // odd rounds walk the list (brick order) backwards: a brick visited
+        // later in a round sees what earlier visits wrote, so alternating the
+        // direction lets fronts in every direction cross several bricks per
+        // round, as the plane sweeps do inside a brick
+        const bool rev = (r & 1u) != 0u;
+        auto entry = [&](uint32_t i) { return __ldcg(F + (rev ? nB - 1u - i : i)); };
+        uint32_t bnext = (wbase + warp < nB) ? entry(wbase + warp) : 0u;
         for (uint32_t base = wbase; base < nB; base += wstride) {
             const uint32_t idx = base + warp;
             const uint32_t b = bnext;
-            bnext = (idx + wstride < nB) ? __ldcg(F + idx + wstride) : 0u;
+            bnext = (idx + wstride < nB) ? entry(idx + wstride) : 0u;
             if (idx < nB) {
                 if (lane == 0) ++visits;
                 uint32_t zb, yb, xb;
