@@ -628,7 +628,16 @@ def average_distance_of_touching_neighbors(distance_matrix: Image, touch_matrix:
 
 
 def _n_nearest_vector(pts_a, pts_b, n, exclude_self):
-    vec = create([1, pts_a.shape[1] + 1])
+    na, nb = pts_a.shape[1], pts_b.shape[1]
+    vec = create([1, na + 1])
+    if na == 0 or nb == 0:
+        # an empty point list (an image without labels): the kernel's means
+        # over no rows are 0 / 0 = NaN; column 0 (the background) over nb
+        # zero distances is 0 when n >= 1
+        vec.tensor.fill_(float("nan"))
+        if nb > 0 and int(n) >= 1:
+            vec.tensor[0, 0] = 0.0
+        return vec
     _call("cle_average_distance_of_n_nearest_points", _lib.ref(_T(pts_a)), _lib.ref(_T(pts_b)), int(n),
           1 if exclude_self else 0, _lib.ref(_T(vec)), _lib.stream_ptr())
     return vec
@@ -668,6 +677,9 @@ def average_neighbor_distance_map(labels: Image, distance_map: Image = None) -> 
     centroids = centroids_of_labels(labels)
     L = centroids.shape[1]
     vec = create([1, L + 1])
+    if L == 0:
+        vec.tensor.zero_()                      # no labels: nothing touches
+        return replace_intensities(labels, vec, distance_map)
     ws = _ws("cle_average_distance_of_touching_labels_workspace_bytes", int(L), device=labels.tensor.device)
     _call("cle_average_distance_of_touching_labels", _lib.ref(_T(labels)), _lib.ref(_T(centroids)),
           _lib.ref(_T(vec)), _ptr(ws), ws.numel(), _lib.stream_ptr())

@@ -304,3 +304,19 @@ def test_n_distances_rejects_large_n(cle):
     D = cle.generate_distance_matrix(c, c)
     with pytest.raises(ValueError):
         cle.average_distance_of_n_shortest_distances(D, n=1001)
+
+
+def test_neighbor_maps_without_labels(cle, oracle):
+    # an image without labels (empty point lists): the reference kernels'
+    # means over no rows are NaN, a label touching nothing gets 0
+    zero = np.zeros((6, 7), np.float32)
+    some = np.zeros((6, 7), np.float32)
+    some[1:3, 2:4] = 1
+    some[4, 5] = 2
+    for lab, other in ((zero, zero), (zero, some), (some, zero)):
+        got = cle.pull(cle.average_distance_of_n_nearest_neighbors_map(cle.push(lab), n=2))
+        assert _close(got, oracle.average_distance_of_n_nearest_neighbors_map(lab, 2))
+        got = cle.pull(cle.average_distance_to_n_nearest_other_labels_map(cle.push(lab), cle.push(other), n=1))
+        assert _close(got, oracle.average_distance_to_n_nearest_other_labels_map(lab, other, 1))
+        got = cle.pull(cle.average_neighbor_distance_map(cle.push(lab)))
+        assert _close(got, oracle.average_neighbor_distance_map(lab))
