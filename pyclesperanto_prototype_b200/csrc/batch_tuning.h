@@ -13,11 +13,11 @@ struct BatchTuning {
 };
 
 static const BatchTuning kBatchTuning[] = {
-    {0.0, 16},   // 64x64 x 256 tiles; Mvoxels/s by lanes {1: 27, 2: 52, 4: 103, 8: 173, 12: 152, 16: 198}
-    {16384.0, 16},   // 256x256 x 256 tiles; Mvoxels/s by lanes {1: 208, 2: 383, 4: 739, 8: 1399, 12: 1126, 16: 1460}
-    {185363.8, 16},   // 32x128x128 x 256 tiles; Mvoxels/s by lanes {1: 722, 2: 1375, 4: 2621, 8: 4594, 12: 3898, 16: 4787}
-    {1482910.4, 8},   // 64x256x256 x 47 tiles; Mvoxels/s by lanes {1: 6074, 2: 10318, 4: 15401, 8: 19116, 12: 17063, 16: 17449}
-    {10273904.6, 4},   // 96x512x512 x 7 tiles; Mvoxels/s by lanes {1: 13956, 2: 16871, 4: 17555}
+    {0.0, 16},   // 64x64 x 256 tiles; Mvoxels/s by lanes {1: 35, 2: 47, 4: 102, 8: 155, 12: 158, 16: 182}
+    {16384.0, 16},   // 256x256 x 256 tiles; Mvoxels/s by lanes {1: 389, 2: 646, 4: 1349, 8: 2255, 12: 2007, 16: 2401}
+    {185363.8, 16},   // 32x128x128 x 256 tiles; Mvoxels/s by lanes {1: 1818, 2: 2714, 4: 4780, 8: 6337, 12: 5875, 16: 6640}
+    {1482910.4, 8},   // 64x256x256 x 47 tiles; Mvoxels/s by lanes {1: 8717, 2: 13283, 4: 17601, 8: 20245, 12: 16860, 16: 18233}
+    {10273904.6, 4},   // 96x512x512 x 7 tiles; Mvoxels/s by lanes {1: 16360, 2: 18194, 4: 18498}
 };
 
 }  // namespace cle
