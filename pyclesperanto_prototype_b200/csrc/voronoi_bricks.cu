@@ -565,8 +565,10 @@ struct KState {
 __device__ __forceinline__ uint32_t key_of(uint32_t p, uint32_t sg) {
     return (p && (sg & 0x7Fu) != 0x7Fu) ? (((sg & 0x7Fu) << 24) | (p ^ 0x00FFFFFFu)) : kKInf;
 }
-__device__ __forceinline__ uint32_t key_face(uint32_t k) { return k == kKInf ? kKInf : k + kKS1; }
-__device__ __forceinline__ uint32_t key_diag(uint32_t k) { return k == kKInf ? kKInf : ((k + kKS1) | kKS1); }
+// The two maps, with infinity kept: a real key's step is at most 127, so
+// min(k, INF - S1) only changes infinity, which then maps to infinity again.
+__device__ __forceinline__ uint32_t key_face(uint32_t k) { return min(k, kKInf - kKS1) + kKS1; }
+__device__ __forceinline__ uint32_t key_diag(uint32_t k) { return (min(k, kKInf - kKS1) + kKS1) | kKS1; }
 
 template <bool IS3D, int BZ, int KBT>
 __global__ void __launch_bounds__(KBT, 1)
@@ -756,10 +758,14 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                         const uint32_t sz = __shfl_sync(0xffffffffu, dhm, src_s);
                         const uint32_t qz = __shfl_sync(0xffffffffu, dhm, src_q);
                         const uint32_t hl = __shfl_up_sync(0xffffffffu, hz, 1), hr = __shfl_down_sync(0xffffffffu, hz, 1);
-                        HX[j] = min(hz, min(x0 ? qz : hl, x1 ? qz : hr));
-                        SZ[j] = sz;
-                        HC[j] = __shfl_sync(0xffffffffu, h[kc], src_h);
-                        SC[j] = __shfl_sync(0xffffffffu, h[kc], src_s);
+                        const uint32_t hc = __shfl_sync(0xffffffffu, h[kc], src_h);
+                        const uint32_t sc = __shfl_sync(0xffffffffu, h[kc], src_s);
+                        // only the brick's edge lanes see the halo; elsewhere
+                        // infinity, the minimum's neutral value
+                        HX[j] = (y0 || y1) ? min(hz, min(x0 ? qz : hl, x1 ? qz : hr)) : kKInf;
+                        SZ[j] = (x0 || x1) ? sz : kKInf;
+                        HC[j] = (y0 || y1) ? hc : kKInf;
+                        SC[j] = (x0 || x1) ? sc : kKInf;
                     }
                 }
                 uint32_t k0[BZ], dk[K];
@@ -780,18 +786,24 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                     if constexpr (j < BZ) {
                         constexpr int kc = j + ZR;
                         if ((act >> j) & 1u) {
-                            // box term over the map-2 keys: planes, then x, then y
+                            // box term over the map-2 keys: planes, then x, then y.
+                            // Shuffles within a row (width 8) and across the
+                            // brick's rows give an edge lane its own value, which
+                            // a minimum may include (a voxel's own key never
+                            // beats its true candidates); the halo enters through
+                            // SZ / HX, infinity on interior lanes.
                             uint32_t dz = dk[kc];
                             if constexpr (ZR > 0) dz = min(dz, min(dk[kc - 1], dk[kc + 1]));
-                            const uint32_t cl = __shfl_up_sync(0xffffffffu, dz, 1), cr = __shfl_down_sync(0xffffffffu, dz, 1);
-                            const uint32_t rx = min(dz, min(x0 ? SZ[j] : cl, x1 ? SZ[j] : cr));
+                            const uint32_t cl = __shfl_up_sync(0xffffffffu, dz, 1, kBX);
+                            const uint32_t cr = __shfl_down_sync(0xffffffffu, dz, 1, kBX);
+                            const uint32_t rx = min(min(dz, SZ[j]), min(cl, cr));
                             const uint32_t ru = __shfl_up_sync(0xffffffffu, rx, kBX), rd = __shfl_down_sync(0xffffffffu, rx, kBX);
-                            const uint32_t bm = min(rx, min(y0 ? HX[j] : ru, y1 ? HX[j] : rd));
-                            // face term over the raw keys
+                            const uint32_t bm = min(min(rx, HX[j]), min(ru, rd));
+                            // face term over the raw keys (the same edge rule)
                             const uint32_t v = k[kc];
-                            const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1), fr = __shfl_down_sync(0xffffffffu, v, 1);
+                            const uint32_t fl = __shfl_up_sync(0xffffffffu, v, 1, kBX), fr = __shfl_down_sync(0xffffffffu, v, 1, kBX);
                             const uint32_t fu = __shfl_up_sync(0xffffffffu, v, kBX), fd = __shfl_down_sync(0xffffffffu, v, kBX);
-                            uint32_t fm = min(min(x0 ? SC[j] : fl, x1 ? SC[j] : fr), min(y0 ? HC[j] : fu, y1 ? HC[j] : fd));
+                            uint32_t fm = min(min(min(fl, fr), min(fu, fd)), min(SC[j], HC[j]));
                             if constexpr (ZR > 0) fm = min(fm, min(k[kc - 1], k[kc + 1]));
                             const uint32_t nk = cand[j] ? min(key_face(fm), bm) : v;
                             const bool c = nk != v;
