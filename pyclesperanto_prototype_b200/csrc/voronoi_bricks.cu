@@ -807,8 +807,9 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                             if constexpr (ZR > 0) fm = min(fm, min(k[kc - 1], k[kc + 1]));
                             const uint32_t nk = cand[j] ? min(key_face(fm), bm) : v;
                             const bool c = nk != v;
+                            k[kc] = nk;                  // unchanged lanes store their own value
+                            dk[kc] = key_diag(nk);
                             if (__any_sync(0xffffffffu, c)) {
-                                if (c) { k[kc] = nk; dk[kc] = key_diag(nk); }
                                 const unsigned nb3 = ((7u << j) >> 1) & cmask;   // planes j-1 .. j+1
                                 nxt |= nb3;
                                 act |= nb3;   // the plane the sweep reaches next sees it now

@@ -318,6 +318,26 @@ def test_vol_equal_sigmas_3d_exact(cle, oracle, shape, n, sigma):
     assert np.array_equal(got, ref) and ref.max() > 1
 
 
+@pytest.mark.parametrize("shape", [(20, 60, 64), (9, 33, 45), (70, 90)])
+def test_vol_equal_sigmas_into_dirty_or_aliased_destination(cle, oracle, shape):
+    # equal sigmas with a uint32 destination: the blur clears the label buffer
+    # and the seed pass writes only the seeds -- a destination full of other
+    # values must come out exactly as a fresh one; a destination sharing the
+    # float32 source's memory keeps the seed pass's full write
+    import torch
+    from pyclesperanto_prototype_b200 import synthetic
+    vol = synthetic.nuclei_volume(shape if len(shape) == 3 else (1,) + shape, 12, seed=41)
+    vol = vol.reshape(shape).astype(np.float32)
+    ref = oracle.voronoi_otsu_labeling(vol, 2, 2)
+    dirty = cle.B200Array(torch.full(shape, 0xFFFFFFF0, dtype=torch.uint32, device="cuda"))
+    got = cle.pull(cle.voronoi_otsu_labeling(cle.push(vol), dirty, spot_sigma=2, outline_sigma=2))
+    assert np.array_equal(got, ref) and ref.max() > 0
+    src = torch.from_numpy(vol.copy()).cuda()
+    alias = cle.B200Array(src.view(torch.uint32))
+    got = cle.pull(cle.voronoi_otsu_labeling(cle.B200Array(src), alias, spot_sigma=2, outline_sigma=2))
+    assert np.array_equal(got, ref)
+
+
 def test_vol_edge_cases(cle):
     assert cle.pull(cle.voronoi_otsu_labeling(np.full((16, 16), 3.0, np.float32))).max() == 0
     assert cle.pull(cle.voronoi_otsu_labeling(np.zeros((1, 1), np.float32))).max() == 0
