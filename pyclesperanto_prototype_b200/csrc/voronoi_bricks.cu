@@ -692,19 +692,39 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                 // no neighbour (key infinity), as the reference skips them
                 uint32_t k[K], h[K];
                 bool cm[K], hm[K];   // mask voxels: the lane's column, its halo voxel
+                // a brick whose halo lies inside the image (most of them) needs
+                // no clamps and no validity tests (warp-uniform)
+                const bool inner = z0 >= ZR && z0 + BZ + ZR <= (int)g.D && x0b >= 1 && x0b + kBX < (int)g.W &&
+                                   y0b >= 1 && y0b + kBY < (int)g.H;
+                if (inner) {
+                    const uint32_t HWp = g.H * g.W;
 #pragma unroll
-                for (int q = 0; q < K; ++q) {
-                    const int zq = z0 - ZR + q;
-                    const bool zin = zq >= 0 && zq < (int)g.D;
-                    const uint32_t zo = (uint32_t)clampi(zq, 0, (int)g.D - 1) * g.H * g.W;
-                    const uint32_t kp = ld_cg(lab + zo + coff);
-                    const uint32_t hp = lane < 28 ? ld_cg(lab + zo + hoff) : 0u;
-                    const uint32_t ks = __ldcg(seg + zo + coff);
-                    const uint32_t hs = lane < 28 ? (uint32_t)__ldcg(seg + zo + hoff) : 0u;
-                    cm[q] = zin && xyin && ks != 0u;
-                    hm[q] = zin && hin && hs != 0u;
-                    k[q] = (zin && xyin) ? key_of(kp, ks) : kKInf;
-                    h[q] = (zin && hin) ? key_of(hp, hs) : kKInf;
+                    for (int q = 0; q < K; ++q) {
+                        const uint32_t zo = (uint32_t)(z0 - ZR + q) * HWp;
+                        const uint32_t kp = ld_cg(lab + zo + coff);
+                        const uint32_t hp = lane < 28 ? ld_cg(lab + zo + hoff) : 0u;
+                        const uint32_t ks = __ldcg(seg + zo + coff);
+                        const uint32_t hs = lane < 28 ? (uint32_t)__ldcg(seg + zo + hoff) : 0u;
+                        cm[q] = ks != 0u;
+                        hm[q] = hs != 0u;
+                        k[q] = key_of(kp, ks);
+                        h[q] = key_of(hp, hs);   // lanes 28..31: label 0, infinity
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < K; ++q) {
+                        const int zq = z0 - ZR + q;
+                        const bool zin = zq >= 0 && zq < (int)g.D;
+                        const uint32_t zo = (uint32_t)clampi(zq, 0, (int)g.D - 1) * g.H * g.W;
+                        const uint32_t kp = ld_cg(lab + zo + coff);
+                        const uint32_t hp = lane < 28 ? ld_cg(lab + zo + hoff) : 0u;
+                        const uint32_t ks = __ldcg(seg + zo + coff);
+                        const uint32_t hs = lane < 28 ? (uint32_t)__ldcg(seg + zo + hoff) : 0u;
+                        cm[q] = zin && xyin && ks != 0u;
+                        hm[q] = zin && hin && hs != 0u;
+                        k[q] = (zin && xyin) ? key_of(kp, ks) : kKInf;
+                        h[q] = (zin && hin) ? key_of(hp, hs) : kKInf;
+                    }
                 }
                 // candidates: mask voxels that are not seeds (seeds have s = 0)
                 bool cand[BZ];
