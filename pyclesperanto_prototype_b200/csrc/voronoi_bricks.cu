@@ -633,6 +633,17 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
     const int src_h = yl == 0 ? xl : 8 + xl;
     const int src_s = (xl == 0 ? 16 : 20) + (yl & 3);
     const int src_q = 24 + (yl == kBY - 1 ? 2 : 0) + (xl == kBX - 1 ? 1 : 0);
+    // the neighbouring brick lane d < 27 stands for in the queueing and the
+    // presence test: its offset, the brick voxels (as ballot bits) that face
+    // it, and the halo lanes that lie in it -- fixed for the whole launch
+    const int qdz = lane / 9 - 1, qdy = (lane / 3) % 3 - 1, qdx = lane % 3 - 1;
+    const bool qself = qdz == 0 && qdy == 0 && qdx == 0;
+    const bool qlive = lane < 27 && (IS3D || qdz == 0);
+    const unsigned qmask = (qdy < 0 ? 0x000000FFu : qdy > 0 ? 0xFF000000u : 0xFFFFFFFFu) &
+                           (qdx < 0 ? 0x01010101u : qdx > 0 ? 0x80808080u : 0xFFFFFFFFu);
+    const unsigned qhsel = qdy == 0 ? (qdx < 0 ? 0x000F0000u : 0x00F00000u)
+                         : qdx == 0 ? (qdy < 0 ? 0x000000FFu : 0x0000FF00u)
+                         : (1u << (24 + (qdy > 0 ? 2 : 0) + (qdx > 0 ? 1 : 0)));
 
     const uint64_t t_start = global_ns();
     // trace: the last two rows hold the set-up (round 0's queue) and the
@@ -739,17 +750,13 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                 // change that brick, and it is not queued for it
                 bool present = false;
                 {
-                    const int dzn = lane / 9 - 1, dyn = (lane / 3) % 3 - 1, dxn = lane % 3 - 1;
-                    const unsigned hsel = dyn == 0 ? (dxn < 0 ? 0x000F0000u : 0x00F00000u)
-                                        : dxn == 0 ? (dyn < 0 ? 0x000000FFu : 0x0000FF00u)
-                                        : (1u << (24 + (dyn > 0 ? 2 : 0) + (dxn > 0 ? 1 : 0)));
                     unsigned pres = 0u;
 #pragma unroll
                     for (int q = 0; q < K; ++q) {
                         const unsigned cb = __ballot_sync(0xffffffffu, cm[q] && (k[q] >> 24) != 0u);
                         const unsigned hb = __ballot_sync(0xffffffffu, hm[q] && (h[q] >> 24) != 0u);
-                        const bool inP = dzn < 0 ? q == 0 : (dzn > 0 ? q == K - 1 : (q >= ZR && q < ZR + BZ));
-                        if (inP) pres |= (dyn == 0 && dxn == 0) ? cb : (hb & hsel);
+                        const bool inP = qdz < 0 ? q == 0 : (qdz > 0 ? q == K - 1 : (q >= ZR && q < ZR + BZ));
+                        if (inP) pres |= (qdy == 0 && qdx == 0) ? cb : (hb & qhsel);
                     }
                     present = lane < 27 && pres != 0u;
                 }
@@ -875,23 +882,17 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                 }
                 if (over) atomicExch(&S->overflow, 1);
                 if (chall && lane == 0) atomicOr(touched + (b >> 5), 1u << (b & 31u));
+                // this brick again if it is still changing, a neighbour when a
+                // changed voxel faces it and it holds a candidate next to them
                 bool want = false;
-                if (lane < 27) {
-                    const int dz = lane / 9 - 1, dyb = (lane / 3) % 3 - 1, dxb = lane % 3 - 1;
-                    if (IS3D || dz == 0) {
-                        unsigned sel = dz < 0 ? chb[0] : (dz > 0 ? chb[BZ - 1] : chall);
-                        if (dyb < 0) sel &= 0x000000FFu;
-                        else if (dyb > 0) sel &= 0xFF000000u;
-                        if (dxb < 0) sel &= 0x01010101u;
-                        else if (dxb > 0) sel &= 0x80808080u;
-                        want = sel != 0u && present && !(dz == 0 && dyb == 0 && dxb == 0);
-                        if (!conv && dz == 0 && dyb == 0 && dxb == 0) want = true;
-                    }
+                if (qlive) {
+                    const unsigned sel = (qdz < 0 ? chb[0] : (qdz > 0 ? chb[BZ - 1] : chall)) & qmask;
+                    want = qself ? !conv : (sel != 0u && present);
                 }
                 if (bitmap) {
-                    uint32_t nb = 0;
-                    if (want && neighbour_brick(G, zb, yb, xb, lane, nb))
-                        atomicOr(Qb.q + (nb >> 5), 1u << (nb & 31u));
+                    const uint32_t zz = zb + (uint32_t)qdz, yy = yb + (uint32_t)qdy, xx = xb + (uint32_t)qdx;
+                    if (want && zz < G.DB && yy < G.HB && xx < G.WB)   // unsigned: -1 wraps above
+                        atomicOr(Qb.q + (((zz * G.HB + yy) * G.WB + xx) >> 5), 1u << (((zz * G.HB + yy) * G.WB + xx) & 31u));
                 } else {
                     queue_neighbours(G, zb, yb, xb, want, tag, bstep, ap);
                 }
