@@ -574,7 +574,7 @@ template <bool IS3D, int BZ, int KBT>
 __global__ void __launch_bounds__(KBT, 1)
 voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                     const uint32_t *d_seed_count, const uint32_t *d_max_label, uint32_t *B0, uint32_t *B1,
-                    uint32_t *bstep, uint32_t *touched, KState *S, int *d_status, uint32_t max_steps,
+                    uint32_t *bstep, KState *S, int *d_status, uint32_t max_steps,
                     uint64_t loop_ns, uint64_t barrier_ns, const volatile int *cancel,
                     unsigned long long *trace, BQueue Qb, int use_bitmap) {
     constexpr int NW = KBT / 32;
@@ -881,7 +881,6 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
                     chall |= chb[j];
                 }
                 if (over) atomicExch(&S->overflow, 1);
-                if (chall && lane == 0) atomicOr(touched + (b >> 5), 1u << (b & 31u));
                 // this brick again if it is still changing, a neighbour when a
                 // changed voxel faces it and it holds a candidate next to them
                 bool want = false;
@@ -952,31 +951,11 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
     const bool cut = s_off[1] != 0u;
     if (cut) {
         // labels of voxels that arrived after step S (or, after an overflow,
-        // of every grown voxel) go back to 0: the touched bricks in a list
-        // (the next-round bitmap q is clear and serves as the empty filter)
-        BQueue Tq = Qb;
-        Tq.q = touched;
-        Tq.done = Qb.q;
-        ok = compact_queue(Tq, B0, &S->sizes[0], S, barrier_ns, s_red, s_scan, s_off);
-        if (!ok) {
-            if (gtid == 0) *d_status = *(volatile int *)&S->err;
-            return;
-        }
-        const uint32_t nT = __ldcg(&S->sizes[0]);
-        for (uint32_t idx = blockIdx.x * NW + warp; idx < nT; idx += gridDim.x * NW) {
-            const uint32_t b = __ldcg(B0 + idx);
-            uint32_t zb, yb, xb;
-            brick_zyx(G, b, zb, yb, xb);
-            const uint32_t x = xb * kBX + (uint32_t)xl, y = yb * kBY + (uint32_t)yl;
-            if (x >= g.W || y >= g.H) continue;
-#pragma unroll
-            for (int j = 0; j < BZ; ++j) {
-                const uint32_t z = zb * BZ + (uint32_t)j;
-                if (z >= g.D) break;
-                const uint32_t m = (z * g.H + y) * g.W + x;
-                const uint32_t sv = (uint32_t)__ldcg(seg + m) & 0x7Fu;
-                if (sv > stop && ld_cg(lab + m) != 0u) st_cg(lab + m, 0u);
-            }
+        // of every grown voxel) go back to 0: a pass over the mask bytes
+        const int64_t nvox = (int64_t)g.D * g.H * g.W;
+        for (int64_t m = (int64_t)blockIdx.x * KBT + threadIdx.x; m < nvox; m += (int64_t)gridDim.x * KBT) {
+            const uint32_t sg = (uint32_t)__ldcg(seg + m);
+            if (sg != 0u && (sg & 0x7Fu) > stop && (sg & 0x7Fu) != 0x7Fu && ld_cg(lab + m) != 0u) st_cg(lab + (size_t)m, 0u);
         }
     }
     if (trace) {
@@ -1087,7 +1066,6 @@ size_t keys_part_bytes(const Img &im) {
     a.take<uint32_t>(nb);               // per-brick round tags
     a.take<uint32_t>((nb + 31) / 32);   // queue bitmap
     a.take<uint32_t>((nb + 31) / 32);   // bricks without candidates
-    a.take<uint32_t>((nb + 31) / 32);   // bricks with grown voxels
     a.take<uint32_t>(2048);             // per-CTA counts of the compaction
     return a.off;
 }
@@ -1114,13 +1092,12 @@ int voronoi_grow(const Img &im, uint32_t *lab, uint8_t *seg, const uint32_t *see
     Qb.nwords = (uint32_t)((nb + 31) / 32);
     Qb.q = ws.take<uint32_t>(Qb.nwords);
     Qb.done = ws.take<uint32_t>(Qb.nwords);
-    uint32_t *touched = ws.take<uint32_t>(Qb.nwords);
     Qb.ccount = ws.take<uint32_t>(2048);
     if (!ws.ok()) { set_error("masked_voronoi_labeling: workspace too small"); return CLE_ERR_WORKSPACE; }
     CLE_CUDA(cudaMemsetAsync(S, 0, sizeof(KState), st));
     CLE_CUDA(cudaMemsetAsync(bstep, 0, sizeof(uint32_t) * nb, st));
-    // q, done and touched are adjacent: one clear
-    CLE_CUDA(cudaMemsetAsync(Qb.q, 0, (size_t)((char *)(touched + Qb.nwords) - (char *)Qb.q), st));
+    // q and done are adjacent: one clear
+    CLE_CUDA(cudaMemsetAsync(Qb.q, 0, (size_t)((char *)(Qb.done + Qb.nwords) - (char *)Qb.q), st));
     BGeo G;
     G.g = make_geo(im);
     G.WB = bricks_x(im);
@@ -1147,7 +1124,7 @@ int voronoi_grow(const Img &im, uint32_t *lab, uint8_t *seg, const uint32_t *see
         (unsigned long long *)profile_trace_buffer(4 * kTraceSteps * sizeof(unsigned long long), st);
     int use_bitmap = im.n() > kWideVoxels ? 1 : 0;
     void *args[] = {&lab, (void *)&seg, &G, (void *)&seeds, (void *)&d_seed_count, (void *)&d_max_label,
-                    &B0, &B1, &bstep, &touched, &S, &d_status, &max_steps, &loop_ns, &barrier_ns,
+                    &B0, &B1, &bstep, &S, &d_status, &max_steps, &loop_ns, &barrier_ns,
                     (void *)&cancel, &trace, &Qb, &use_bitmap};
     CLE_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kKeyBT), args, smem, st));
     count_launches(1);
