@@ -138,10 +138,10 @@ MEASURED_TRAFFIC = {
                },
     # slab captures (128x1024x1024) scaled by 4 to the 512x1024x1024 volume:
     # the same recipe and cell density, traffic in proportion to the voxels
-    "lightsheet": {"voronoi_growth": (4 * 1.486e9, "voronoi_keys_kernel_lightsheet_slab_128x1024x1024.md"),
+    "lightsheet": {"voronoi_growth": (4 * 1.494e9, "voronoi_keys_kernel_lightsheet_slab_128x1024x1024.md"),
                    "blur_spot": (4 * 0.792e9, "blur_fused_kernel_lightsheet_slab_128x1024x1024.md"),
                    "threshold_seeds": (4 * 1.165e9, "maxima_seeds_kernel_lightsheet_slab_128x1024x1024.md")},
-    "lightsheet_slab": {"voronoi_growth": (1.486e9, "voronoi_keys_kernel_lightsheet_slab_128x1024x1024.md"),
+    "lightsheet_slab": {"voronoi_growth": (1.494e9, "voronoi_keys_kernel_lightsheet_slab_128x1024x1024.md"),
                         "blur_spot": (0.792e9, "blur_fused_kernel_lightsheet_slab_128x1024x1024.md"),
                         "threshold_seeds": (1.165e9, "maxima_seeds_kernel_lightsheet_slab_128x1024x1024.md")},
 }
