@@ -526,15 +526,18 @@ voronoi_bricks_kernel(uint32_t *lab, const uint8_t *__restrict__ seg, BGeo G,
 // queues nothing.
 //
 // The reference's loop stops at the first step that labels nothing: with S
-// the smallest s >= 1 that no voxel holds, voxels of s > S stay unlabelled,
-// and a last pass turns the kept keys into labels.  Per-CTA counts of the
-// voxels per s (kept up to date at every write) give S.
+// the smallest s >= 1 that no voxel holds, voxels of s > S stay unlabelled.
+// Per-CTA counts of the voxels per s (kept up to date at every write) give S;
+// only when some voxel holds an s above S does a last pass over the mask
+// bytes set those labels back to 0.
 //
-// The label buffer holds, during the growth: 0 (unlabelled or outside the
-// mask), a seed's label L (s = 0), or s << 24 | L for a grown voxel; the key
-// of a stored value p != 0 is p ^ 0xFFFFFF.  Labels above 2^24 - 1 or an s
+// The label buffer holds plain labels throughout (0: unlabelled or outside
+// the mask); a labelled voxel's s lives in its mask byte (bit 7: in the mask,
+// bits 0-6: s, 127 while not yet known, as the seed passes write it), and
+// its key is s << 24 | (label ^ 0xFFFFFF).  Labels above 2^24 - 1 or an s
 // above kKeyMaxS do not fit: the kernel then leaves the labels as it found
-// them and raises the gate word, and the brick kernel grows them instead.
+// them (after an overflow it sets every grown voxel back to 0) and raises the
+// gate word, and the brick kernel grows them instead.
 
 constexpr uint32_t kKInf = 0xFFFFFFFFu;
 constexpr uint32_t kKS1 = 0x01000000u;
@@ -543,7 +546,7 @@ constexpr int kKeyIters = 32;     // local iterations per visit; a brick still c
 #ifndef CLE_KEY_BT
 #define CLE_KEY_BT 1024
 #endif
-constexpr int kKeyBT = CLE_KEY_BT; // threads per CTA of the key kernel (1024: light-sheet 4.10 ms vs 4.63 at 768)
+constexpr int kKeyBT = CLE_KEY_BT; // threads per CTA of the key kernel (1024: 32 warps per SM, measured faster than 768 or 2 x 512)
 
 struct KState {
     GridBarrier bar;
@@ -551,9 +554,9 @@ struct KState {
     int gate;          // 1: the brick kernel grows the labels after this launch
     int overflow;      // an s above kKeyMaxS was reached
     uint32_t sizes[4];
-    uint32_t rounds;
-    uint32_t stop_s;   // S
-    uint32_t visits;
+    uint32_t rounds;   // diagnostics of the last launch: rounds run,
+    uint32_t stop_s;   // S,
+    uint32_t visits;   // brick visits
     int hist[256];     // grown voxels per s
 };
 
@@ -908,7 +911,7 @@ voronoi_keys_kernel(uint32_t *lab, uint8_t *seg, BGeo G, const uint32_t *seeds,
         if (trace && gtid == 0 && r < kTraceSteps) trace[4 * r + 3] = global_ns() - t_start;
         ++r;
     }
-    // ---- finish: S from the counts, keys back to labels ----------------------
+    // ---- finish: S from the counts, the cut of voxels that arrived after S ----
     if (trace && gtid == 0) trace[4 * (kTraceSteps - 1)] = global_ns() - t_start;
     const uint32_t vs = block_total(visits, s_red);
     if (threadIdx.x == 0 && vs) atomicAdd(&S->visits, vs);
